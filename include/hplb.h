@@ -1,0 +1,153 @@
+/*
+ * hplb.h -- C ABI of the B200-native HPL solve path (single process, P = Q = 1).
+ *
+ * Drop-in boundary for rocHPL's solve path.  Each entry point names the
+ * reference interface it replaces (paths are within the rocHPL tree):
+ *
+ *   hplb_matgen   <- HPL_pdrandmat / hpl_randmat   src/matgen/HPL_pdrandmat_device.cpp:84-201
+ *   hplb_pdgesv   <- HPL_pdgesv                     include/hpl_pgesv.hpp:162,
+ *                                                   src/pgesv/HPL_pdgesv.cpp:19-368
+ *   hplb_residual <- the check in HPL_pdtest        src/HPL_pdtest.cpp:307-438
+ *                    with HPL_pdlange               src/pauxil/HPL_pdlange_device.cpp:118-302
+ *   hplb_default_ld <- the ld padding of HPL_pdmatgen src/matgen/HPL_pdmatgen.cpp:109-110
+ *
+ * Conventions
+ *  - Matrices are column-major FP64 in device memory owned by the caller;
+ *    [A|b] is N x (N+1) with b in column N, exactly as HPL_pdmatgen lays it out.
+ *  - The context owns its streams, events and workspaces; one context per host
+ *    thread.  Calls return once the device work they queued has finished.
+ *  - Every call returns an hplb_status; nothing calls exit().  Device-side waits
+ *    are bounded and surface as HPLB_ERR_TIMEOUT.
+ */
+#ifndef HPLB_H
+#define HPLB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum hplb_status {
+  HPLB_OK              = 0,
+  HPLB_ERR_ARG         = 1, /* invalid argument (message in hplb_last_error) */
+  HPLB_ERR_OOM         = 2, /* workspace allocation failed */
+  HPLB_ERR_SINGULAR    = 3, /* exact zero pivot; the solve still completed */
+  HPLB_ERR_TIMEOUT     = 4, /* a bounded device-side wait expired */
+  HPLB_ERR_CUDA        = 5, /* CUDA runtime error (message in hplb_last_error) */
+  HPLB_ERR_UNSUPPORTED = 6  /* parameter combination rocHPL also rejects */
+} hplb_status;
+
+typedef struct hplb_ctx hplb_ctx;
+
+/* Algorithm parameters: the HPL.dat fields of HPL_T_palg that reach the solve
+ * (include/hpl_pgesv.hpp:63-81).  pfact / rfact use the HPL.dat encoding:
+ * 0 = left-looking, 1 = Crout, 2 = right-looking. */
+typedef struct hplb_algo {
+  int nb;       /* panel width NB (>= 1) */
+  int nbmin;    /* recursion stopping width NBMIN (>= 1) */
+  int ndiv;     /* panels per recursion level NDIV (>= 2) */
+  int pfact;    /* leaf factorisation PFACT */
+  int rfact;    /* recursive factorisation RFACT */
+  int depth;    /* look-ahead depth; rocHPL accepts 1 only (src/HPL_pdinfo.cpp:931-935) */
+  int l1notran; /* L1 form; 0 (transposed) or 1; no effect on results */
+} hplb_algo;
+
+/* Residual check results (src/HPL_pdtest.cpp:330-438). */
+typedef struct hplb_resid {
+  double resid;     /* ||b-Ax||oo / (eps (||A||oo ||x||oo + ||b||oo) N) */
+  double rnorm_inf; /* ||b-Ax||oo */
+  double anorm_1;   /* ||A||1 */
+  double anorm_inf; /* ||A||oo */
+  double xnorm_1;   /* ||x||1 */
+  double xnorm_inf; /* ||x||oo */
+  double bnorm_inf; /* ||b||oo */
+  double eps;       /* 2^-53, HPL_dlamch's eps (src/auxil/HPL_dlamch.cpp:104-111) */
+} hplb_resid;
+
+/* Per-call timings of the last hplb_pdgesv, from CUDA events (ms). */
+typedef struct hplb_timing {
+  double total_ms;  /* whole solve, LU + back-solve */
+  double lu_ms;     /* factorisation incl. trailing updates */
+  double trsv_ms;   /* back-solve */
+  double gemm_ms;   /* sum of trailing-update DGEMM kernel time */
+  double gemm_flops; /* algorithmic DGEMM flops of those kernels */
+  double panel_ms;  /* sum of panel factorisation time (concurrent with updates) */
+  int    gemm_launches;
+  int    kernel_launches; /* every kernel this library queued during the call */
+} hplb_timing;
+
+/* Create a context on CUDA device `device`.  Returns NULL on failure, with the
+ * reason in *status when status is not NULL. */
+hplb_ctx* hplb_create(int device, hplb_status* status);
+void      hplb_destroy(hplb_ctx* ctx);
+
+const char* hplb_status_string(hplb_status s);
+/* Message of the last failing call on this context (never NULL). */
+const char* hplb_last_error(const hplb_ctx* ctx);
+
+/* rocHPL's padded leading dimension for an n-row local matrix:
+ * ((max(1,n)+95)/128)*128 + 32 (src/matgen/HPL_pdmatgen.cpp:109-110). */
+int64_t hplb_default_ld(int n);
+
+/* HPL_pdrandmat at P = Q = 1: fill the m x n column-major device matrix dA
+ * (leading dimension ld >= m) from the 64-bit LCG with seed `seed`; entry
+ * (i, j) is the value of state X(1 + i + j*m).  Bit-exact with rocHPL.
+ * nb is accepted for interface parity and does not change the values. */
+hplb_status hplb_matgen(hplb_ctx* ctx, int m, int n, int nb, uint64_t seed,
+                        double* dA, int64_t ld);
+
+/* HPL_pdgesv at P = Q = 1: LU-factor the n x (n+1) [A|b] in dA (ld >= n) with
+ * row partial pivoting and look-ahead depth 1, then back-solve U x = y into
+ * dX (n doubles, device).  On exit dA holds U in its upper triangle, the panel
+ * multipliers below it (unpivoted across panels, as in rocHPL) and y in
+ * column n.  ipiv_out (device, n ints, may be NULL) receives, for each column
+ * j, the global row swapped into row j.  *info (host, may be NULL) receives
+ * the first zero-pivot column (1-based) or 0; a zero pivot also returns
+ * HPLB_ERR_SINGULAR after the solve completes. */
+hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA,
+                        int64_t ld, double* dX, int* ipiv_out, int* info);
+
+/* The HPL residual check: dA must hold the regenerated [A|b] (hplb_matgen with
+ * the seed of the solve), dX the solution.  Results go to *out (host). */
+hplb_status hplb_residual(hplb_ctx* ctx, int n, const double* dA, int64_t ld,
+                          const double* dX, hplb_resid* out);
+
+/* Same check without a stored matrix: [A|b] is regenerated from the LCG inside
+ * the kernel (bit-identical values), so no N x N buffer is read or written. */
+hplb_status hplb_residual_lcg(hplb_ctx* ctx, int n, uint64_t seed,
+                              const double* dX, hplb_resid* out);
+
+/* Timings of the last hplb_pdgesv on this context. */
+hplb_status hplb_last_timing(const hplb_ctx* ctx, hplb_timing* out);
+
+/* Building blocks, exposed for tests and tools (device pointers, synchronous).
+ *   hplb_dgemm_sub : C(m x n) -= A(m x k) B(k x n), column-major; the trailing
+ *                    update kernel of hplb_pdgesv (rocblas_dgemm call in
+ *                    src/pgesv/HPL_pdupdateTT.cpp:131-163).
+ *   hplb_laswp_trsm: apply the row interchanges ipiv (jb global rows, first row
+ *                    ia) to columns [c0, c0+n) of dA and replace the top jb rows
+ *                    by L11^-1 times them, L11 the unit lower triangle at
+ *                    (ia, lc) (HPL_dlaswp00N + rocblas_dtrsm,
+ *                    src/pgesv/HPL_pdupdateTT.cpp:95-106). */
+hplb_status hplb_dgemm_sub(hplb_ctx* ctx, int m, int n, int k, const double* dA,
+                           int64_t lda, const double* dB, int64_t ldb, double* dC,
+                           int64_t ldc);
+hplb_status hplb_laswp_trsm(hplb_ctx* ctx, double* dA, int64_t ld, int ia, int jb,
+                            int lc, const int* ipiv_host, int c0, int n);
+
+/* Measurement and self-test utilities (no counterpart in the reference).
+ *   hplb_fp64_peak          : FP64 tensor-core (DMMA m16n8k8) and FP64 FMA issue
+ *                             rates of this GPU in TFLOP/s, the roofline
+ *                             denominators for the trailing-update DGEMM.
+ *   hplb_selftest_wait_timeout : runs one bounded device wait on a flag nothing
+ *                             sets, with a budget of budget_ns nanoseconds; returns
+ *                             HPLB_ERR_TIMEOUT and leaves the context usable. */
+hplb_status hplb_fp64_peak(hplb_ctx* ctx, int iters, double* dmma_tflops, double* dfma_tflops);
+hplb_status hplb_selftest_wait_timeout(hplb_ctx* ctx, uint64_t budget_ns);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HPLB_H */

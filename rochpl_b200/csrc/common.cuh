@@ -1,0 +1,94 @@
+// Shared device helpers for the B200 HPL solve path.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "hplb.h"
+
+#define HPLB_DEV __device__ __forceinline__
+
+namespace hplb {
+
+// Device status word layout (int32 each), written by kernels, read by the host
+// after a synchronisation point.
+enum : int {
+  ST_TIMEOUT = 0,  // nonzero: a bounded device wait gave up (value = site id)
+  ST_INFO    = 1,  // first zero-pivot column, 1-based (atomicMin-style, 0 = none)
+  ST_COUNT   = 4
+};
+
+// Wait budget for every spin in this library (ns of %globaltimer).  Long enough
+// for a co-scheduled trailing-update grid to drain, short enough that a lost
+// block surfaces as HPLB_ERR_TIMEOUT instead of a hung GPU.
+constexpr unsigned long long kWaitBudgetNs = 4000000000ull;
+
+HPLB_DEV unsigned long long globaltimer() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
+
+HPLB_DEV int ld_acquire_gpu(const int* p) {
+  int v;
+  asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+HPLB_DEV void st_release_gpu(int* p, int v) {
+  asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// Grid-wide barrier for co-resident (cooperatively launched) grids.
+// bar[0] = arrival count, bar[1] = generation.  Every wait is bounded: on
+// expiry the block records `site` in status[ST_TIMEOUT] and the barrier
+// returns false; callers then leave the kernel.  A timed-out barrier leaves
+// bar[] inconsistent, so the host zeroes it before every launch.
+HPLB_DEV bool grid_sync(int* bar, int nblocks, int* status, int site) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    int ok = 1;
+    if(ld_acquire_gpu(status + ST_TIMEOUT) != 0) {
+      ok = 0;
+    } else {
+      const int gen = ld_acquire_gpu(bar + 1);
+      __threadfence();
+      const int arrived = atomicAdd(bar, 1);
+      if(arrived == nblocks - 1) {
+        bar[0] = 0;
+        __threadfence();
+        atomicAdd(bar + 1, 1);
+      } else {
+        const unsigned long long t0 = globaltimer();
+        while(ld_acquire_gpu(bar + 1) == gen) {
+          if(globaltimer() - t0 > kWaitBudgetNs) {
+            atomicCAS(status + ST_TIMEOUT, 0, site);
+            ok = 0;
+            break;
+          }
+          if(ld_acquire_gpu(status + ST_TIMEOUT) != 0) {
+            ok = 0;
+            break;
+          }
+          __nanosleep(32);
+        }
+      }
+      __threadfence();
+    }
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// Record the first (lowest) zero-pivot column, 1-based.
+HPLB_DEV void record_info(int* status, int col1) {
+  int old = status[ST_INFO];
+  while(old == 0 || col1 < old) {
+    const int prev = atomicCAS(status + ST_INFO, old, col1);
+    if(prev == old) break;
+    old = prev;
+  }
+}
+
+}  // namespace hplb

@@ -1,0 +1,530 @@
+// Host runtime and C ABI of libhplb200 (include/hplb.h).
+//
+// hplb_pdgesv is the single-process HPL_pdgesv (src/pgesv/HPL_pdgesv.cpp:19-368)
+// with look-ahead depth 1 made real on the GPU: the panel factorisation runs on
+// a high-priority stream concurrently with the bulk of the previous panel's
+// trailing update on the update stream.  Per panel j:
+//
+//   update stream : wait(panel j) -> swap+TRSM and DGEMM on the next panel's
+//                   columns (look-ahead) -> record -> swap+TRSM and DGEMM on
+//                   the rest of the trailing matrix, b included
+//   panel stream  :                       wait(look-ahead) -> factor panel j+1
+//
+// which is the order of :182-191 with the two halves genuinely overlapped.
+// Pivots never leave the device: the leaf kernel records them and a tiny
+// kernel turns them into the row map the trailing swap uses (the reference
+// copies pivots to the host and back once per panel, HPL_pdpanel_swapids.cpp).
+#include <algorithm>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "internal.h"
+
+using namespace hplb;
+
+struct hplb_ctx {
+  int          device  = 0;
+  int          num_sms = 0;
+  cudaStream_t s_upd   = nullptr;
+  cudaStream_t s_pan   = nullptr;
+  std::string  err;
+  hplb_timing  timing{};
+
+  int*    d_status = nullptr;  // ST_COUNT ints
+  int*    d_bar    = nullptr;  // 2 ints
+  double* d_out8   = nullptr;  // residual outputs
+
+  int*    d_ipiv   = nullptr;
+  size_t  ipiv_cap = 0;
+  int*    d_perm[2] = {nullptr, nullptr};
+  double* d_dinv[2] = {nullptr, nullptr};
+  double* d_dinv_piece = nullptr;
+  int     nb_cap       = 0;
+  double* d_cand       = nullptr;
+  double* d_cur        = nullptr;
+  size_t  cand_cap     = 0;  // doubles
+  double* d_res        = nullptr;
+  size_t  res_cap      = 0;  // doubles
+
+  std::vector<cudaEvent_t> events;  // pool
+  size_t                   ev_next = 0;
+  int                      launches = 0;
+};
+
+namespace {
+
+hplb_status set_err(hplb_ctx* c, hplb_status s, const char* fmt, ...) {
+  char    buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if(c) c->err = buf;
+  return s;
+}
+
+#define CK(expr)                                                                       \
+  do {                                                                                 \
+    cudaError_t e__ = (expr);                                                          \
+    if(e__ != cudaSuccess)                                                             \
+      return set_err(ctx, HPLB_ERR_CUDA, "%s failed: %s (%s:%d)", #expr,               \
+                     cudaGetErrorString(e__), __FILE__, __LINE__);                     \
+  } while(0)
+
+template <class T>
+hplb_status grow(hplb_ctx* ctx, T** p, size_t* cap, size_t need) {
+  if(*cap >= need && *p) return HPLB_OK;
+  if(*p) cudaFree(*p);
+  *p   = nullptr;
+  *cap = 0;
+  if(cudaMalloc((void**)p, need * sizeof(T)) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return set_err(ctx, HPLB_ERR_OOM, "workspace allocation of %zu bytes failed",
+                   need * sizeof(T));
+  }
+  *cap = need;
+  return HPLB_OK;
+}
+
+cudaEvent_t next_event(hplb_ctx* ctx) {
+  if(ctx->ev_next == ctx->events.size()) {
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    ctx->events.push_back(e);
+  }
+  return ctx->events[ctx->ev_next++];
+}
+
+hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
+  hplb_status s;
+  if((s = grow(ctx, &ctx->d_ipiv, &ctx->ipiv_cap, (size_t)std::max(n, 1))) != HPLB_OK) return s;
+  if(nb > ctx->nb_cap) {
+    for(int i = 0; i < 2; ++i) {
+      if(ctx->d_perm[i]) cudaFree(ctx->d_perm[i]);
+      if(ctx->d_dinv[i]) cudaFree(ctx->d_dinv[i]);
+      ctx->d_perm[i] = nullptr;
+      ctx->d_dinv[i] = nullptr;
+    }
+    if(ctx->d_dinv_piece) cudaFree(ctx->d_dinv_piece);
+    ctx->d_dinv_piece = nullptr;
+    const size_t nblk = (size_t)(nb + 31) / 32 + 1;
+    for(int i = 0; i < 2; ++i) {
+      if(cudaMalloc(&ctx->d_perm[i], 2 * (size_t)nb * sizeof(int)) != cudaSuccess ||
+         cudaMalloc(&ctx->d_dinv[i], nblk * 32 * 32 * sizeof(double)) != cudaSuccess) {
+        cudaGetLastError();
+        return set_err(ctx, HPLB_ERR_OOM, "panel workspace allocation failed");
+      }
+    }
+    if(cudaMalloc(&ctx->d_dinv_piece, nblk * 32 * 32 * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      return set_err(ctx, HPLB_ERR_OOM, "panel workspace allocation failed");
+    }
+    ctx->nb_cap = nb;
+  }
+  const int    gmax = leaf_grid_size(ctx->num_sms, std::max(n, 1));
+  const size_t need = 2 * (size_t)gmax * (2 + std::min(nbmin, kMaxLeaf)) + 2 * kMaxLeaf;
+  if((s = grow(ctx, &ctx->d_cand, &ctx->cand_cap, need)) != HPLB_OK) return s;
+  ctx->d_cur = ctx->d_cand + 2 * (size_t)gmax * (2 + std::min(nbmin, kMaxLeaf));
+  return HPLB_OK;
+}
+
+struct Solve {
+  hplb_ctx*        ctx;
+  const hplb_algo* algo;
+  double*          A;
+  int64_t          ld;
+  int              n;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> gemm_ev;
+  std::vector<double>                              gemm_flops;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> panel_ev;
+
+  double* a(int i, int j) const { return A + (size_t)i + (size_t)j * (size_t)ld; }
+
+  // Leaf plus the propagation of its interchanges to the rest of the panel.
+  hplb_status leaf(int r0, int c0, int w, int pc, int pw) {
+    hplb_ctx* ctx  = this->ctx;
+    const int grid = leaf_grid_size(ctx->num_sms, n - r0);
+    CK(launch_leaf(A, ld, r0, n, c0, w, ctx->d_ipiv, ctx->d_cand, ctx->d_cur, ctx->d_bar,
+                   ctx->d_status, grid, ctx->s_pan));
+    CK(launch_panel_swap(A, ld, ctx->d_ipiv, r0, c0, w, pc, pw, ctx->s_pan));
+    ctx->launches += 2;
+    return HPLB_OK;
+  }
+
+  // Recursive panel factorisation of rows [r0, n) x columns [c0, c0+N) of the
+  // panel [pc, pc+pw) (src/pfact/HPL_pdrpanrlT.cpp:74-160 and the left / Crout
+  // orderings of HPL_pdrpanllT.cpp / HPL_pdrpancrT.cpp).
+  hplb_status rpanel(int r0, int c0, int N, int pc, int pw) {
+    hplb_ctx*   ctx   = this->ctx;
+    const int   nbmin = std::min(std::max(algo->nbmin, 1), kMaxLeaf);
+    const int   ndiv  = std::max(algo->ndiv, 2);
+    hplb_status s;
+    if(N <= nbmin) return leaf(r0, c0, N, pc, pw);
+    const int nbs = (((N + nbmin - 1) / nbmin + ndiv - 1) / ndiv) * nbmin;
+    int       jj = 0, rem = N, jb = nbs;
+    cudaStream_t st = ctx->s_pan;
+    if(algo->rfact == 2) {
+      do {
+        rem -= jb;
+        if((s = rpanel(r0 + jj, c0 + jj, jb, pc, pw)) != HPLB_OK) return s;
+        if(rem > 0) {
+          CK(launch_diag_inv(A, ld, r0 + jj, c0 + jj, jb, ctx->d_dinv_piece, st));
+          CK(launch_laswp_trsm(A, ld, r0 + jj, jb, c0 + jj, nullptr, ctx->d_dinv_piece,
+                               c0 + jj + jb, rem, st));
+          CK(launch_dgemm_sub(n - (r0 + jj + jb), rem, jb, a(r0 + jj + jb, c0 + jj), ld,
+                              a(r0 + jj, c0 + jj + jb), ld, a(r0 + jj + jb, c0 + jj + jb), ld,
+                              st));
+          ctx->launches += 3;
+        }
+        jj += jb;
+        jb = std::min(rem, nbs);
+      } while(rem > 0);
+    } else {
+      do {
+        rem -= jb;
+        const int cj = c0 + jj;
+        if(jj > 0) {
+          CK(launch_diag_inv(A, ld, r0, c0, jj, ctx->d_dinv_piece, st));
+          CK(launch_laswp_trsm(A, ld, r0, jj, c0, nullptr, ctx->d_dinv_piece, cj, jb, st));
+          CK(launch_dgemm_sub(n - (r0 + jj), jb, jj, a(r0 + jj, c0), ld, a(r0, cj), ld,
+                              a(r0 + jj, cj), ld, st));
+          ctx->launches += 3;
+        }
+        if((s = rpanel(r0 + jj, cj, jb, pc, pw)) != HPLB_OK) return s;
+        jj += jb;
+        jb = std::min(rem, nbs);
+      } while(rem > 0);
+    }
+    return HPLB_OK;
+  }
+
+  // Factor panel j on the panel stream and build its row map and diagonal
+  // inverses; records `done` when finished.
+  hplb_status panel(int j, int set, cudaEvent_t done) {
+    hplb_ctx*   ctx = this->ctx;
+    const int   jb  = std::min(algo->nb, n - j);
+    cudaEvent_t e0  = next_event(ctx), e1 = next_event(ctx);
+    CK(cudaEventRecord(e0, ctx->s_pan));
+    hplb_status s = rpanel(j, j, jb, j, jb);
+    if(s != HPLB_OK) return s;
+    CK(launch_perm(ctx->d_ipiv + j, j, jb, ctx->d_perm[set], ctx->s_pan));
+    CK(launch_diag_inv(A, ld, j, j, jb, ctx->d_dinv[set], ctx->s_pan));
+    ctx->launches += 2;
+    CK(cudaEventRecord(e1, ctx->s_pan));
+    CK(cudaEventRecord(done, ctx->s_pan));
+    panel_ev.emplace_back(e0, e1);
+    return HPLB_OK;
+  }
+
+  // Row interchanges + U12 + trailing DGEMM of panel j on columns [c, c+w).
+  hplb_status update(int j, int set, int c, int w) {
+    hplb_ctx* ctx = this->ctx;
+    if(w <= 0) return HPLB_OK;
+    const int jb = std::min(algo->nb, n - j);
+    CK(launch_laswp_trsm(A, ld, j, jb, j, ctx->d_perm[set], ctx->d_dinv[set], c, w, ctx->s_upd));
+    ctx->launches += 1;
+    const int m = n - (j + jb);
+    if(m > 0) {
+      cudaEvent_t e0 = next_event(ctx), e1 = next_event(ctx);
+      CK(cudaEventRecord(e0, ctx->s_upd));
+      CK(launch_dgemm_sub(m, w, jb, a(j + jb, j), ld, a(j, c), ld, a(j + jb, c), ld, ctx->s_upd));
+      CK(cudaEventRecord(e1, ctx->s_upd));
+      ctx->launches += 1;
+      gemm_ev.emplace_back(e0, e1);
+      gemm_flops.push_back(2.0 * m * (double)w * jb);
+    }
+    return HPLB_OK;
+  }
+};
+
+hplb_status read_status(hplb_ctx* ctx, int* info_out) {
+  int st[ST_COUNT];
+  CK(cudaMemcpy(st, ctx->d_status, sizeof st, cudaMemcpyDeviceToHost));
+  if(info_out) *info_out = st[ST_INFO];
+  if(st[ST_TIMEOUT] != 0)
+    return set_err(ctx, HPLB_ERR_TIMEOUT, "a bounded device wait expired (site %d)",
+                   st[ST_TIMEOUT]);
+  return HPLB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* hplb_status_string(hplb_status s) {
+  switch(s) {
+    case HPLB_OK: return "ok";
+    case HPLB_ERR_ARG: return "invalid argument";
+    case HPLB_ERR_OOM: return "out of device memory";
+    case HPLB_ERR_SINGULAR: return "matrix is singular (zero pivot)";
+    case HPLB_ERR_TIMEOUT: return "device wait timed out";
+    case HPLB_ERR_CUDA: return "CUDA error";
+    case HPLB_ERR_UNSUPPORTED: return "unsupported parameter";
+  }
+  return "unknown status";
+}
+
+const char* hplb_last_error(const hplb_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int64_t hplb_default_ld(int n) { return ((int64_t)std::max(1, n) + 95) / 128 * 128 + 32; }
+
+hplb_ctx* hplb_create(int device, hplb_status* status) {
+  auto fail = [&](hplb_status s) -> hplb_ctx* {
+    if(status) *status = s;
+    return nullptr;
+  };
+  int ndev = 0;
+  if(cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+    cudaGetLastError();
+    return fail(ndev == 0 ? HPLB_ERR_CUDA : HPLB_ERR_ARG);
+  }
+  if(cudaSetDevice(device) != cudaSuccess) return fail(HPLB_ERR_CUDA);
+  hplb_ctx* ctx = new hplb_ctx();
+  ctx->device   = device;
+  cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+  int lo = 0, hi = 0;
+  cudaDeviceGetStreamPriorityRange(&lo, &hi);
+  bool ok = cudaStreamCreateWithPriority(&ctx->s_upd, cudaStreamNonBlocking, lo) == cudaSuccess &&
+            cudaStreamCreateWithPriority(&ctx->s_pan, cudaStreamNonBlocking, hi) == cudaSuccess &&
+            cudaMalloc(&ctx->d_status, ST_COUNT * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&ctx->d_bar, 2 * sizeof(int)) == cudaSuccess &&
+            cudaMalloc(&ctx->d_out8, 8 * sizeof(double)) == cudaSuccess;
+  if(!ok) {
+    cudaGetLastError();
+    hplb_destroy(ctx);
+    return fail(HPLB_ERR_CUDA);
+  }
+  cudaMemset(ctx->d_status, 0, ST_COUNT * sizeof(int));
+  cudaMemset(ctx->d_bar, 0, 2 * sizeof(int));
+  if(status) *status = HPLB_OK;
+  return ctx;
+}
+
+void hplb_destroy(hplb_ctx* ctx) {
+  if(!ctx) return;
+  cudaSetDevice(ctx->device);
+  if(ctx->s_upd) cudaStreamSynchronize(ctx->s_upd);
+  if(ctx->s_pan) cudaStreamSynchronize(ctx->s_pan);
+  for(auto e : ctx->events) cudaEventDestroy(e);
+  void* bufs[] = {ctx->d_status, ctx->d_bar,      ctx->d_out8,        ctx->d_ipiv,
+                  ctx->d_perm[0], ctx->d_perm[1], ctx->d_dinv[0],     ctx->d_dinv[1],
+                  ctx->d_dinv_piece, ctx->d_cand, ctx->d_res};
+  for(void* b : bufs)
+    if(b) cudaFree(b);
+  if(ctx->s_upd) cudaStreamDestroy(ctx->s_upd);
+  if(ctx->s_pan) cudaStreamDestroy(ctx->s_pan);
+  delete ctx;
+}
+
+hplb_status hplb_matgen(hplb_ctx* ctx, int m, int n, int nb, uint64_t seed, double* dA,
+                        int64_t ld) {
+  if(!ctx) return HPLB_ERR_ARG;
+  (void)nb;
+  if(m < 0 || n < 0) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen: negative size");
+  if(ld < std::max(1, m)) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen: ld < max(1,m)");
+  if(m > 0 && n > 0 && !dA) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen: null matrix");
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_matgen(m, n, seed, dA, ld, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return HPLB_OK;
+}
+
+hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA, int64_t ld,
+                        double* dX, int* ipiv_out, int* info) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(!algo) return set_err(ctx, HPLB_ERR_ARG, "hplb_pdgesv: null algo");
+  if(n < 0) return set_err(ctx, HPLB_ERR_ARG, "Value of N less than 0");
+  if(algo->nb < 1) return set_err(ctx, HPLB_ERR_ARG, "Value of NB less than 1");
+  if(algo->nbmin < 1) return set_err(ctx, HPLB_ERR_ARG, "Value of NBMIN less than 1");
+  if(algo->ndiv < 2) return set_err(ctx, HPLB_ERR_ARG, "Value of NDIV less than 2");
+  if(algo->pfact < 0 || algo->pfact > 2)
+    return set_err(ctx, HPLB_ERR_ARG, "Value of PFACT out of range");
+  if(algo->rfact < 0 || algo->rfact > 2)
+    return set_err(ctx, HPLB_ERR_ARG, "Value of RFACT out of range");
+  if(algo->depth != 1)
+    return set_err(ctx, HPLB_ERR_UNSUPPORTED, "Only lookahead depth 1 is supported");
+  if(algo->nbmin > kMaxLeaf)
+    return set_err(ctx, HPLB_ERR_UNSUPPORTED, "NBMIN above %d is not supported", kMaxLeaf);
+  if(algo->nb > 2048) return set_err(ctx, HPLB_ERR_UNSUPPORTED, "NB above 2048 is not supported");
+  if(ld < std::max(1, n)) return set_err(ctx, HPLB_ERR_ARG, "hplb_pdgesv: ld < max(1,N)");
+  if(info) *info = 0;
+  ctx->timing = hplb_timing{};
+  if(n == 0) return HPLB_OK;
+  if(!dA || !dX) return set_err(ctx, HPLB_ERR_ARG, "hplb_pdgesv: null matrix or solution");
+  CK(cudaSetDevice(ctx->device));
+  hplb_status s = ensure_solve_ws(ctx, n, algo->nb, algo->nbmin);
+  if(s != HPLB_OK) return s;
+
+  ctx->ev_next  = 0;
+  ctx->launches = 0;
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
+  Solve S{ctx, algo, dA, ld, n, {}, {}, {}};
+  cudaEvent_t ev_start = next_event(ctx), ev_lu = next_event(ctx), ev_end = next_event(ctx);
+  cudaEvent_t ev_panel[2] = {next_event(ctx), next_event(ctx)};
+  CK(cudaEventRecord(ev_start, ctx->s_upd));
+  CK(cudaStreamWaitEvent(ctx->s_pan, ev_start, 0));
+
+  const int nb = algo->nb;
+  if((s = S.panel(0, 0, ev_panel[0])) != HPLB_OK) return s;
+  for(int j = 0; j < n; j += nb) {
+    const int set = (j / nb) & 1;
+    const int jb  = std::min(nb, n - j);
+    CK(cudaStreamWaitEvent(ctx->s_upd, ev_panel[set], 0));
+    const int c1 = j + jb;                              // first trailing column
+    const int la = c1 < n ? std::min(nb, n - c1) : 0;   // look-ahead width
+    if((s = S.update(j, set, c1, la)) != HPLB_OK) return s;
+    if(la > 0) {
+      cudaEvent_t ev_la = next_event(ctx);
+      CK(cudaEventRecord(ev_la, ctx->s_upd));
+      CK(cudaStreamWaitEvent(ctx->s_pan, ev_la, 0));
+      if((s = S.panel(c1, set ^ 1, ev_panel[set ^ 1])) != HPLB_OK) return s;
+    }
+    if((s = S.update(j, set, c1 + la, n + 1 - (c1 + la))) != HPLB_OK) return s;
+  }
+  CK(cudaEventRecord(ev_lu, ctx->s_upd));
+  CK(launch_trsv(dA, ld, n, dX, ctx->d_status, ctx->s_upd, &ctx->launches));
+  if(ipiv_out)
+    CK(cudaMemcpyAsync(ipiv_out, ctx->d_ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice,
+                       ctx->s_upd));
+  CK(cudaEventRecord(ev_end, ctx->s_upd));
+  {
+    cudaError_t e = cudaStreamSynchronize(ctx->s_upd);
+    if(e == cudaSuccess) e = cudaStreamSynchronize(ctx->s_pan);
+    if(e != cudaSuccess)
+      return set_err(ctx, HPLB_ERR_CUDA, "solve failed: %s", cudaGetErrorString(e));
+  }
+  int inf = 0;
+  s       = read_status(ctx, &inf);
+  if(info) *info = inf;
+
+  hplb_timing& T = ctx->timing;
+  float        ms = 0.f;
+  cudaEventElapsedTime(&ms, ev_start, ev_end);
+  T.total_ms = ms;
+  cudaEventElapsedTime(&ms, ev_start, ev_lu);
+  T.lu_ms = ms;
+  cudaEventElapsedTime(&ms, ev_lu, ev_end);
+  T.trsv_ms = ms;
+  for(size_t i = 0; i < S.gemm_ev.size(); ++i) {
+    cudaEventElapsedTime(&ms, S.gemm_ev[i].first, S.gemm_ev[i].second);
+    T.gemm_ms += ms;
+    T.gemm_flops += S.gemm_flops[i];
+  }
+  for(auto& p : S.panel_ev) {
+    cudaEventElapsedTime(&ms, p.first, p.second);
+    T.panel_ms += ms;
+  }
+  T.gemm_launches   = (int)S.gemm_ev.size();
+  T.kernel_launches = ctx->launches;
+  if(s != HPLB_OK) return s;
+  if(inf != 0) return set_err(ctx, HPLB_ERR_SINGULAR, "zero pivot in column %d", inf);
+  return HPLB_OK;
+}
+
+static hplb_status residual_common(hplb_ctx* ctx, int n, const double* dA, int64_t ld, bool lcg,
+                                   uint64_t seed, const double* dX, hplb_resid* out) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(n < 0 || !out) return set_err(ctx, HPLB_ERR_ARG, "hplb_residual: bad argument");
+  if(!lcg && n > 0 && (!dA || ld < n)) return set_err(ctx, HPLB_ERR_ARG, "hplb_residual: bad matrix");
+  if(n > 0 && !dX) return set_err(ctx, HPLB_ERR_ARG, "hplb_residual: null solution");
+  CK(cudaSetDevice(ctx->device));
+  hplb_status s = grow(ctx, &ctx->d_res, &ctx->res_cap, residual_ws_doubles(std::max(n, 1)));
+  if(s != HPLB_OK) return s;
+  CK(launch_residual(n, dA, ld, lcg, seed, dX, ctx->d_res, ctx->d_out8, ctx->s_upd));
+  double o[8];
+  CK(cudaMemcpyAsync(o, ctx->d_out8, sizeof o, cudaMemcpyDeviceToHost, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  out->resid     = o[0];
+  out->rnorm_inf = o[1];
+  out->anorm_1   = o[2];
+  out->anorm_inf = o[3];
+  out->xnorm_1   = o[4];
+  out->xnorm_inf = o[5];
+  out->bnorm_inf = o[6];
+  out->eps       = o[7];
+  return HPLB_OK;
+}
+
+hplb_status hplb_residual(hplb_ctx* ctx, int n, const double* dA, int64_t ld, const double* dX,
+                          hplb_resid* out) {
+  return residual_common(ctx, n, dA, ld, false, 0, dX, out);
+}
+
+hplb_status hplb_residual_lcg(hplb_ctx* ctx, int n, uint64_t seed, const double* dX,
+                              hplb_resid* out) {
+  return residual_common(ctx, n, nullptr, 0, true, seed, dX, out);
+}
+
+hplb_status hplb_last_timing(const hplb_ctx* ctx, hplb_timing* out) {
+  if(!ctx || !out) return HPLB_ERR_ARG;
+  *out = ctx->timing;
+  return HPLB_OK;
+}
+
+hplb_status hplb_dgemm_sub(hplb_ctx* ctx, int m, int n, int k, const double* dA, int64_t lda,
+                           const double* dB, int64_t ldb, double* dC, int64_t ldc) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(m < 0 || n < 0 || k < 0) return set_err(ctx, HPLB_ERR_ARG, "hplb_dgemm_sub: negative size");
+  if(lda < std::max(1, m) || ldb < std::max(1, k) || ldc < std::max(1, m))
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_dgemm_sub: leading dimension too small");
+  CK(cudaSetDevice(ctx->device));
+  CK(launch_dgemm_sub(m, n, k, dA, lda, dB, ldb, dC, ldc, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return HPLB_OK;
+}
+
+hplb_status hplb_laswp_trsm(hplb_ctx* ctx, double* dA, int64_t ld, int ia, int jb, int lc,
+                            const int* ipiv_host, int c0, int n) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(jb < 0 || jb > 2048 || n < 0 || ia < 0 || lc < 0 || c0 < 0)
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_laswp_trsm: bad argument");
+  if(jb == 0 || n == 0) return HPLB_OK;
+  CK(cudaSetDevice(ctx->device));
+  hplb_status s = ensure_solve_ws(ctx, ia + jb, std::max(jb, 1), 1);
+  if(s != HPLB_OK) return s;
+  const int* perm = nullptr;
+  if(ipiv_host) {
+    for(int i = 0; i < jb; ++i)
+      if(ipiv_host[i] < ia + i || ipiv_host[i] >= ld)
+        return set_err(ctx, HPLB_ERR_ARG, "hplb_laswp_trsm: ipiv[%d] = %d out of range", i,
+                       ipiv_host[i]);
+    CK(cudaMemcpyAsync(ctx->d_ipiv, ipiv_host, (size_t)jb * sizeof(int), cudaMemcpyHostToDevice,
+                       ctx->s_upd));
+    CK(launch_perm(ctx->d_ipiv, ia, jb, ctx->d_perm[0], ctx->s_upd));
+    perm = ctx->d_perm[0];
+  }
+  CK(launch_diag_inv(dA, ld, ia, lc, jb, ctx->d_dinv[0], ctx->s_upd));
+  CK(launch_laswp_trsm(dA, ld, ia, jb, lc, perm, ctx->d_dinv[0], c0, n, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return HPLB_OK;
+}
+
+hplb_status hplb_fp64_peak(hplb_ctx* ctx, int iters, double* dmma_tflops, double* dfma_tflops) {
+  if(!ctx || iters < 1 || !dmma_tflops || !dfma_tflops) return HPLB_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(fp64_peak(ctx->num_sms, iters, dmma_tflops, dfma_tflops, ctx->s_upd));
+  return HPLB_OK;
+}
+
+hplb_status hplb_selftest_wait_timeout(hplb_ctx* ctx, uint64_t budget_ns) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(budget_ns > 10000000000ull)
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_selftest_wait_timeout: budget above 10 s");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
+  // d_bar[0] is the flag: zeroed and never set.
+  CK(cudaMemsetAsync(ctx->d_bar, 0, 2 * sizeof(int), ctx->s_upd));
+  CK(launch_wait_selftest(ctx->d_bar, ctx->d_status, budget_ns, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  hplb_status s = read_status(ctx, nullptr);
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return s;
+}
+
+}  // extern "C"

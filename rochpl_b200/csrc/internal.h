@@ -1,0 +1,47 @@
+// Internal launcher interface shared by the .cu files of libhplb200.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hplb {
+
+constexpr int kMaxLeaf = 128;  // widest leaf (NBMIN) the leaf kernel holds
+
+cudaError_t launch_matgen(int m, int n, uint64_t seed, double* A, int64_t ld,
+                          cudaStream_t stream);
+
+cudaError_t launch_dgemm_sub(int m, int n, int k, const double* A, int64_t lda,
+                             const double* B, int64_t ldb, double* C, int64_t ldc,
+                             cudaStream_t stream);
+
+int         leaf_grid_size(int num_sms, int rows);
+cudaError_t launch_leaf(double* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
+                        double* cand, double* cur, int* bar, int* status, int grid,
+                        cudaStream_t stream);
+cudaError_t launch_panel_swap(double* A, int64_t ld, const int* ipiv, int r0, int c0, int w,
+                              int pc, int pw, cudaStream_t stream);
+cudaError_t launch_perm(const int* ipiv, int ia, int jb, int* permU, cudaStream_t stream);
+cudaError_t launch_diag_inv(const double* A, int64_t ld, int r0, int c0, int n, double* inv,
+                            cudaStream_t stream);
+int         trsm_wcol(int jb);
+size_t      trsm_smem_bytes(int jb);
+cudaError_t launch_laswp_trsm(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
+                              const double* dinv, int c0, int n, cudaStream_t stream);
+
+// Back-solve U x = y, y = column n of A, x written to X.
+cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* status,
+                        cudaStream_t stream, int* launches);
+
+// Residual check.  ws must hold residual_ws_doubles(n) doubles.
+size_t      residual_ws_doubles(int n);
+cudaError_t launch_residual(int n, const double* A, int64_t ld, bool lcg, uint64_t seed,
+                            const double* X, double* ws, double* out8, cudaStream_t stream);
+
+// FP64 issue-rate probes (TFLOP/s) and the bounded-wait self test.
+cudaError_t fp64_peak(int num_sms, int iters, double* dmma_tflops, double* dfma_tflops,
+                      cudaStream_t stream);
+cudaError_t launch_wait_selftest(const int* flag, int* status, unsigned long long budget_ns,
+                                 cudaStream_t stream);
+
+}  // namespace hplb

@@ -1,0 +1,486 @@
+// Panel factorisation and row-interchange kernels of the single-process solve.
+//
+//  leaf_kernel      -- right-looking unblocked LU of an M x w leaf with partial
+//                      pivoting, one persistent cooperative grid, pivot search by
+//                      warp shuffles and one bounded grid barrier per column.
+//                      Replaces pdpanrlT<1024> and its per-column host handshake
+//                      (src/pfact/HPL_pdpanrlT_device.cpp:23-320, :455-463;
+//                      src/pfact/HPL_pdmxswp.cpp:96-121): the pivot row travels
+//                      through a device workspace instead of pinned host memory.
+//  panel_swap_kernel-- the leaf's interchanges applied to the other columns of
+//                      the panel (the reference swaps full panel rows inside the
+//                      leaf, :200-214; the result is the same).
+//  perm_kernel      -- ipiv -> permU (src/pgesv/HPL_pipid.cpp,
+//                      src/panel/HPL_pdpanel_swapids.cpp:22-44) on the device.
+//  diag_inv_kernel  -- inverses of the 32 x 32 unit-lower diagonal blocks of L11.
+//  laswp_trsm_kernel-- fused row interchange (HPL_dlaswp00N) + unit-lower TRSM
+//                      (rocblas_dtrsm, src/pgesv/HPL_pdupdateTT.cpp:95-106)
+//                      over a block of columns held in shared memory.
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace hplb {
+
+namespace {
+
+constexpr int kLeafThreads = 256;
+constexpr int kTri         = 32;  // diagonal block size of the blocked TRSM
+
+// (|v|, row) ordering for the pivot search: larger |v| wins, ties go to the
+// lower row; row < 0 marks "no candidate".
+HPLB_DEV bool better(double av, int ar, double bv, int br) {
+  if(br < 0) return ar >= 0;
+  if(ar < 0) return false;
+  const double fa = fabs(av), fb = fabs(bv);
+  if(fa > fb) return true;
+  if(fa < fb) return false;
+  return ar < br;
+}
+
+// Block-wide arg-max; result valid in every thread.
+HPLB_DEV void block_argmax(double& v, int& r, double* s_v, int* s_r) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for(int off = 16; off > 0; off >>= 1) {
+    const double ov = __shfl_down_sync(0xffffffffu, v, off);
+    const int    orow = __shfl_down_sync(0xffffffffu, r, off);
+    if(better(ov, orow, v, r)) {
+      v = ov;
+      r = orow;
+    }
+  }
+  __syncthreads();
+  if(lane == 0) {
+    s_v[warp] = v;
+    s_r[warp] = r;
+  }
+  __syncthreads();
+  if(warp == 0) {
+    const int nw = blockDim.x >> 5;
+    v = lane < nw ? s_v[lane] : 0.0;
+    r = lane < nw ? s_r[lane] : -1;
+#pragma unroll
+    for(int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, v, off);
+      const int    orow = __shfl_down_sync(0xffffffffu, r, off);
+      if(better(ov, orow, v, r)) {
+        v = ov;
+        r = orow;
+      }
+    }
+    if(lane == 0) {
+      s_v[0] = v;
+      s_r[0] = r;
+    }
+  }
+  __syncthreads();
+  v = s_v[0];
+  r = s_r[0];
+  __syncthreads();
+}
+
+struct LeafParams {
+  double* A;
+  int64_t ld;
+  int     r0, end;  // leaf rows [r0, end)
+  int     c0, w;    // leaf columns [c0, c0 + w), w <= kMaxLeaf
+  int     rpb;      // rows owned per block
+  int*    ipiv;     // ipiv[c] = global pivot row of column c
+  double* cand;     // [2][grid][2 + w]  (value, row, leaf row values)
+  double* cur;      // [2][w]            (the diagonal row's leaf values)
+  int*    bar;      // grid barrier words
+  int*    status;
+};
+
+// Publish this block's pivot candidate for leaf column k (its rows >= d) and,
+// when it owns row d, the diagonal row itself.
+HPLB_DEV void leaf_publish(const LeafParams& P, int k, int par, double* s_v, int* s_r) {
+  const int d   = P.r0 + k;
+  const int lo  = P.r0 + blockIdx.x * P.rpb;
+  const int hi  = min(P.end, lo + P.rpb);
+  const int beg = max(lo, d);
+  const double* colk = P.A + (size_t)(P.c0 + k) * P.ld;
+  double v = 0.0;
+  int    r = -1;
+  for(int i = beg + threadIdx.x; i < hi; i += blockDim.x) {
+    const double a = colk[i];
+    if(better(a, i, v, r)) {
+      v = a;
+      r = i;
+    }
+  }
+  block_argmax(v, r, s_v, s_r);
+  double* slot = P.cand + ((size_t)par * gridDim.x + blockIdx.x) * (2 + P.w);
+  if(threadIdx.x == 0) {
+    slot[0] = v;
+    slot[1] = (double)r;
+  }
+  if(r >= 0)
+    for(int c = threadIdx.x; c < P.w; c += blockDim.x)
+      slot[2 + c] = P.A[(size_t)r + (size_t)(P.c0 + c) * P.ld];
+  if(d >= lo && d < hi)
+    for(int c = threadIdx.x; c < P.w; c += blockDim.x)
+      P.cur[par * P.w + c] = P.A[(size_t)d + (size_t)(P.c0 + c) * P.ld];
+}
+
+__global__ void __launch_bounds__(kLeafThreads) leaf_kernel(LeafParams P) {
+  __shared__ double s_v[32];
+  __shared__ int    s_r[32];
+  __shared__ double s_u[kMaxLeaf];    // pivot row (leaf columns)
+  __shared__ double s_cur[kMaxLeaf];  // old diagonal row
+  __shared__ double s_piv;
+  __shared__ int    s_p;
+
+  const int G   = gridDim.x;
+  const int lo  = P.r0 + blockIdx.x * P.rpb;
+  const int hi  = min(P.end, lo + P.rpb);
+  const size_t ld = (size_t)P.ld;
+
+  leaf_publish(P, 0, 0, s_v, s_r);
+  if(!grid_sync(P.bar, G, P.status, 11)) return;
+
+  for(int k = 0; k < P.w; ++k) {
+    const int par = k & 1;
+    const int c   = P.c0 + k;
+    const int d   = P.r0 + k;
+    // Global pivot: warp 0 scans every block's candidate.
+    if(threadIdx.x < 32) {
+      double v = 0.0;
+      int    r = -1, slot = -1;
+      for(int b = threadIdx.x; b < G; b += 32) {
+        const double* sl = P.cand + ((size_t)par * G + b) * (2 + P.w);
+        const double  sv = __ldcg(sl);
+        const int     sr = (int)__ldcg(sl + 1);
+        if(better(sv, sr, v, r)) {
+          v = sv;
+          r = sr;
+          slot = b;
+        }
+      }
+#pragma unroll
+      for(int off = 16; off > 0; off >>= 1) {
+        const double ov = __shfl_down_sync(0xffffffffu, v, off);
+        const int    orow = __shfl_down_sync(0xffffffffu, r, off);
+        const int    os = __shfl_down_sync(0xffffffffu, slot, off);
+        if(better(ov, orow, v, r)) {
+          v = ov;
+          r = orow;
+          slot = os;
+        }
+      }
+      slot = __shfl_sync(0xffffffffu, slot, 0);
+      if(slot < 0) {  // unreachable while the leaf has rows >= d; keeps reads in bounds
+        slot = 0;
+        v    = 0.0;
+        r    = d;
+      }
+      if(threadIdx.x == 0) {
+        s_piv = v;
+        s_p   = r;
+      }
+      const double* sl = P.cand + ((size_t)par * G + slot) * (2 + P.w);
+      for(int cc = threadIdx.x; cc < P.w; cc += 32) {
+        s_u[cc]   = __ldcg(sl + 2 + cc);
+        s_cur[cc] = __ldcg(P.cur + par * P.w + cc);
+      }
+    }
+    __syncthreads();
+    const double piv = s_piv;
+    const int    p   = s_p;
+    if(blockIdx.x == 0 && threadIdx.x == 0) {
+      P.ipiv[c] = p;
+      if(piv == 0.0) record_info(P.status, c + 1);
+    }
+    // Interchange rows d and p over the leaf columns.
+    if(p != d && p >= lo && p < hi)
+      for(int cc = threadIdx.x; cc < P.w; cc += blockDim.x)
+        P.A[(size_t)p + (size_t)(P.c0 + cc) * ld] = s_cur[cc];
+    if(d >= lo && d < hi)
+      for(int cc = threadIdx.x; cc < P.w; cc += blockDim.x)
+        P.A[(size_t)d + (size_t)(P.c0 + cc) * ld] = s_u[cc];
+    __syncthreads();
+    // Scale column c below the diagonal (division, as the reference does at
+    // src/pfact/HPL_pdpanrlT_device.cpp:232) and apply the rank-1 update to the
+    // remaining leaf columns.
+    double* colc = P.A + (size_t)c * ld;
+    for(int i = max(lo, d + 1) + threadIdx.x; i < hi; i += blockDim.x) {
+      const double l = colc[i] / piv;
+      colc[i]        = l;
+      for(int cc = k + 1; cc < P.w; ++cc) {
+        double* a = P.A + (size_t)i + (size_t)(P.c0 + cc) * ld;
+        *a        = *a - l * s_u[cc];
+      }
+    }
+    if(k + 1 == P.w) break;
+    __syncthreads();
+    leaf_publish(P, k + 1, par ^ 1, s_v, s_r);
+    if(!grid_sync(P.bar, G, P.status, 12)) return;
+  }
+}
+
+// Apply the w interchanges of leaf columns [c0, c0+w) to the panel columns
+// outside the leaf, in order.  One thread per column.
+__global__ void panel_swap_kernel(double* A, int64_t ld, const int* ipiv, int r0, int c0,
+                                  int w, int pc, int pw) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if(j >= pw - w) return;
+  const int col = (pc + j < c0) ? pc + j : pc + j + w;
+  double*   a   = A + (size_t)col * ld;
+  for(int k = 0; k < w; ++k) {
+    const int d = r0 + k, p = ipiv[c0 + k];
+    if(p != d) {
+      const double t = a[d];
+      a[d]           = a[p];
+      a[p]           = t;
+    }
+  }
+}
+
+// permU from the panel's jb pivots (global rows), relative to row ia:
+//   permU[x]      = source row landing in row ia + x, x < jb
+//   permU[jb + s] = destination of original top row s when it leaves the top
+//                   block, else -1.
+// Each thread traces one row through the interchange sequence.
+__global__ void perm_kernel(const int* ipiv, int ia, int jb, int* permU) {
+  extern __shared__ int s_piv[];
+  for(int i = threadIdx.x; i < jb; i += blockDim.x) s_piv[i] = ipiv[i] - ia;
+  __syncthreads();
+  for(int x = threadIdx.x; x < jb; x += blockDim.x) {
+    int pos = x;
+    for(int i = jb - 1; i >= 0; --i) {
+      const int p = s_piv[i];
+      pos         = (pos == i) ? p : (pos == p ? i : pos);
+    }
+    permU[x] = pos;
+    pos      = x;
+    for(int i = 0; i < jb; ++i) {
+      const int p = s_piv[i];
+      pos         = (pos == i) ? p : (pos == p ? i : pos);
+    }
+    permU[jb + x] = pos >= jb ? pos : -1;
+  }
+}
+
+// Inverses of the unit-lower kTri x kTri diagonal blocks of L (n x n at
+// (r0, c0)); block b's inverse goes to inv[b * kTri * kTri], column-major.
+// A partial last block is padded with the identity.
+__global__ void diag_inv_kernel(const double* A, int64_t ld, int r0, int c0, int n,
+                                double* inv) {
+  __shared__ double L[kTri][kTri + 1];
+  const int b = blockIdx.x, lane = threadIdx.x;
+  const int base = b * kTri;
+  for(int c = 0; c < kTri; ++c) {
+    const bool in = (base + lane < n) && (base + c < n);
+    L[lane][c] = in ? A[(size_t)(r0 + base + lane) + (size_t)(c0 + base + c) * ld] : 0.0;
+  }
+  __syncwarp();
+  // Column `lane` of L^-1: forward substitution with the unit diagonal.
+  double x[kTri];
+#pragma unroll
+  for(int i = 0; i < kTri; ++i) {
+    double s = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+    for(int k = 0; k < i; ++k) s -= L[i][k] * x[k];
+    x[i] = (i < lane) ? 0.0 : s;
+  }
+  double* out = inv + (size_t)b * kTri * kTri + (size_t)lane * kTri;
+#pragma unroll
+  for(int i = 0; i < kTri; ++i) out[i] = x[i];
+}
+
+// Fused interchange + TRSM over WCOL columns per CTA.
+//   X = rows [ia, ia+jb) of columns [c0 + blockIdx.x*WCOL, ...).
+//   permU (optional): apply the panel's interchanges first (dlaswp00N
+//   semantics: gather the new top rows, send displaced top rows down).
+//   Then X := L^-1 X with L the unit-lower jb x jb block at (ia, lc), blocked
+//   by kTri rows: X_b = Dinv_b (X_b - L(b, 0:b) X(0:b)).
+template <int WCOL>
+__global__ void __launch_bounds__(256)
+laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
+                  const double* dinv, int c0, int n) {
+  extern __shared__ double sx[];  // [WCOL][jb + 1] column-major, padded
+  const int ldx = jb + 1;
+  const int cb  = c0 + blockIdx.x * WCOL;
+  const int nc  = min(WCOL, c0 + n - cb);
+  const size_t lds = (size_t)ld;
+
+  // Load the top block; with permU, gather the new top rows first (the old
+  // top rows are still intact in global memory), then send displaced top
+  // rows down.  The gathers from rows >= jb read exactly the positions the
+  // displaced rows are written to, hence the barrier between the two.
+  for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
+    const int c = idx / jb, x = idx % jb;
+    const int src = permU ? permU[x] : x;
+    sx[(size_t)c * ldx + x] = A[(size_t)(ia + src) + (size_t)(cb + c) * lds];
+  }
+  __syncthreads();
+  if(permU) {
+    for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
+      const int c = idx / jb, s = idx % jb;
+      const int dst = permU[jb + s];
+      if(dst >= 0)
+        A[(size_t)(ia + dst) + (size_t)(cb + c) * lds] = A[(size_t)(ia + s) + (size_t)(cb + c) * lds];
+    }
+  }
+  __syncthreads();
+
+  // Blocked forward substitution.  Thread layout: row r = tid % 32 of the
+  // current 32-row block, column group cg = tid / 32 handles WCOL/8 columns.
+  constexpr int CPT = WCOL / 8;
+  const int r  = threadIdx.x & 31;
+  const int cg = threadIdx.x >> 5;
+  const int nblk = (jb + kTri - 1) / kTri;
+  for(int b = 0; b < nblk; ++b) {
+    const int row0 = b * kTri;
+    double acc[CPT];
+#pragma unroll
+    for(int q = 0; q < CPT; ++q) acc[q] = 0.0;
+    const int gr = row0 + r;
+    if(gr < jb) {
+      const double* Lrow = A + (size_t)(ia + gr) + (size_t)lc * lds;
+      for(int kk = 0; kk < row0; ++kk) {
+        const double l = Lrow[(size_t)kk * lds];
+#pragma unroll
+        for(int q = 0; q < CPT; ++q) acc[q] += l * sx[(size_t)(cg * CPT + q) * ldx + kk];
+      }
+    }
+    // R = X_b - acc, kept in registers; then X_b = Dinv_b R via shared memory.
+    double rv[CPT];
+#pragma unroll
+    for(int q = 0; q < CPT; ++q) {
+      const int c = cg * CPT + q;
+      rv[q] = (gr < jb) ? sx[(size_t)c * ldx + gr] - acc[q] : 0.0;
+    }
+    __syncthreads();
+#pragma unroll
+    for(int q = 0; q < CPT; ++q) {
+      const int c = cg * CPT + q;
+      if(gr < jb) sx[(size_t)c * ldx + gr] = rv[q];
+    }
+    __syncthreads();
+    const double* D = dinv + (size_t)b * kTri * kTri;
+#pragma unroll
+    for(int q = 0; q < CPT; ++q) acc[q] = 0.0;
+    for(int kk = 0; kk < kTri && row0 + kk < jb; ++kk) {
+      const double dv = D[(size_t)kk * kTri + r];
+#pragma unroll
+      for(int q = 0; q < CPT; ++q) acc[q] += dv * sx[(size_t)(cg * CPT + q) * ldx + row0 + kk];
+    }
+    __syncthreads();
+#pragma unroll
+    for(int q = 0; q < CPT; ++q) {
+      const int c = cg * CPT + q;
+      if(gr < jb) sx[(size_t)c * ldx + gr] = acc[q];
+    }
+    __syncthreads();
+  }
+
+  for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
+    const int c = idx / jb, x = idx % jb;
+    A[(size_t)(ia + x) + (size_t)(cb + c) * lds] = sx[(size_t)c * ldx + x];
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Host launchers
+// ---------------------------------------------------------------------------
+
+int leaf_grid_size(int num_sms, int rows) {
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_kernel, kLeafThreads, 0);
+  if(per_sm < 1) per_sm = 1;
+  const int max_grid = num_sms * per_sm;
+  // At least ~256 rows per block so the barrier count is worth the parallelism.
+  int g = (rows + 255) / 256;
+  if(g > max_grid) g = max_grid;
+  if(g < 1) g = 1;
+  return g;
+}
+
+cudaError_t launch_leaf(double* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
+                        double* cand, double* cur, int* bar, int* status, int grid,
+                        cudaStream_t stream) {
+  LeafParams P;
+  P.A = A;
+  P.ld = ld;
+  P.r0 = r0;
+  P.end = end;
+  P.c0 = c0;
+  P.w = w;
+  P.rpb = (end - r0 + grid - 1) / grid;
+  P.ipiv = ipiv;
+  P.cand = cand;
+  P.cur = cur;
+  P.bar = bar;
+  P.status = status;
+  cudaError_t e = cudaMemsetAsync(bar, 0, 2 * sizeof(int), stream);
+  if(e != cudaSuccess) return e;
+  void* args[] = {&P};
+  return cudaLaunchCooperativeKernel((const void*)leaf_kernel, dim3(grid), dim3(kLeafThreads),
+                                     args, 0, stream);
+}
+
+cudaError_t launch_panel_swap(double* A, int64_t ld, const int* ipiv, int r0, int c0, int w,
+                              int pc, int pw, cudaStream_t stream) {
+  const int ncols = pw - w;
+  if(ncols <= 0) return cudaSuccess;
+  panel_swap_kernel<<<(ncols + 127) / 128, 128, 0, stream>>>(A, ld, ipiv, r0, c0, w, pc, pw);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_perm(const int* ipiv, int ia, int jb, int* permU, cudaStream_t stream) {
+  if(jb <= 0) return cudaSuccess;
+  perm_kernel<<<1, 1024, jb * sizeof(int), stream>>>(ipiv, ia, jb, permU);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_diag_inv(const double* A, int64_t ld, int r0, int c0, int n, double* inv,
+                            cudaStream_t stream) {
+  if(n <= 0) return cudaSuccess;
+  diag_inv_kernel<<<(n + kTri - 1) / kTri, kTri, 0, stream>>>(A, ld, r0, c0, n, inv);
+  return cudaGetLastError();
+}
+
+int trsm_wcol(int jb) { return jb <= 512 ? 32 : (jb <= 1024 ? 16 : 8); }
+
+size_t trsm_smem_bytes(int jb) {
+  const int w = trsm_wcol(jb);
+  return (size_t)w * (jb + 1) * 8;
+}
+
+cudaError_t launch_laswp_trsm(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
+                              const double* dinv, int c0, int n, cudaStream_t stream) {
+  if(n <= 0 || jb <= 0) return cudaSuccess;
+  const int    w    = trsm_wcol(jb);
+  const size_t smem = trsm_smem_bytes(jb);
+  const int    grid = (n + w - 1) / w;
+  cudaError_t  e    = cudaSuccess;
+  switch(w) {
+    case 32:
+      e = cudaFuncSetAttribute(laswp_trsm_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+      if(e == cudaSuccess)
+        laswp_trsm_kernel<32><<<grid, 256, smem, stream>>>(A, ld, ia, jb, lc, permU, dinv, c0, n);
+      break;
+    case 16:
+      e = cudaFuncSetAttribute(laswp_trsm_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+      if(e == cudaSuccess)
+        laswp_trsm_kernel<16><<<grid, 256, smem, stream>>>(A, ld, ia, jb, lc, permU, dinv, c0, n);
+      break;
+    default:
+      e = cudaFuncSetAttribute(laswp_trsm_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem);
+      if(e == cudaSuccess)
+        laswp_trsm_kernel<8><<<grid, 256, smem, stream>>>(A, ld, ia, jb, lc, permU, dinv, c0, n);
+      break;
+  }
+  if(e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+}  // namespace hplb

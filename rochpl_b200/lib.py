@@ -1,0 +1,173 @@
+"""ctypes binding of libhplb200.so (include/hplb.h).
+
+Every entry point declared in the header is bound here with its exact C
+signature; device buffers are passed as raw integer addresses (for example a
+torch CUDA tensor's data_ptr()).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libhplb200.so")
+
+HPLB_OK = 0
+HPLB_ERR_ARG = 1
+HPLB_ERR_OOM = 2
+HPLB_ERR_SINGULAR = 3
+HPLB_ERR_TIMEOUT = 4
+HPLB_ERR_CUDA = 5
+HPLB_ERR_UNSUPPORTED = 6
+
+# Every symbol include/hplb.h declares (checked by the CPU test suite).
+EXPORTS = [
+    "hplb_create", "hplb_destroy", "hplb_status_string", "hplb_last_error",
+    "hplb_default_ld", "hplb_matgen", "hplb_pdgesv", "hplb_residual",
+    "hplb_residual_lcg", "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm",
+    "hplb_fp64_peak", "hplb_selftest_wait_timeout",
+]
+
+
+class hplb_algo(C.Structure):
+    _fields_ = [("nb", C.c_int), ("nbmin", C.c_int), ("ndiv", C.c_int), ("pfact", C.c_int),
+                ("rfact", C.c_int), ("depth", C.c_int), ("l1notran", C.c_int)]
+
+
+class hplb_resid(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("resid", "rnorm_inf", "anorm_1", "anorm_inf",
+                                          "xnorm_1", "xnorm_inf", "bnorm_inf", "eps")]
+
+
+class hplb_timing(C.Structure):
+    _fields_ = [("total_ms", C.c_double), ("lu_ms", C.c_double), ("trsv_ms", C.c_double),
+                ("gemm_ms", C.c_double), ("gemm_flops", C.c_double), ("panel_ms", C.c_double),
+                ("gemm_launches", C.c_int), ("kernel_launches", C.c_int)]
+
+
+class HplError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"hplb status {status}: {message}")
+        self.status = status
+
+
+_lib = None
+
+
+def load() -> C.CDLL:
+    """Load libhplb200.so; raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"{LIB_PATH} is missing: build it with `python -m rochpl_b200.build` "
+                          "(there is no CPU fallback)")
+    L = C.CDLL(LIB_PATH)
+    vp, i64, i32, u64 = C.c_void_p, C.c_int64, C.c_int, C.c_uint64
+    L.hplb_create.argtypes = [i32, C.POINTER(C.c_int)]
+    L.hplb_create.restype = vp
+    L.hplb_destroy.argtypes = [vp]
+    L.hplb_destroy.restype = None
+    L.hplb_status_string.argtypes = [i32]
+    L.hplb_status_string.restype = C.c_char_p
+    L.hplb_last_error.argtypes = [vp]
+    L.hplb_last_error.restype = C.c_char_p
+    L.hplb_default_ld.argtypes = [i32]
+    L.hplb_default_ld.restype = i64
+    L.hplb_matgen.argtypes = [vp, i32, i32, i32, u64, vp, i64]
+    L.hplb_pdgesv.argtypes = [vp, C.POINTER(hplb_algo), i32, vp, i64, vp, vp, C.POINTER(C.c_int)]
+    L.hplb_residual.argtypes = [vp, i32, vp, i64, vp, C.POINTER(hplb_resid)]
+    L.hplb_residual_lcg.argtypes = [vp, i32, u64, vp, C.POINTER(hplb_resid)]
+    L.hplb_last_timing.argtypes = [vp, C.POINTER(hplb_timing)]
+    L.hplb_dgemm_sub.argtypes = [vp, i32, i32, i32, vp, i64, vp, i64, vp, i64]
+    L.hplb_laswp_trsm.argtypes = [vp, vp, i64, i32, i32, i32, vp, i32, i32]
+    L.hplb_fp64_peak.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.hplb_selftest_wait_timeout.argtypes = [vp, u64]
+    for name in ("hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_matgen", "hplb_pdgesv", "hplb_residual", "hplb_residual_lcg",
+                 "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm"):
+        getattr(L, name).restype = i32
+    _lib = L
+    return L
+
+
+class Library:
+    """One hplb context (device, streams, workspaces) on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        st = C.c_int(0)
+        self.ctx = self.L.hplb_create(device, C.byref(st))
+        if not self.ctx:
+            raise HplError(st.value, "hplb_create failed: "
+                           + self.L.hplb_status_string(st.value).decode())
+        self.device = device
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.L.hplb_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, st: int, allow=(HPLB_OK,)) -> int:
+        if st not in allow:
+            raise HplError(st, self.L.hplb_last_error(self.ctx).decode())
+        return st
+
+    def matgen(self, m: int, n: int, seed: int, A: int, ld: int, nb: int = 0):
+        self._check(self.L.hplb_matgen(self.ctx, m, n, nb, seed, A, ld))
+
+    def pdgesv(self, algo: hplb_algo, n: int, A: int, ld: int, X: int, ipiv: int | None = None):
+        info = C.c_int(0)
+        st = self.L.hplb_pdgesv(self.ctx, C.byref(algo), n, A, ld, X, ipiv or None,
+                                C.byref(info))
+        self._check(st, allow=(HPLB_OK, HPLB_ERR_SINGULAR))
+        return info.value
+
+    def residual(self, n: int, A: int, ld: int, X: int) -> dict:
+        r = hplb_resid()
+        self._check(self.L.hplb_residual(self.ctx, n, A, ld, X, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in hplb_resid._fields_}
+
+    def residual_lcg(self, n: int, seed: int, X: int) -> dict:
+        r = hplb_resid()
+        self._check(self.L.hplb_residual_lcg(self.ctx, n, seed, X, C.byref(r)))
+        return {k: getattr(r, k) for k, _ in hplb_resid._fields_}
+
+    def last_timing(self) -> dict:
+        t = hplb_timing()
+        self._check(self.L.hplb_last_timing(self.ctx, C.byref(t)))
+        return {k: getattr(t, k) for k, _ in hplb_timing._fields_}
+
+    def dgemm_sub(self, m, n, k, A, lda, B, ldb, Cp, ldc):
+        self._check(self.L.hplb_dgemm_sub(self.ctx, m, n, k, A, lda, B, ldb, Cp, ldc))
+
+    def laswp_trsm(self, A, ld, ia, jb, lc, ipiv_host, c0, n):
+        arr = None
+        if ipiv_host is not None:
+            arr = (C.c_int * len(ipiv_host))(*[int(v) for v in ipiv_host])
+        self._check(self.L.hplb_laswp_trsm(self.ctx, A, ld, ia, jb, lc, arr, c0, n))
+
+
+    def fp64_peak(self, iters: int = 20000) -> tuple[float, float]:
+        a, b = C.c_double(0), C.c_double(0)
+        self._check(self.L.hplb_fp64_peak(self.ctx, iters, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def selftest_wait_timeout(self, budget_ns: int) -> int:
+        """Returns the status of a bounded wait that is made to expire."""
+        return self.L.hplb_selftest_wait_timeout(self.ctx, budget_ns)
+
+
+_default = {}
+
+
+def library(device: int = 0) -> Library:
+    """Process-wide context per device."""
+    if device not in _default:
+        _default[device] = Library(device)
+    return _default[device]

@@ -1,0 +1,115 @@
+"""Kernel-level parity of the CUDA path against the oracle and against
+rocHPL's own matgen / row-swap code (oracle/_ref), through the C ABI."""
+import numpy as np
+import pytest
+
+from gpu_util import from_dev, to_dev
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("m,n", [(1, 2), (2, 3), (31, 32), (257, 258), (1000, 1001),
+                                 (4096, 4097), (5000, 37), (513, 7)])
+def test_matgen_bit_exact_vs_oracle(hlib, oracle, m, n):
+    import torch
+
+    ld = oracle.default_ld(m)
+    dA = torch.full((ld * n,), np.nan, dtype=torch.float64, device="cuda")
+    hlib.matgen(m, n, 100, dA.data_ptr(), ld)
+    got = from_dev(dA, ld, n)
+    ref = oracle.matgen(m, n, 100, ld=ld)
+    assert np.array_equal(got[:m].view(np.uint64), ref[:m].view(np.uint64))
+    assert np.all(np.isnan(got[m:]))  # padding rows untouched
+
+
+@pytest.mark.parametrize("m,n,nb", [(4096, 4097, 256), (1000, 1001, 64), (33, 34, 32)])
+def test_matgen_bit_exact_vs_reference_kernel(hlib, oracle, m, n, nb):
+    import torch
+
+    R = oracle.ref()
+    if R is None:
+        pytest.skip("oracle/_ref not built")
+    ld = oracle.default_ld(m)
+    d1 = torch.zeros(ld * n, dtype=torch.float64, device="cuda")
+    d2 = torch.zeros(ld * n, dtype=torch.float64, device="cuda")
+    hlib.matgen(m, n, 100, d1.data_ptr(), ld, nb)
+    assert R.ref_pdrandmat(m, n, nb, d2.data_ptr(), ld, 100) == 0
+    assert torch.equal(d1.view(torch.int64), d2.view(torch.int64))
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (7, 5, 3), (128, 128, 16), (200, 300, 512),
+                                   (1000, 513, 512), (4097, 129, 256), (130, 4100, 33)])
+@pytest.mark.parametrize("offset", [0, 1])
+def test_dgemm_sub(hlib, m, n, k, offset):
+    import torch
+
+    g = torch.Generator(device="cpu").manual_seed(m * 7 + n + k)
+    lda = m + 3 + offset
+    A = torch.rand(k * lda + offset, generator=g, dtype=torch.float64) - 0.5
+    B = torch.rand(n * (k + 1) + offset, generator=g, dtype=torch.float64) - 0.5
+    Cm = torch.rand(n * lda + offset, generator=g, dtype=torch.float64) - 0.5
+    dA, dB, dC = A.cuda(), B.cuda(), Cm.cuda()
+    ldb = k + 1
+    hlib.dgemm_sub(m, n, k, dA.data_ptr() + 8 * offset, lda, dB.data_ptr() + 8 * offset, ldb,
+                   dC.data_ptr() + 8 * offset, lda)
+    Am = A[offset:offset + k * lda].view(k, lda).T[:m]
+    Bm = B[offset:offset + n * ldb].view(n, ldb).T[:k]
+    Cr = Cm[offset:offset + n * lda].view(n, lda).T.clone()
+    Cr[:m] -= Am @ Bm
+    got = dC.cpu()[offset:offset + n * lda].view(n, lda).T
+    err = (got - Cr).abs().max().item()
+    assert err <= 1e-14 * k + 1e-15
+    # padding rows of C untouched
+    assert torch.equal(got[m:], Cm[offset:offset + n * lda].view(n, lda).T[m:])
+
+
+@pytest.mark.parametrize("jb,n,rows", [(1, 3, 10), (32, 40, 200), (256, 257, 600),
+                                       (512, 100, 2000), (300, 65, 900)])
+def test_laswp_trsm_vs_oracle(hlib, oracle, jb, n, rows):
+    """Row interchanges + unit-lower TRSM on a block of trailing columns."""
+    rng = np.random.default_rng(jb + n)
+    ld = rows + 5
+    ia = 3
+    ncols = ia + jb + n
+    A = np.asfortranarray(rng.uniform(-0.5, 0.5, (ld, ncols)))
+    # A well-conditioned unit-lower L11 at (ia, ia): small multipliers.
+    A[ia:ia + jb, ia:ia + jb] *= 0.02
+    ipiv = np.array([ia + i + int(rng.integers(0, rows - ia - i)) for i in range(jb)], np.int32)
+    dA = to_dev(A)
+    hlib.laswp_trsm(dA.data_ptr(), ld, ia, jb, ia, ipiv, ia + jb, n)
+    got = from_dev(dA, ld, ncols)
+    ref = A.copy(order="F")
+    cols = slice(ia + jb, ia + jb + n)
+    for i in range(jb):
+        p = ipiv[i]
+        ref[[ia + i, p], cols] = ref[[p, ia + i], cols]
+    L = np.tril(ref[ia:ia + jb, ia:ia + jb], -1) + np.eye(jb)
+    ref[ia:ia + jb, cols] = np.linalg.solve(L, ref[ia:ia + jb, cols])
+    assert np.allclose(got[:, cols], ref[:, cols], rtol=0, atol=1e-12)
+    # columns outside the block untouched
+    assert np.array_equal(got[:, :ia + jb], A[:, :ia + jb])
+
+
+def test_row_swap_matches_reference_dlaswp00N(hlib, oracle):
+    """The swap half of laswp_trsm against rocHPL's own HPL_dlaswp00N, with an
+    identity L11 so the TRSM leaves the rows as they are."""
+    import torch
+
+    R = oracle.ref()
+    if R is None:
+        pytest.skip("oracle/_ref not built")
+    rng = np.random.default_rng(5)
+    jb, n, rows = 64, 50, 400
+    ld = rows
+    A = np.asfortranarray(rng.uniform(-0.5, 0.5, (ld, jb + n)))
+    A[:jb, :jb] = np.eye(jb)  # L11 = I below the diagonal
+    ipiv = np.array([i + int(rng.integers(0, rows - i)) for i in range(jb)], np.int32)
+    dA = to_dev(A)
+    hlib.laswp_trsm(dA.data_ptr(), ld, 0, jb, 0, ipiv, jb, n)
+    ours = from_dev(dA, ld, jb + n)[:, jb:]
+    permU = oracle.swapids(0, ipiv)
+    dB = to_dev(np.asfortranarray(A[:, jb:]))
+    dperm = torch.from_numpy(permU).cuda()
+    assert R.ref_dlaswp00N(jb, n, dB.data_ptr(), ld, dperm.data_ptr()) == 0
+    theirs = from_dev(dB, ld, n)
+    assert np.array_equal(ours, theirs)

@@ -1,0 +1,146 @@
+"""End-to-end parity of hplb_pdgesv against the oracle: identical pivot
+vectors, x within tolerance, HPL scaled residual below 16, plus the error and
+bounded-wait paths."""
+import numpy as np
+import pytest
+
+from gpu_util import from_dev, to_dev
+
+pytestmark = pytest.mark.gpu
+
+# x tolerance: ||x - x_oracle||oo / ||x_oracle||oo <= 64 * n * eps * kappa_est, with
+# kappa_est = ||A||oo * ||A^-1||oo estimated from the oracle solve; HPL LCG matrices
+# at these sizes have kappa ~ 1e3..1e5.
+EPS = 2.0 ** -53
+
+
+def solve_both(hlib, oracle, n, nb, nbmin=32, ndiv=2, pfact=2, rfact=2, seed=100):
+    import torch
+
+    from rochpl_b200.hpl import Algo
+
+    ld = oracle.default_ld(n)
+    A0 = oracle.matgen(n, n + 1, seed, ld=ld)
+    dA = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+    hlib.matgen(n, n + 1, seed, dA.data_ptr(), ld, nb)
+    dX = torch.zeros(max(n, 1), dtype=torch.float64, device="cuda")
+    dP = torch.zeros(max(n, 1), dtype=torch.int32, device="cuda")
+    info = hlib.pdgesv(Algo(nb, nbmin, ndiv, pfact, rfact, 1, 0).c(), n, dA.data_ptr(), ld,
+                       dX.data_ptr(), dP.data_ptr())
+    Ao = A0.copy(order="F")
+    xo, po, info_o = oracle.pdgesv(Ao, n, nb, nbmin, ndiv, pfact, rfact)
+    return dict(x=dX.cpu().numpy()[:n], ipiv=dP.cpu().numpy()[:n], info=info, A0=A0, dA=dA,
+                dX=dX, ld=ld, xo=xo, po=po, info_o=info_o, Ao=Ao)
+
+
+CASES = [(1, 1, 1), (2, 1, 1), (31, 8, 4), (100, 32, 8), (257, 64, 16), (257, 256, 32),
+         (1000, 256, 32), (1000, 128, 16), (1031, 96, 32), (2048, 512, 32), (4096, 256, 32)]
+
+
+@pytest.mark.parametrize("n,nb,nbmin", CASES)
+def test_solve_parity(hlib, oracle, n, nb, nbmin):
+    r = solve_both(hlib, oracle, n, nb, nbmin)
+    assert r["info"] == 0 and r["info_o"] == 0
+    div = np.nonzero(r["ipiv"] != r["po"])[0]
+    assert div.size == 0, f"pivot divergence at columns {div[:10]}"
+    xo = r["xo"]
+    kappa = np.linalg.cond(r["A0"][:n, :n], np.inf) if n <= 2048 else 1e5
+    tol = 64 * n * EPS * kappa
+    err = np.max(np.abs(r["x"] - xo)) / np.max(np.abs(xo))
+    assert err <= tol, (err, tol)
+    res = oracle.residual(r["A0"], n, r["x"])
+    assert res["resid"] < 16.0
+
+
+@pytest.mark.parametrize("pfact,rfact", [(0, 0), (1, 1), (2, 0), (0, 2), (1, 2), (2, 1)])
+def test_solve_variants(hlib, oracle, pfact, rfact):
+    r = solve_both(hlib, oracle, 600, 128, 16, 2, pfact, rfact)
+    assert np.array_equal(r["ipiv"], r["po"])
+    assert oracle.residual(r["A0"], 600, r["x"])["resid"] < 16.0
+
+
+@pytest.mark.parametrize("ndiv", [2, 3, 4])
+def test_solve_ndiv(hlib, oracle, ndiv):
+    r = solve_both(hlib, oracle, 700, 192, 16, ndiv)
+    assert np.array_equal(r["ipiv"], r["po"])
+    assert oracle.residual(r["A0"], 700, r["x"])["resid"] < 16.0
+
+
+@pytest.mark.parametrize("n", [1000, 4096])
+def test_device_residual_matches_oracle(hlib, oracle, n):
+    """hplb_residual (stored matrix) and hplb_residual_lcg (regenerated in the
+    kernel) against the oracle's long-double residual of the same x."""
+    import torch
+
+    r = solve_both(hlib, oracle, n, 256, 32)
+    ld = r["ld"]
+    hlib.matgen(n, n + 1, 100, r["dA"].data_ptr(), ld)
+    d1 = hlib.residual(n, r["dA"].data_ptr(), ld, r["dX"].data_ptr())
+    d2 = hlib.residual_lcg(n, 100, r["dX"].data_ptr())
+    o = oracle.residual(r["A0"], n, r["x"])
+    for d in (d1, d2):
+        for k in ("anorm_1", "anorm_inf", "xnorm_1", "xnorm_inf", "bnorm_inf"):
+            assert d[k] == pytest.approx(o[k], rel=1e-12), k
+        # ||r|| is itself a rounding-level quantity: agree to within the
+        # rounding of the sum (n * eps * ||A||oo ||x||oo).
+        assert abs(d["rnorm_inf"] - o["rnorm_inf"]) <= n * EPS * o["anorm_inf"] * o["xnorm_inf"]
+        assert d["resid"] < 16.0
+    for k in d1:
+        assert d1[k] == d2[k], k  # the two sources are bit-identical
+
+
+def test_factors_match_oracle(hlib, oracle):
+    """The factored matrix (U, panel multipliers, y) against the oracle's."""
+    n = 512
+    r = solve_both(hlib, oracle, n, 128, 32)
+    got = from_dev(r["dA"], r["ld"], n + 1)[:n]
+    ref = r["Ao"][:n]
+    scale = np.max(np.abs(ref))
+    assert np.max(np.abs(got - ref)) / scale < 1e-9
+
+
+def test_zero_pivot_reports_singular(hlib, oracle):
+    import torch
+
+    from rochpl_b200.hpl import Algo
+
+    n = 300
+    ld = oracle.default_ld(n)
+    A = oracle.matgen(n, n + 1, 100, ld=ld)
+    A[:, 77] = 0.0
+    dA = to_dev(A)
+    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+    info = hlib.pdgesv(Algo(64, 16, 2, 2, 2, 1, 0).c(), n, dA.data_ptr(), ld, dX.data_ptr())
+    assert info == 78
+
+
+def test_bad_arguments(hlib):
+    from rochpl_b200.hpl import Algo
+    from rochpl_b200.lib import HPLB_ERR_ARG, HPLB_ERR_UNSUPPORTED, HplError
+
+    with pytest.raises(HplError) as e:
+        hlib.pdgesv(Algo(0, 32, 2, 2, 2, 1, 0).c(), 10, 1, 10, 1)
+    assert e.value.status == HPLB_ERR_ARG
+    with pytest.raises(HplError) as e:
+        hlib.pdgesv(Algo(64, 32, 2, 2, 2, 0, 0).c(), 10, 1, 10, 1)
+    assert e.value.status == HPLB_ERR_UNSUPPORTED
+    with pytest.raises(HplError) as e:
+        hlib.pdgesv(Algo(64, 32, 1, 2, 2, 1, 0).c(), 10, 1, 10, 1)
+    assert e.value.status == HPLB_ERR_ARG
+    with pytest.raises(HplError) as e:
+        hlib.pdgesv(Algo(64, 32, 2, 2, 2, 1, 0).c(), 100, 1, 50, 1)  # ld < n
+    assert e.value.status == HPLB_ERR_ARG
+
+
+def test_bounded_wait_times_out_and_context_survives(hlib, oracle):
+    from rochpl_b200.lib import HPLB_ERR_TIMEOUT
+
+    assert hlib.selftest_wait_timeout(200_000_000) == HPLB_ERR_TIMEOUT  # 0.2 s
+    r = solve_both(hlib, oracle, 200, 64, 16)  # the context still works
+    assert np.array_equal(r["ipiv"], r["po"])
+
+
+def test_repeat_solves_are_bitwise_reproducible(hlib, oracle):
+    a = solve_both(hlib, oracle, 1500, 256, 32)
+    b = solve_both(hlib, oracle, 1500, 256, 32)
+    assert np.array_equal(a["x"].view(np.uint64), b["x"].view(np.uint64))
