@@ -1,0 +1,333 @@
+"""HPL benchmark: FP64 solve throughput on B200 (TFLOP/s, 2/3 N^3 + 2 N^2).
+
+Default workload: N = 131072, NB = 512, NBMIN = 32, NDIV = 2, right-looking
+recursion and leaf, look-ahead depth 1, seed 100 -- the plain FP64 HPL at
+near-full HBM on one B200 (the [A|b] matrix is 137.5 GB, far larger than L2).
+
+A step is one HPL_pdgesv (LU + back-solve), the region rocHPL times
+(src/HPL_pdtest.cpp:132-134); [A|b] is regenerated from the LCG before every
+step, outside the timed region, as rocHPL does before each of its `-it`
+repeats.  Timing is CUDA events on the launching streams, max over ranks.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Multi-GPU runs are replicas (each rank solves its own system; P = Q = 1 has
+no inter-GPU data path), reported as weak scaling.
+
+--impl reference times the reference algorithm's CPU restatement (the oracle,
+host OpenBLAS on every host core) on bounded samples of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "HPL TFLOP/s at N=131072: FP64 LU vs BF16 LU+IR at same residual; % of peak"
+UNIT = "TFLOP/s"
+
+
+def hpl_flops(n: int) -> float:
+    return 2.0 / 3.0 * n ** 3 + 2.0 * n ** 2
+
+
+def dist_env():
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(prefix="hplb_clocks_", suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons, power = [], [], set(), []
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                "sw_power_cap"), f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        os.unlink(self.path)
+        loaded = [s for s, p in zip(sm, power) if p > 200] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(smax) if smax else None, "reasons": sorted(reasons),
+                "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle port with host OpenBLAS
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(n: int, nb: int, steps: int = 1) -> dict:
+    from oracle import oracle as O
+
+    O.lib()
+    have_blas = O.use_blas(os.cpu_count())
+    best = None
+    for _ in range(steps):
+        t0 = time.perf_counter()
+        x, ipiv, info, resid = O.hpl_test(n, nb, 32, 2)
+        t = time.perf_counter() - t0
+        best = t if best is None else min(best, t)
+    return {"value": hpl_flops(n) / best / 1e12, "unit": UNIT, "cores": os.cpu_count(),
+            "kind": "port",
+            "sample": f"N={n} NB={nb} NBMIN=32 NDIV=2 R/R seed 100, generate+LU+back-solve+check "
+                      f"on the host, {'OpenBLAS' if have_blas else 'scalar'} level-3, "
+                      f"{os.cpu_count()} threads; value = (2/3N^3+2N^2)/t",
+            "resid": resid, "seconds": best}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    n_sample = args.cpu_n
+    for _ in range(args.warmup):
+        cpu_baseline(max(1024, n_sample // 4), args.nb)
+    vals = []
+    for _ in range(args.steps):
+        vals.append(cpu_baseline(n_sample, args.nb))
+    v = statistics.median([c["value"] for c in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": statistics.median([c["seconds"] for c in vals]) * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (HPL LCG, seed 100)",
+        "config": {"workload": f"HPL FP64 solve, bounded host sample N={n_sample} of the "
+                               f"N={args.n} NB={args.nb} workload", "n": n_sample, "nb": args.nb,
+                   "parallelism": "host threads"},
+        "cpu_baseline": cb,
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# GPU arm
+# ---------------------------------------------------------------------------
+
+def run_ours(args):
+    import torch
+
+    from rochpl_b200 import library
+    from rochpl_b200.hpl import Algo, default_ld
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800))
+        pg = dist
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if pg is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    lib = library(local)
+    n, nb = args.n, args.nb
+    algo = Algo(nb, 32, 2, 2, 2, 1, 0)
+    ld = default_ld(n)
+    seed = 100 + rank  # each replica its own system
+    dA = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+    dP = torch.zeros(n, dtype=torch.int32, device="cuda")
+
+    dmma_peak, dfma_peak = lib.fp64_peak(20000)
+
+    def step():
+        lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, nb)  # outside the timed region
+        torch.cuda.synchronize()
+        barrier()
+        lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr(), dP.data_ptr())
+        torch.cuda.synchronize()
+        return lib.last_timing()
+
+    for _ in range(args.warmup):
+        step()
+    clocks = ClockSampler(local)
+    clocks.start()
+    timings = [step() for _ in range(args.steps)]
+    clk = clocks.stop()
+    barrier()
+
+    solve_ms = sum(t["total_ms"] for t in timings) / len(timings)
+    solve_ms_max = max_over_ranks(solve_ms)
+    value = world * hpl_flops(n) / (solve_ms_max * 1e-3) / 1e12
+    gemm_ms = sum(t["gemm_ms"] for t in timings)
+    gemm_flops = sum(t["gemm_flops"] for t in timings)
+    gemm_launches = sum(t["gemm_launches"] for t in timings)
+    gemm_tf = gemm_flops / (gemm_ms * 1e-3) / 1e12 if gemm_ms > 0 else 0.0
+    launches = sum(t["kernel_launches"] for t in timings)
+
+    res = lib.residual_lcg(n, seed, dX.data_ptr())
+
+    # End to end through the C ABI with host buffers: [A|b] uploaded from
+    # pinned host memory, solve, x read back -- all inside the timed region.
+    e2e = None
+    if not args.no_e2e:
+        e2e = end_to_end(lib, algo, n, ld, seed, dA, dX, barrier, max_over_ranks, world)
+
+    cb = None
+    if rank == 0 and not args.no_cpu_baseline:
+        cb = cpu_baseline(args.cpu_n, nb)
+
+    if rank == 0:
+        peak = dmma_peak
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": solve_ms_max, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (HPL LCG matrix, seed 100 + rank, entries in (-0.5, 0.5])",
+            "config": {"workload": f"HPL FP64 solve N={n} NB={nb} NBMIN=32 NDIV=2 "
+                                   "PFACT=R RFACT=R depth 1, P=Q=1 per GPU",
+                       "n": n, "nb": nb, "nbmin": 32, "ndiv": 2,
+                       "l2": "inputs larger than L2 ([A|b] is %.1f GB)" % (ld * (n + 1) * 8 / 1e9),
+                       "parallelism": f"replicas x{world}"},
+            "frac_of_fp64_peak": value / world / peak,
+            "resid": res["resid"], "resid_passed": res["resid"] < 16.0,
+            "gflops_reference_formula": world * (2 / 3 * n ** 3 + 1.5 * n ** 2)
+            / (solve_ms_max * 1e-3) / 1e9,
+            "roofline": {"kernel": "dgemm_sub_kernel (trailing-update DMMA DGEMM)",
+                         "bound": "tensor", "achieved": gemm_tf, "peak": peak, "unit": "TFLOP/s",
+                         "frac": gemm_tf / peak, "traffic": args.gemm_traffic,
+                         "peak_source": "FP64 DMMA m16n8k8 issue rate measured live by "
+                                        "hplb_fp64_peak (MEASURED_PEAKS.json has no FP64 figure)",
+                         "gemm_share_of_solve": gemm_ms / sum(t["total_ms"] for t in timings),
+                         "gemm_launches": gemm_launches},
+            "fp64_probe": {"dmma_tflops": dmma_peak, "dfma_tflops": dfma_peak},
+            "clocks": clk,
+            "gpu_launches": launches,
+            "timing_ms": {k: statistics.mean(t[k] for t in timings)
+                          for k in ("total_ms", "lu_ms", "trsv_ms", "gemm_ms", "panel_ms")},
+        }
+        if e2e is not None:
+            line["e2e"] = e2e
+        if cb is not None:
+            line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+def end_to_end(lib, algo, n, ld, seed, dA, dX, barrier, max_over_ranks, world):
+    import torch
+
+    nbytes = ld * (n + 1) * 8
+    try:
+        hA = torch.empty(ld * (n + 1), dtype=torch.float64, pin_memory=True)
+    except RuntimeError:
+        hA = None
+    hX = torch.empty(n, dtype=torch.float64, pin_memory=True)
+    if hA is None:
+        note = "pinned host buffer unavailable: inputs generated from the seed by hplb_matgen"
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, algo.nb)
+        lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr())
+        hX.copy_(dX)
+        torch.cuda.synchronize()
+        t = max_over_ranks(time.perf_counter() - t0)
+        return {"value": world * hpl_flops(n) / t / 1e12, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": n * 8, "note": note}
+    lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, algo.nb)
+    hA.copy_(dA)  # the host copy of [A|b] (same LCG matrix)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    dA.copy_(hA, non_blocking=True)
+    torch.cuda.synchronize()
+    lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr())
+    hX.copy_(dX)
+    torch.cuda.synchronize()
+    t = max_over_ranks(time.perf_counter() - t0)
+    del hA
+    return {"value": world * hpl_flops(n) / t / 1e12, "unit": UNIT,
+            "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": n * 8,
+            "note": "[A|b] from pinned host memory, hplb_pdgesv, x back to the host; wall clock"}
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=1)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--n", type=int, default=131072)
+    ap.add_argument("--nb", type=int, default=512)
+    ap.add_argument("--cpu-n", type=int, default=16384,
+                    help="host sample size for the CPU baseline / reference arm")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gemm-traffic", type=float, default=None,
+                    help="DRAM bytes per DGEMM launch from an ncu capture, if known")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -10,6 +10,9 @@
 // Tile: 128 x 128 per CTA, k-slices of 16, 8 warps each owning 64 x 32.  In HPL
 // k = NB (512 at the benchmark size), so each CTA reads its C tile once and
 // writes it once: 256 KB of C traffic per 16.8 MFLOP.
+#include <cstdlib>
+#include <cstring>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -197,7 +200,23 @@ dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A, int64_t lda,
 
 cudaError_t launch_dgemm_sub(int m, int n, int k, const double* A, int64_t lda,
                              const double* B, int64_t ldb, double* C, int64_t ldc,
-                             cudaStream_t stream) {
+                             int* status, cudaStream_t stream) {
+  if(m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  static const int path = [] {
+    const char* e = getenv("HPLB_DGEMM_PATH");
+    return (e && strcmp(e, "cpasync") == 0) ? 1 : 0;
+  }();
+  if(status && path == 0 && dgemm_tma_eligible(m, n, k, A, lda, B, ldb)) {
+    cudaError_t e = launch_dgemm_tma(m, n, k, A, lda, B, ldb, C, ldc, status, stream);
+    if(e == cudaSuccess) return e;
+    cudaGetLastError();  // fall back to the cp.async kernel
+  }
+  return launch_dgemm_cpasync(m, n, k, A, lda, B, ldb, C, ldc, stream);
+}
+
+cudaError_t launch_dgemm_cpasync(int m, int n, int k, const double* A, int64_t lda,
+                                 const double* B, int64_t ldb, double* C, int64_t ldc,
+                                 cudaStream_t stream) {
   if(m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
   // Paired copies never straddle the logical edge: m and k must be even too.
   const bool vec = ((uintptr_t)A % 16 == 0) && ((uintptr_t)B % 16 == 0) && (lda % 2 == 0) &&

@@ -178,7 +178,7 @@ struct Solve {
                                c0 + jj + jb, rem, st));
           CK(launch_dgemm_sub(n - (r0 + jj + jb), rem, jb, a(r0 + jj + jb, c0 + jj), ld,
                               a(r0 + jj, c0 + jj + jb), ld, a(r0 + jj + jb, c0 + jj + jb), ld,
-                              st));
+                              ctx->d_status, st));
           ctx->launches += 3;
         }
         jj += jb;
@@ -192,7 +192,7 @@ struct Solve {
           CK(launch_diag_inv(A, ld, r0, c0, jj, ctx->d_dinv_piece, st));
           CK(launch_laswp_trsm(A, ld, r0, jj, c0, nullptr, ctx->d_dinv_piece, cj, jb, st));
           CK(launch_dgemm_sub(n - (r0 + jj), jb, jj, a(r0 + jj, c0), ld, a(r0, cj), ld,
-                              a(r0 + jj, cj), ld, st));
+                              a(r0 + jj, cj), ld, ctx->d_status, st));
           ctx->launches += 3;
         }
         if((s = rpanel(r0 + jj, cj, jb, pc, pw)) != HPLB_OK) return s;
@@ -232,7 +232,8 @@ struct Solve {
     if(m > 0) {
       cudaEvent_t e0 = next_event(ctx), e1 = next_event(ctx);
       CK(cudaEventRecord(e0, ctx->s_upd));
-      CK(launch_dgemm_sub(m, w, jb, a(j + jb, j), ld, a(j, c), ld, a(j + jb, c), ld, ctx->s_upd));
+      CK(launch_dgemm_sub(m, w, jb, a(j + jb, j), ld, a(j, c), ld, a(j + jb, c), ld,
+                          ctx->d_status, ctx->s_upd));
       CK(cudaEventRecord(e1, ctx->s_upd));
       ctx->launches += 1;
       gemm_ev.emplace_back(e0, e1);
@@ -473,9 +474,10 @@ hplb_status hplb_dgemm_sub(hplb_ctx* ctx, int m, int n, int k, const double* dA,
   if(lda < std::max(1, m) || ldb < std::max(1, k) || ldc < std::max(1, m))
     return set_err(ctx, HPLB_ERR_ARG, "hplb_dgemm_sub: leading dimension too small");
   CK(cudaSetDevice(ctx->device));
-  CK(launch_dgemm_sub(m, n, k, dA, lda, dB, ldb, dC, ldc, ctx->s_upd));
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
+  CK(launch_dgemm_sub(m, n, k, dA, lda, dB, ldb, dC, ldc, ctx->d_status, ctx->s_upd));
   CK(cudaStreamSynchronize(ctx->s_upd));
-  return HPLB_OK;
+  return read_status(ctx, nullptr);
 }
 
 hplb_status hplb_laswp_trsm(hplb_ctx* ctx, double* dA, int64_t ld, int ia, int jb, int lc,

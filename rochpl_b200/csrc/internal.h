@@ -11,9 +11,20 @@ constexpr int kMaxLeaf = 128;  // widest leaf (NBMIN) the leaf kernel holds
 cudaError_t launch_matgen(int m, int n, uint64_t seed, double* A, int64_t ld,
                           cudaStream_t stream);
 
+// C -= A B.  Uses the TMA-fed warp-specialised kernel when the operands
+// qualify (dgemm_tma_eligible), the cp.async kernel otherwise.  status may be
+// null (then only the cp.async kernel, which has no waits, is used).
 cudaError_t launch_dgemm_sub(int m, int n, int k, const double* A, int64_t lda,
                              const double* B, int64_t ldb, double* C, int64_t ldc,
-                             cudaStream_t stream);
+                             int* status, cudaStream_t stream);
+bool        dgemm_tma_eligible(int m, int n, int k, const double* A, int64_t lda,
+                               const double* B, int64_t ldb);
+cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda,
+                             const double* B, int64_t ldb, double* C, int64_t ldc,
+                             int* status, cudaStream_t stream);
+cudaError_t launch_dgemm_cpasync(int m, int n, int k, const double* A, int64_t lda,
+                                 const double* B, int64_t ldb, double* C, int64_t ldc,
+                                 cudaStream_t stream);
 
 int         leaf_grid_size(int num_sms, int rows);
 cudaError_t launch_leaf(double* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,

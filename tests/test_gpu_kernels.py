@@ -37,19 +37,26 @@ def test_matgen_bit_exact_vs_reference_kernel(hlib, oracle, m, n, nb):
     assert torch.equal(d1.view(torch.int64), d2.view(torch.int64))
 
 
-@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (7, 5, 3), (128, 128, 16), (200, 300, 512),
-                                   (1000, 513, 512), (4097, 129, 256), (130, 4100, 33)])
-@pytest.mark.parametrize("offset", [0, 1])
-def test_dgemm_sub(hlib, m, n, k, offset):
+DGEMM_SHAPES = [(1, 1, 1), (7, 5, 3), (128, 128, 16), (200, 300, 512), (1000, 513, 512),
+                (4097, 129, 256), (130, 4100, 33), (2048, 512, 512), (777, 1031, 64),
+                (129, 129, 17)]
+
+
+@pytest.mark.parametrize("m,n,k", DGEMM_SHAPES)
+@pytest.mark.parametrize("offset,pad", [(0, 16), (0, 3), (1, 3)])
+def test_dgemm_sub(hlib, m, n, k, offset, pad):
+    """offset 0 with an even, padded leading dimension takes the TMA kernel;
+    odd leading dimensions or an 8-byte offset take the cp.async kernel."""
     import torch
 
     g = torch.Generator(device="cpu").manual_seed(m * 7 + n + k)
-    lda = m + 3 + offset
+    lda = m + pad + offset
+    lda += lda % 2 if pad == 16 else 0
     A = torch.rand(k * lda + offset, generator=g, dtype=torch.float64) - 0.5
-    B = torch.rand(n * (k + 1) + offset, generator=g, dtype=torch.float64) - 0.5
+    B = torch.rand(n * (k + 2) + offset, generator=g, dtype=torch.float64) - 0.5
     Cm = torch.rand(n * lda + offset, generator=g, dtype=torch.float64) - 0.5
     dA, dB, dC = A.cuda(), B.cuda(), Cm.cuda()
-    ldb = k + 1
+    ldb = k + (1 if pad != 16 else 2)
     hlib.dgemm_sub(m, n, k, dA.data_ptr() + 8 * offset, lda, dB.data_ptr() + 8 * offset, ldb,
                    dC.data_ptr() + 8 * offset, lda)
     Am = A[offset:offset + k * lda].view(k, lda).T[:m]
