@@ -180,12 +180,28 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
   const int g = lane >> 2, t4 = lane & 3;
   const int wm = (warp & 1) * 64;   // 2 warps along M
   const int wn = (warp >> 1) * 32;  // 4 warps along N
-  // Relabelled reduction index (see the layout note at the top).
-  const int kA0 = (t4 & 1) * 3 + (t4 >> 1) * 12;      // {0, 3, 12, 15}
-  const int kA1 = ((t4 & 1) ? 1 : 2) + (t4 >> 1) * 12;  // {2, 1, 14, 13}
-  const int kB0 = 4 + (t4 & 1) * 3 + (t4 >> 1) * 4;   // {4, 7, 8, 11}
-  const int kB1 = ((t4 & 1) ? 5 : 6) + (t4 >> 1) * 4;   // {6, 5, 10, 9}
+  // Relabelled reduction index (see the layout note at the top): this lane's
+  // k for a0/b0 and for a2/b1, in MMA k-steps 0 and 1.
+  int kk[2][2];
+  kk[0][0] = (t4 & 1) * 3 + (t4 >> 1) * 12;         // {0, 3, 12, 15}
+  kk[0][1] = ((t4 & 1) ? 1 : 2) + (t4 >> 1) * 12;     // {2, 1, 14, 13}
+  kk[1][0] = 4 + (t4 & 1) * 3 + (t4 >> 1) * 4;      // {4, 7, 8, 11}
+  kk[1][1] = ((t4 & 1) ? 5 : 6) + (t4 >> 1) * 4;      // {6, 5, 10, 9}
+  // Swizzled element offsets of this lane's fragments, fixed for the whole
+  // kernel: A rows g / g+8 of the warp's first slab, B column g of its first
+  // n-tile.  Slab i adds i*256 and n-tile j adds j*128 doubles (immediates).
+  int oA[2][2][2], oB[2][2];
+#pragma unroll
+  for(int st = 0; st < 2; ++st)
+#pragma unroll
+    for(int h = 0; h < 2; ++h) {
+      oA[st][h][0] = a_off(wm >> 4, kk[st][h], g);
+      oA[st][h][1] = a_off(wm >> 4, kk[st][h], g + 8);
+      oB[st][h]    = b_off(wn + g, kk[st][h]);
+    }
   int       q  = 0;                 // running k-slice index
+  int       slot = 0;               // q % STAGES
+  uint32_t  phase = 0;              // (q / STAGES) & 1
   for(int t = t_begin; t < t_end; ++t) {
     int tm, tn;
     tile_coords(t, tiles_m, tiles_n, tm, tn);
@@ -206,32 +222,27 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
         for(int r = 0; r < 4; ++r) acc[i][j][r] = 0.0;
 
     for(int kt = 0; kt < KT; ++kt, ++q) {
-      const int s = q % STAGES;
-      if(!mbar_wait(&full[s], (uint32_t)((q / STAGES) & 1), &s_abort)) {
+      if(!mbar_wait(&full[slot], phase, &s_abort)) {
         if(lane == 0) atomicCAS(status + ST_TIMEOUT, 0, 22);
         s_abort = 1;
         return;
       }
-      const double* a = (const double*)(sA + s * A_BYTES);
-      const double* b = (const double*)(sB + s * B_BYTES);
+      const double* a = (const double*)(sA + slot * A_BYTES);
+      const double* b = (const double*)(sB + slot * B_BYTES);
 #pragma unroll
-      for(int step = 0; step < 2; ++step) {
-        const int k0 = step ? kB0 : kA0;  // this lane's k for a0 / b0
-        const int k1 = step ? kB1 : kA1;  // ... and for a2 / b1
+      for(int st = 0; st < 2; ++st) {
         double af[4][4], bf[4][2];
 #pragma unroll
         for(int i = 0; i < 4; ++i) {
-          const int slab = (wm >> 4) + i;
-          af[i][0] = a[a_off(slab, k0, g)];
-          af[i][1] = a[a_off(slab, k0, g + 8)];
-          af[i][2] = a[a_off(slab, k1, g)];
-          af[i][3] = a[a_off(slab, k1, g + 8)];
+          af[i][0] = a[oA[st][0][0] + i * 256];
+          af[i][1] = a[oA[st][0][1] + i * 256];
+          af[i][2] = a[oA[st][1][0] + i * 256];
+          af[i][3] = a[oA[st][1][1] + i * 256];
         }
 #pragma unroll
         for(int j = 0; j < 4; ++j) {
-          const int nn = wn + j * 8 + g;
-          bf[j][0] = b[b_off(nn, k0)];
-          bf[j][1] = b[b_off(nn, k1)];
+          bf[j][0] = b[oB[st][0] + j * 128];
+          bf[j][1] = b[oB[st][1] + j * 128];
         }
 #pragma unroll
         for(int i = 0; i < 4; ++i)
@@ -241,11 +252,15 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
       // The last warp to finish with the slot refills it with slice q + STAGES.
       __syncwarp();
       if(lane == 0) {
-        if(atomicAdd(&s_done[s], 1) == NCONS - 1) {
-          s_done[s] = 0;
+        if(atomicAdd(&s_done[slot], 1) == NCONS - 1) {
+          s_done[slot] = 0;
           if(q + STAGES < nslices)
             issue_slice(q + STAGES, t_begin, KT, tiles_m, tiles_n, &tmA, &tmB, sA, sB, full);
         }
+      }
+      if(++slot == STAGES) {
+        slot = 0;
+        phase ^= 1u;
       }
     }
 
