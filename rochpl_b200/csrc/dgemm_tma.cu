@@ -60,9 +60,6 @@ HPLB_DEV void mbar_expect_tx(uint64_t* b, uint32_t bytes) {
                "r"(bytes)
                : "memory");
 }
-HPLB_DEV void mbar_arrive(uint64_t* b) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(b)) : "memory");
-}
 HPLB_DEV bool mbar_try_wait(uint64_t* b, uint32_t parity) {
   uint32_t ok;
   asm volatile(
