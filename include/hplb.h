@@ -146,6 +146,27 @@ hplb_status hplb_laswp_trsm(hplb_ctx* ctx, double* dA, int64_t ld, int ia, int j
 hplb_status hplb_fp64_peak(hplb_ctx* ctx, int iters, double* dmma_tflops, double* dfma_tflops);
 hplb_status hplb_selftest_wait_timeout(hplb_ctx* ctx, uint64_t budget_ns);
 
+/* Largest n hplb_residual_lcg_noalloc accepts (its static scratch is sized for it). */
+#define HPLB_NOALLOC_MAX_N 16384
+
+/* Allocation-free variant of hplb_residual_lcg.  No counterpart in the
+ * reference: it exists for callers that must not allocate device memory, such
+ * as a program whose device memory is all handed to its own pool allocator, or
+ * a check run between solves where cudaMalloc's implicit synchronisation is not
+ * allowed.  It needs no context and calls no allocating routine; its scratch is
+ * a fixed array in the library's device image (about 2.1 MB, held by every GPU
+ * that loads the library until exit), so n is limited to HPLB_NOALLOC_MAX_N
+ * (larger n returns HPLB_ERR_ARG with a message on stderr).
+ *   dX     : the solution, n doubles in device memory of the current device
+ *   stream : a cudaStream_t (NULL = the default stream); the call waits for it
+ *   out    : host results, as hplb_residual_lcg
+ * The first call on each device looks up the scratch address on that device
+ * (make it with that device current and before any stream capture).  All calls
+ * on a device share the one scratch array: calls that overlap on the GPU (two
+ * host threads, or two streams) race and must be serialised by the caller. */
+hplb_status hplb_residual_lcg_noalloc(int n, uint64_t seed, const double* dX, void* stream,
+                                      hplb_resid* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -246,3 +246,98 @@ cudaError_t launch_residual(int n, const double* A, int64_t ld, bool lcg, uint64
 }
 
 }  // namespace hplb
+
+// ---------------------------------------------------------------------------
+// Allocation-free residual check.
+//
+// For callers that must not allocate device memory at all: a host program that
+// has handed every byte of device memory to its own pool, or a check that runs
+// between solves in a loop where cudaMalloc's implicit device synchronisation is
+// not allowed.  The scratch of the kernels above lives in the file-scope array
+// below instead of a context workspace, so this entry point needs neither a
+// context nor an allocation.  The array is fixed in size (it serves
+// n <= HPLB_NOALLOC_MAX_N) and every GPU that loads the library holds it until
+// the process exits.
+// ---------------------------------------------------------------------------
+
+#include <cstdio>
+#include <mutex>
+
+namespace hplb {
+namespace {
+
+constexpr int    kNoAllocMaxN = HPLB_NOALLOC_MAX_N;
+constexpr size_t kNoAllocWs   = 2 * ((size_t)(kNoAllocMaxN + kChunk - 1) / kChunk) * kNoAllocMaxN +
+                                5 * ((size_t)(kNoAllocMaxN + kRowThreads - 1) / kRowThreads) +
+                                (size_t)(kNoAllocMaxN + 7) / 8 + (sizeof(ResTabs) + 7) / 8 + 16 + 8;
+
+// Shared by every call on a device; it keeps the last call's contents.  No
+// kernel of the check accumulates into it (every partial sum, per-block value
+// and output is overwritten before it is read), so nothing has to be cleared.
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocWs];
+
+constexpr int kMaxDevices = 64;
+std::mutex    g_noalloc_mu;
+double*       g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device (with that device current) and cached.
+cudaError_t noalloc_scratch(int dev, double** out) {
+  std::lock_guard<std::mutex> lk(g_noalloc_mu);
+  if(!g_noalloc_ptr[dev]) {
+    void*       p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if(e != cudaSuccess) return e;
+    g_noalloc_ptr[dev] = (double*)p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace hplb
+
+extern "C" hplb_status hplb_residual_lcg_noalloc(int n, uint64_t seed, const double* dX,
+                                                 void* stream, hplb_resid* out) {
+  using namespace hplb;
+  if(!out || n < 0 || (n > 0 && !dX)) return HPLB_ERR_ARG;
+  if(n > kNoAllocMaxN) {
+    fprintf(stderr,
+            "hplb_residual_lcg_noalloc: n = %d exceeds the static scratch limit "
+            "HPLB_NOALLOC_MAX_N = %d; use hplb_residual_lcg\n",
+            n, kNoAllocMaxN);
+    return HPLB_ERR_ARG;
+  }
+  int dev = 0;
+  if(cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    cudaGetLastError();
+    return HPLB_ERR_CUDA;
+  }
+  double* ws = nullptr;
+  if(noalloc_scratch(dev, &ws) != cudaSuccess) {
+    cudaGetLastError();
+    return HPLB_ERR_CUDA;
+  }
+  cudaStream_t st   = (cudaStream_t)stream;
+  double*      out8 = ws + (kNoAllocWs - 8);
+  if(launch_residual(n, nullptr, 0, true, seed, dX, ws, out8, st) != cudaSuccess) {
+    cudaGetLastError();
+    return HPLB_ERR_CUDA;
+  }
+  double o[8];
+  if(cudaMemcpyAsync(o, out8, sizeof o, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+     cudaStreamSynchronize(st) != cudaSuccess) {
+    cudaGetLastError();
+    return HPLB_ERR_CUDA;
+  }
+  out->resid     = o[0];
+  out->rnorm_inf = o[1];
+  out->anorm_1   = o[2];
+  out->anorm_inf = o[3];
+  out->xnorm_1   = o[4];
+  out->xnorm_inf = o[5];
+  out->bnorm_inf = o[6];
+  out->eps       = o[7];
+  return HPLB_OK;
+}

@@ -25,7 +25,7 @@ EXPORTS = [
     "hplb_create", "hplb_destroy", "hplb_status_string", "hplb_last_error",
     "hplb_default_ld", "hplb_matgen", "hplb_pdgesv", "hplb_residual",
     "hplb_residual_lcg", "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm",
-    "hplb_fp64_peak", "hplb_selftest_wait_timeout",
+    "hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_residual_lcg_noalloc",
 ]
 
 
@@ -83,6 +83,8 @@ def load() -> C.CDLL:
     L.hplb_laswp_trsm.argtypes = [vp, vp, i64, i32, i32, i32, vp, i32, i32]
     L.hplb_fp64_peak.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.hplb_selftest_wait_timeout.argtypes = [vp, u64]
+    L.hplb_residual_lcg_noalloc.argtypes = [i32, u64, vp, vp, C.POINTER(hplb_resid)]
+    L.hplb_residual_lcg_noalloc.restype = i32
     for name in ("hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_matgen", "hplb_pdgesv", "hplb_residual", "hplb_residual_lcg",
                  "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm"):
         getattr(L, name).restype = i32
@@ -161,6 +163,14 @@ class Library:
     def selftest_wait_timeout(self, budget_ns: int) -> int:
         """Returns the status of a bounded wait that is made to expire."""
         return self.L.hplb_selftest_wait_timeout(self.ctx, budget_ns)
+
+
+def residual_lcg_noalloc(n: int, seed: int, X: int, stream: int = 0):
+    """hplb_residual_lcg_noalloc: (status, results dict); needs no context."""
+    L = load()
+    r = hplb_resid()
+    st = L.hplb_residual_lcg_noalloc(n, seed, X, stream or None, C.byref(r))
+    return st, {k: getattr(r, k) for k, _ in hplb_resid._fields_}
 
 
 _default = {}
