@@ -63,7 +63,7 @@ constexpr int MT = WM / 16, NT = WN / 8;
 
 // VEC: 16-byte cp.async (needs 16-byte aligned pointers and even leading
 // dimensions and row offsets; the host checks).
-template <bool VEC>
+template <bool VEC, bool ACCUM>
 __global__ void __launch_bounds__(NTHREADS, 1)
 dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A, int64_t lda,
                  const double* __restrict__ B, int64_t ldb, double* __restrict__ C,
@@ -177,7 +177,7 @@ dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A, int64_t lda,
   }
   cp_async_wait<0>();
 
-  // Epilogue: C -= acc.
+  // Epilogue: C -= acc, or C = acc in the store form.
 #pragma unroll
   for(int i = 0; i < MT; ++i)
 #pragma unroll
@@ -190,7 +190,7 @@ dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A, int64_t lda,
         const int cc = c + (q & 1);
         if(rr < m && cc < n) {
           double* p = C + (size_t)rr + (size_t)cc * ldc;
-          *p = *p - acc[i][j][q];
+          *p = ACCUM ? *p - acc[i][j][q] : acc[i][j][q];
         }
       }
     }
@@ -198,50 +198,65 @@ dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A, int64_t lda,
 
 }  // namespace
 
-cudaError_t launch_dgemm_sub(int m, int n, int k, const double* A, int64_t lda,
-                             const double* B, int64_t ldb, double* C, int64_t ldc,
-                             int* status, cudaStream_t stream) {
-  if(m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+static cudaError_t launch_dgemm_any(int m, int n, int k, const double* A, int64_t lda,
+                                    const double* B, int64_t ldb, double* C, int64_t ldc,
+                                    int* status, bool accumulate, cudaStream_t stream) {
+  if(m <= 0 || n <= 0) return cudaSuccess;
   static const int path = [] {
     const char* e = getenv("HPLB_DGEMM_PATH");
     return (e && strcmp(e, "cpasync") == 0) ? 1 : 0;
   }();
-  if(status && path == 0 && dgemm_tma_eligible(m, n, k, A, lda, B, ldb)) {
-    cudaError_t e = launch_dgemm_tma(m, n, k, A, lda, B, ldb, C, ldc, status, stream);
+  if(k > 0 && status && path == 0 && dgemm_tma_eligible(m, n, k, A, lda, B, ldb)) {
+    cudaError_t e = launch_dgemm_tma(m, n, k, A, lda, B, ldb, C, ldc, status, accumulate, stream);
     if(e == cudaSuccess) return e;
     cudaGetLastError();  // fall back to the cp.async kernel
   }
-  return launch_dgemm_cpasync(m, n, k, A, lda, B, ldb, C, ldc, stream);
+  return launch_dgemm_cpasync(m, n, k, A, lda, B, ldb, C, ldc, accumulate, stream);
+}
+
+cudaError_t launch_dgemm_sub(int m, int n, int k, const double* A, int64_t lda,
+                             const double* B, int64_t ldb, double* C, int64_t ldc,
+                             int* status, cudaStream_t stream) {
+  if(k <= 0) return cudaSuccess;
+  return launch_dgemm_any(m, n, k, A, lda, B, ldb, C, ldc, status, true, stream);
+}
+
+cudaError_t launch_dgemm_set(int m, int n, int k, const double* A, int64_t lda,
+                             const double* B, int64_t ldb, double* C, int64_t ldc,
+                             int* status, cudaStream_t stream) {
+  return launch_dgemm_any(m, n, k, A, lda, B, ldb, C, ldc, status, false, stream);
+}
+
+template <bool VEC, bool ACCUM>
+static cudaError_t launch_cpasync_t(dim3 grid, int m, int n, int k, const double* A,
+                                    int64_t lda, const double* B, int64_t ldb, double* C,
+                                    int64_t ldc, cudaStream_t stream) {
+  static bool attr = false;
+  if(!attr) {
+    cudaError_t e = cudaFuncSetAttribute(dgemm_sub_kernel<VEC, ACCUM>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if(e != cudaSuccess) return e;
+    attr = true;
+  }
+  dgemm_sub_kernel<VEC, ACCUM><<<grid, NTHREADS, SMEM_BYTES, stream>>>(m, n, k, A, lda, B, ldb,
+                                                                       C, ldc);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_dgemm_cpasync(int m, int n, int k, const double* A, int64_t lda,
                                  const double* B, int64_t ldb, double* C, int64_t ldc,
-                                 cudaStream_t stream) {
-  if(m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+                                 bool accumulate, cudaStream_t stream) {
+  if(m <= 0 || n <= 0) return cudaSuccess;
   // Paired copies never straddle the logical edge: m and k must be even too.
   const bool vec = ((uintptr_t)A % 16 == 0) && ((uintptr_t)B % 16 == 0) && (lda % 2 == 0) &&
                    (ldb % 2 == 0) && (m % 2 == 0) && (k % 2 == 0);
-  static bool attr_set[2] = {false, false};
   dim3 grid((m + BM - 1) / BM, (n + BN - 1) / BN);
   if(grid.y > 65535) return cudaErrorInvalidValue;
-  if(vec) {
-    if(!attr_set[1]) {
-      cudaFuncSetAttribute(dgemm_sub_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           SMEM_BYTES);
-      attr_set[1] = true;
-    }
-    dgemm_sub_kernel<true><<<grid, NTHREADS, SMEM_BYTES, stream>>>(m, n, k, A, lda, B, ldb, C,
-                                                                   ldc);
-  } else {
-    if(!attr_set[0]) {
-      cudaFuncSetAttribute(dgemm_sub_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           SMEM_BYTES);
-      attr_set[0] = true;
-    }
-    dgemm_sub_kernel<false><<<grid, NTHREADS, SMEM_BYTES, stream>>>(m, n, k, A, lda, B, ldb, C,
-                                                                    ldc);
-  }
-  return cudaGetLastError();
+  if(vec)
+    return accumulate ? launch_cpasync_t<true, true>(grid, m, n, k, A, lda, B, ldb, C, ldc, stream)
+                      : launch_cpasync_t<true, false>(grid, m, n, k, A, lda, B, ldb, C, ldc, stream);
+  return accumulate ? launch_cpasync_t<false, true>(grid, m, n, k, A, lda, B, ldb, C, ldc, stream)
+                    : launch_cpasync_t<false, false>(grid, m, n, k, A, lda, B, ldb, C, ldc, stream);
 }
 
 }  // namespace hplb

@@ -142,7 +142,7 @@ HPLB_DEV void issue_slice(int q, int t_begin, int KT, int tiles_m, int tiles_n,
   tma_load_2d(sB + s * B_BYTES, tmB, &full[s], kt * BK, tn * BN);
 }
 
-template <int TPC>
+template <int TPC, bool ACCUM>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  int m, int n, int k, double* __restrict__ C, int64_t ldc, int tiles_m,
@@ -206,7 +206,7 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
     // Pull this warp's 64 x 32 block of C into L2 while the tile is computed.
     {
       const int col = n0 + lane;
-      if(col < n)
+      if(ACCUM && col < n)
         for(int r = m0; r < min(m0 + 64, m); r += 16)
           asm volatile("prefetch.global.L2 [%0];" ::"l"(C + (size_t)r + (size_t)col * ldc));
     }
@@ -261,7 +261,8 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
       }
     }
 
-    // Epilogue: C -= acc (C rows/cols outside m x n are never touched).  Two
+    // Epilogue: C -= acc, or C = acc in the store form (C rows/cols outside
+    // m x n are never touched).  Two
     // halves; all loads of a half are issued before its stores, so they are
     // in flight together instead of one dependent round trip per element.
 #pragma unroll
@@ -275,7 +276,8 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
           for(int r = 0; r < 4; ++r) {
             const int row = m0 + (2 * h + i) * 16 + g + (r >> 1) * 8;
             const int col = n0 + j * 8 + 2 * t4 + (r & 1);
-            cv[i][j][r] = (row < m && col < n) ? C[(size_t)row + (size_t)col * ldc] : 0.0;
+            cv[i][j][r] =
+                (ACCUM && row < m && col < n) ? C[(size_t)row + (size_t)col * ldc] : 0.0;
           }
 #pragma unroll
       for(int i = 0; i < 2; ++i)
@@ -286,7 +288,8 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
             const int row = m0 + (2 * h + i) * 16 + g + (r >> 1) * 8;
             const int col = n0 + j * 8 + 2 * t4 + (r & 1);
             if(row < m && col < n)
-              C[(size_t)row + (size_t)col * ldc] = cv[i][j][r] - acc[2 * h + i][j][r];
+              C[(size_t)row + (size_t)col * ldc] =
+                  ACCUM ? cv[i][j][r] - acc[2 * h + i][j][r] : acc[2 * h + i][j][r];
           }
     }
   }
@@ -324,7 +327,7 @@ bool dgemm_tma_eligible(int m, int n, int k, const double* A, int64_t lda, const
 }
 
 cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda, const double* B,
-                             int64_t ldb, double* C, int64_t ldc, int* status,
+                             int64_t ldb, double* C, int64_t ldc, int* status, bool accumulate,
                              cudaStream_t stream) {
   CUtensorMap mA, mB;
   {
@@ -349,8 +352,11 @@ cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda, 
   }
   static bool attr = false;
   if(!attr) {
-    cudaError_t e = cudaFuncSetAttribute(dgemm_tma_kernel<kTpc>,
+    cudaError_t e = cudaFuncSetAttribute(dgemm_tma_kernel<kTpc, true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if(e == cudaSuccess)
+      e = cudaFuncSetAttribute(dgemm_tma_kernel<kTpc, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if(e != cudaSuccess) return e;
     attr = true;
   }
@@ -358,8 +364,12 @@ cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda, 
   const long long ntiles = (long long)tiles_m * tiles_n;
   const long long grid   = (ntiles + kTpc - 1) / kTpc;
   if(grid > 0x7fffffff) return cudaErrorInvalidValue;
-  dgemm_tma_kernel<kTpc><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
-      mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
+  if(accumulate)
+    dgemm_tma_kernel<kTpc, true><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
+        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
+  else
+    dgemm_tma_kernel<kTpc, false><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
+        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
   return cudaGetLastError();
 }
 

@@ -15,6 +15,7 @@
 // kernel turns them into the row map the trailing swap uses (the reference
 // copies pivots to the host and back once per panel, HPL_pdpanel_swapids.cpp).
 #include <algorithm>
+#include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -42,7 +43,10 @@ struct hplb_ctx {
   size_t  ipiv_cap = 0;
   int*    d_perm[2] = {nullptr, nullptr};
   double* d_dinv[2] = {nullptr, nullptr};
+  double* d_linv[2] = {nullptr, nullptr};  // L11^-1 per panel set (nb x nb)
   double* d_dinv_piece = nullptr;
+  double* d_w          = nullptr;  // gathered top rows of the trailing columns (nb x (n+1))
+  size_t  w_cap        = 0;        // doubles
   int     nb_cap       = 0;
   double* d_cand       = nullptr;
   double* d_cur        = nullptr;
@@ -100,6 +104,16 @@ cudaEvent_t next_event(hplb_ctx* ctx) {
   return ctx->events[ctx->ev_next++];
 }
 
+// U12 = L11^-1 (P A12) as a DMMA GEMM (default), or by the blocked
+// substitution kernel (HPLB_TRSM_PATH=substitution, kept for comparison).
+bool trsm_by_inverse() {
+  static const bool inv = [] {
+    const char* e = getenv("HPLB_TRSM_PATH");
+    return !(e && strcmp(e, "substitution") == 0);
+  }();
+  return inv;
+}
+
 hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
   hplb_status s;
   if((s = grow(ctx, &ctx->d_ipiv, &ctx->ipiv_cap, (size_t)std::max(n, 1))) != HPLB_OK) return s;
@@ -107,15 +121,18 @@ hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
     for(int i = 0; i < 2; ++i) {
       if(ctx->d_perm[i]) cudaFree(ctx->d_perm[i]);
       if(ctx->d_dinv[i]) cudaFree(ctx->d_dinv[i]);
+      if(ctx->d_linv[i]) cudaFree(ctx->d_linv[i]);
       ctx->d_perm[i] = nullptr;
       ctx->d_dinv[i] = nullptr;
+      ctx->d_linv[i] = nullptr;
     }
     if(ctx->d_dinv_piece) cudaFree(ctx->d_dinv_piece);
     ctx->d_dinv_piece = nullptr;
     const size_t nblk = (size_t)(nb + 31) / 32 + 1;
     for(int i = 0; i < 2; ++i) {
       if(cudaMalloc(&ctx->d_perm[i], 2 * (size_t)nb * sizeof(int)) != cudaSuccess ||
-         cudaMalloc(&ctx->d_dinv[i], nblk * 32 * 32 * sizeof(double)) != cudaSuccess) {
+         cudaMalloc(&ctx->d_dinv[i], nblk * 32 * 32 * sizeof(double)) != cudaSuccess ||
+         cudaMalloc(&ctx->d_linv[i], (size_t)nb * nb * sizeof(double)) != cudaSuccess) {
         cudaGetLastError();
         return set_err(ctx, HPLB_ERR_OOM, "panel workspace allocation failed");
       }
@@ -126,6 +143,9 @@ hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
     }
     ctx->nb_cap = nb;
   }
+  if(n > 0 && trsm_by_inverse() &&
+     (s = grow(ctx, &ctx->d_w, &ctx->w_cap, (size_t)nb * (size_t)(n + 1))) != HPLB_OK)
+    return s;
   const int    gmax = leaf_grid_size(ctx->num_sms, std::max(n, 1));
   const size_t need = 2 * (size_t)gmax * (2 + std::min(nbmin, kMaxLeaf)) + 2 * kMaxLeaf;
   if((s = grow(ctx, &ctx->d_cand, &ctx->cand_cap, need)) != HPLB_OK) return s;
@@ -215,6 +235,11 @@ struct Solve {
     CK(launch_perm(ctx->d_ipiv + j, j, jb, ctx->d_perm[set], ctx->s_pan));
     CK(launch_diag_inv(A, ld, j, j, jb, ctx->d_dinv[set], ctx->s_pan));
     ctx->launches += 2;
+    if(trsm_by_inverse()) {
+      CK(launch_unit_lower_inverse(a(j, j), ld, jb, ctx->d_dinv[set], ctx->d_linv[set], jb,
+                                   ctx->s_pan));
+      ctx->launches += 2;
+    }
     CK(cudaEventRecord(e1, ctx->s_pan));
     CK(cudaEventRecord(done, ctx->s_pan));
     panel_ev.emplace_back(e0, e1);
@@ -226,8 +251,17 @@ struct Solve {
     hplb_ctx* ctx = this->ctx;
     if(w <= 0) return HPLB_OK;
     const int jb = std::min(algo->nb, n - j);
-    CK(launch_laswp_trsm(A, ld, j, jb, j, ctx->d_perm[set], ctx->d_dinv[set], c, w, ctx->s_upd));
-    ctx->launches += 1;
+    if(trsm_by_inverse()) {
+      // Interchanges into W, then U12 = L11^-1 W straight into the top rows.
+      CK(launch_laswp_gather(A, ld, j, jb, ctx->d_perm[set], ctx->d_w, jb, c, w, ctx->s_upd));
+      CK(launch_dgemm_set(jb, w, jb, ctx->d_linv[set], jb, ctx->d_w, jb, a(j, c), ld,
+                          ctx->d_status, ctx->s_upd));
+      ctx->launches += 2;
+    } else {
+      CK(launch_laswp_trsm(A, ld, j, jb, j, ctx->d_perm[set], ctx->d_dinv[set], c, w,
+                           ctx->s_upd));
+      ctx->launches += 1;
+    }
     const int m = n - (j + jb);
     if(m > 0) {
       cudaEvent_t e0 = next_event(ctx), e1 = next_event(ctx);
@@ -314,7 +348,8 @@ void hplb_destroy(hplb_ctx* ctx) {
   for(auto e : ctx->events) cudaEventDestroy(e);
   void* bufs[] = {ctx->d_status, ctx->d_bar,      ctx->d_out8,        ctx->d_ipiv,
                   ctx->d_perm[0], ctx->d_perm[1], ctx->d_dinv[0],     ctx->d_dinv[1],
-                  ctx->d_dinv_piece, ctx->d_cand, ctx->d_res};
+                  ctx->d_dinv_piece, ctx->d_cand, ctx->d_res, ctx->d_linv[0], ctx->d_linv[1],
+                  ctx->d_w};
   for(void* b : bufs)
     if(b) cudaFree(b);
   if(ctx->s_upd) cudaStreamDestroy(ctx->s_upd);

@@ -17,14 +17,18 @@ cudaError_t launch_matgen(int m, int n, uint64_t seed, double* A, int64_t ld,
 cudaError_t launch_dgemm_sub(int m, int n, int k, const double* A, int64_t lda,
                              const double* B, int64_t ldb, double* C, int64_t ldc,
                              int* status, cudaStream_t stream);
+// C = A B (store form of the same kernels; C is not read).
+cudaError_t launch_dgemm_set(int m, int n, int k, const double* A, int64_t lda,
+                             const double* B, int64_t ldb, double* C, int64_t ldc,
+                             int* status, cudaStream_t stream);
 bool        dgemm_tma_eligible(int m, int n, int k, const double* A, int64_t lda,
                                const double* B, int64_t ldb);
 cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda,
                              const double* B, int64_t ldb, double* C, int64_t ldc,
-                             int* status, cudaStream_t stream);
+                             int* status, bool accumulate, cudaStream_t stream);
 cudaError_t launch_dgemm_cpasync(int m, int n, int k, const double* A, int64_t lda,
                                  const double* B, int64_t ldb, double* C, int64_t ldc,
-                                 cudaStream_t stream);
+                                 bool accumulate, cudaStream_t stream);
 
 int         leaf_grid_size(int num_sms, int rows);
 cudaError_t launch_leaf(double* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
@@ -39,6 +43,14 @@ int         trsm_wcol(int jb);
 size_t      trsm_smem_bytes(int jb);
 cudaError_t launch_laswp_trsm(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
                               const double* dinv, int c0, int n, cudaStream_t stream);
+// Linv (jb x jb, leading dimension ldinv) = L^-1 for the unit-lower L at L
+// (leading dimension ldl), by the blocked substitution applied to the identity.
+cudaError_t launch_unit_lower_inverse(const double* L, int64_t ldl, int jb, const double* dinv,
+                                      double* Linv, int64_t ldinv, cudaStream_t stream);
+// Panel interchanges on columns [c0, c0+n): new top rows gathered into W
+// (jb x n, leading dimension ldw), displaced rows written in place.
+cudaError_t launch_laswp_gather(double* A, int64_t ld, int ia, int jb, const int* permU,
+                                double* W, int64_t ldw, int c0, int n, cudaStream_t stream);
 
 // Back-solve U x = y, y = column n of A, x written to X.
 cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* status,

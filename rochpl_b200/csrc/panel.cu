@@ -298,8 +298,8 @@ __global__ void diag_inv_kernel(const double* A, int64_t ld, int r0, int c0, int
 //   by kTri rows: X_b = Dinv_b (X_b - L(b, 0:b) X(0:b)).
 template <int WCOL>
 __global__ void __launch_bounds__(256)
-laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
-                  const double* dinv, int c0, int n) {
+laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, const double* L, int64_t ldl,
+                  const int* permU, const double* dinv, int c0, int n) {
   extern __shared__ double sx[];  // [WCOL][jb + 1] column-major, padded
   const int ldx = jb + 1;
   const int cb  = c0 + blockIdx.x * WCOL;
@@ -339,9 +339,9 @@ laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, int lc, const int* perm
     for(int q = 0; q < CPT; ++q) acc[q] = 0.0;
     const int gr = row0 + r;
     if(gr < jb) {
-      const double* Lrow = A + (size_t)(ia + gr) + (size_t)lc * lds;
+      const double* Lrow = L + (size_t)gr;
       for(int kk = 0; kk < row0; ++kk) {
-        const double l = Lrow[(size_t)kk * lds];
+        const double l = Lrow[(size_t)kk * (size_t)ldl];
 #pragma unroll
         for(int q = 0; q < CPT; ++q) acc[q] += l * sx[(size_t)(cg * CPT + q) * ldx + kk];
       }
@@ -381,6 +381,38 @@ laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, int lc, const int* perm
     const int c = idx / jb, x = idx % jb;
     A[(size_t)(ia + x) + (size_t)(cb + c) * lds] = sx[(size_t)c * ldx + x];
   }
+}
+
+// Row interchanges of the panel applied to columns [c0, c0+n), with the new
+// top jb rows gathered into W (jb x n, leading dimension ldw) instead of being
+// written back: W then feeds U12 = L11^-1 W as a DMMA GEMM that writes the top
+// rows of A.  Displaced top rows go straight to their new rows below.  Each
+// CTA owns kGatherCols columns; its gathers from rows >= jb read exactly the
+// rows its displaced writes overwrite, hence the barrier between the two.
+constexpr int kGatherCols = 8;
+__global__ void __launch_bounds__(256)
+laswp_gather_kernel(double* A, int64_t ld, int ia, int jb, const int* __restrict__ permU,
+                    double* __restrict__ W, int64_t ldw, int c0, int n) {
+  const int cb = c0 + blockIdx.x * kGatherCols;
+  const int nc = min(kGatherCols, c0 + n - cb);
+  for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
+    const int c = idx / jb, x = idx % jb;
+    W[(size_t)x + (size_t)(cb - c0 + c) * ldw] =
+        A[(size_t)(ia + permU[x]) + (size_t)(cb + c) * ld];
+  }
+  __syncthreads();
+  for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
+    const int c = idx / jb, s = idx % jb;
+    const int dst = permU[jb + s];
+    if(dst >= 0)
+      A[(size_t)(ia + dst) + (size_t)(cb + c) * ld] = A[(size_t)(ia + s) + (size_t)(cb + c) * ld];
+  }
+}
+
+// Writes the jb x jb identity into X (leading dimension ldx).
+__global__ void identity_kernel(double* X, int64_t ldx, int jb) {
+  const int c = blockIdx.x;
+  for(int r = threadIdx.x; r < jb; r += blockDim.x) X[(size_t)r + (size_t)c * ldx] = (r == c);
 }
 
 }  // namespace
@@ -452,8 +484,9 @@ size_t trsm_smem_bytes(int jb) {
   return (size_t)w * (jb + 1) * 8;
 }
 
-cudaError_t launch_laswp_trsm(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
-                              const double* dinv, int c0, int n, cudaStream_t stream) {
+static cudaError_t launch_trsm_any(double* X, int64_t ldx, int ia, int jb, const double* L,
+                                   int64_t ldl, const int* permU, const double* dinv, int c0,
+                                   int n, cudaStream_t stream) {
   if(n <= 0 || jb <= 0) return cudaSuccess;
   const int    w    = trsm_wcol(jb);
   const size_t smem = trsm_smem_bytes(jb);
@@ -464,22 +497,48 @@ cudaError_t launch_laswp_trsm(double* A, int64_t ld, int ia, int jb, int lc, con
       e = cudaFuncSetAttribute(laswp_trsm_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem);
       if(e == cudaSuccess)
-        laswp_trsm_kernel<32><<<grid, 256, smem, stream>>>(A, ld, ia, jb, lc, permU, dinv, c0, n);
+        laswp_trsm_kernel<32><<<grid, 256, smem, stream>>>(X, ldx, ia, jb, L, ldl, permU, dinv,
+                                                           c0, n);
       break;
     case 16:
       e = cudaFuncSetAttribute(laswp_trsm_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem);
       if(e == cudaSuccess)
-        laswp_trsm_kernel<16><<<grid, 256, smem, stream>>>(A, ld, ia, jb, lc, permU, dinv, c0, n);
+        laswp_trsm_kernel<16><<<grid, 256, smem, stream>>>(X, ldx, ia, jb, L, ldl, permU, dinv,
+                                                           c0, n);
       break;
     default:
       e = cudaFuncSetAttribute(laswp_trsm_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem);
       if(e == cudaSuccess)
-        laswp_trsm_kernel<8><<<grid, 256, smem, stream>>>(A, ld, ia, jb, lc, permU, dinv, c0, n);
+        laswp_trsm_kernel<8><<<grid, 256, smem, stream>>>(X, ldx, ia, jb, L, ldl, permU, dinv,
+                                                          c0, n);
       break;
   }
   if(e != cudaSuccess) return e;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_laswp_trsm(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
+                              const double* dinv, int c0, int n, cudaStream_t stream) {
+  return launch_trsm_any(A, ld, ia, jb, A + (size_t)ia + (size_t)lc * ld, ld, permU, dinv, c0, n,
+                         stream);
+}
+
+cudaError_t launch_unit_lower_inverse(const double* L, int64_t ldl, int jb, const double* dinv,
+                                      double* Linv, int64_t ldinv, cudaStream_t stream) {
+  if(jb <= 0) return cudaSuccess;
+  identity_kernel<<<jb, 128, 0, stream>>>(Linv, ldinv, jb);
+  cudaError_t e = cudaGetLastError();
+  if(e != cudaSuccess) return e;
+  return launch_trsm_any(Linv, ldinv, 0, jb, L, ldl, nullptr, dinv, 0, jb, stream);
+}
+
+cudaError_t launch_laswp_gather(double* A, int64_t ld, int ia, int jb, const int* permU,
+                                double* W, int64_t ldw, int c0, int n, cudaStream_t stream) {
+  if(n <= 0 || jb <= 0) return cudaSuccess;
+  laswp_gather_kernel<<<(n + kGatherCols - 1) / kGatherCols, 256, 0, stream>>>(A, ld, ia, jb,
+                                                                              permU, W, ldw, c0, n);
   return cudaGetLastError();
 }
 
