@@ -33,6 +33,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "HPL TFLOP/s at N=131072: FP64 LU vs BF16 LU+IR at same residual; % of peak"
+
+# DRAM bytes per algorithmic flop of the trailing-update DGEMM, from an ncu
+# capture of one 8192 x 8192 x 512 launch (profiles/dgemm_tma_kernel_8192x8192x512.md):
+# (718.5 + 498.3) MB over 68.7 GFLOP.  Its traffic scales with the C-tile count,
+# i.e. with the flops at k = 512, so bench lines scale it to their own launches.
+DGEMM_DRAM_BYTES_PER_FLOP = 1216.8e6 / (2.0 * 8192 * 8192 * 512)
 UNIT = "TFLOP/s"
 
 
@@ -250,7 +256,11 @@ def run_ours(args):
             / (solve_ms_max * 1e-3) / 1e9,
             "roofline": {"kernel": "dgemm_sub_kernel (trailing-update DMMA DGEMM)",
                          "bound": "tensor", "achieved": gemm_tf, "peak": peak, "unit": "TFLOP/s",
-                         "frac": gemm_tf / peak, "traffic": args.gemm_traffic,
+                         "frac": gemm_tf / peak,
+                         "traffic": (args.gemm_traffic if args.gemm_traffic is not None else
+                                     DGEMM_DRAM_BYTES_PER_FLOP * gemm_flops / max(gemm_launches, 1)),
+                         "traffic_note": "DRAM bytes per DGEMM launch, from the ncu capture in "
+                                         "profiles/ scaled by each launch's flops",
                          "peak_source": "FP64 DMMA m16n8k8 issue rate measured live by "
                                         "hplb_fp64_peak (MEASURED_PEAKS.json has no FP64 figure)",
                          "gemm_share_of_solve": gemm_ms / sum(t["total_ms"] for t in timings),
@@ -271,16 +281,43 @@ def run_ours(args):
     return 0
 
 
+def _cudart():
+    """The CUDA runtime torch has already loaded (for exact-size pinned memory:
+    torch's pinned allocator rounds a 137.5 GB request up to 256 GB)."""
+    import ctypes
+
+    for name in ("libcudart.so.12", "libcudart.so"):
+        try:
+            return ctypes.CDLL(name)
+        except OSError:
+            continue
+    return None
+
+
+def _mem_available() -> int:
+    try:
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemAvailable:"):
+                return int(line.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
 def end_to_end(lib, algo, n, ld, seed, dA, dX, barrier, max_over_ranks, world):
+    """[A|b] uploaded from pinned host memory, hplb_pdgesv, x read back to the
+    host, all inside a wall-clock timed region through the C ABI."""
+    import ctypes
+
     import torch
 
     nbytes = ld * (n + 1) * 8
-    try:
-        hA = torch.empty(ld * (n + 1), dtype=torch.float64, pin_memory=True)
-    except RuntimeError:
-        hA = None
+    rt = _cudart()
+    hptr = ctypes.c_void_p()
+    ok = (rt is not None and _mem_available() > nbytes + (24 << 30) and
+          rt.cudaHostAlloc(ctypes.byref(hptr), ctypes.c_size_t(nbytes), 0) == 0)
     hX = torch.empty(n, dtype=torch.float64, pin_memory=True)
-    if hA is None:
+    if not ok:
         note = "pinned host buffer unavailable: inputs generated from the seed by hplb_matgen"
         torch.cuda.synchronize()
         barrier()
@@ -292,21 +329,31 @@ def end_to_end(lib, algo, n, ld, seed, dA, dX, barrier, max_over_ranks, world):
         t = max_over_ranks(time.perf_counter() - t0)
         return {"value": world * hpl_flops(n) / t / 1e12, "unit": UNIT, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": n * 8, "note": note}
-    lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, algo.nb)
-    hA.copy_(dA)  # the host copy of [A|b] (same LCG matrix)
-    torch.cuda.synchronize()
-    barrier()
-    t0 = time.perf_counter()
-    dA.copy_(hA, non_blocking=True)
-    torch.cuda.synchronize()
-    lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr())
-    hX.copy_(dX)
-    torch.cuda.synchronize()
-    t = max_over_ranks(time.perf_counter() - t0)
-    del hA
+    H2D, D2H = 1, 2
+    try:
+        lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, algo.nb)
+        torch.cuda.synchronize()
+        # The host copy of [A|b] (the same LCG matrix), made before timing.
+        assert rt.cudaMemcpy(hptr, ctypes.c_void_p(dA.data_ptr()), ctypes.c_size_t(nbytes),
+                             D2H) == 0
+        dA.zero_()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        assert rt.cudaMemcpy(ctypes.c_void_p(dA.data_ptr()), hptr, ctypes.c_size_t(nbytes),
+                             H2D) == 0
+        t_h2d = time.perf_counter() - t0
+        lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr())
+        hX.copy_(dX)
+        torch.cuda.synchronize()
+        t = max_over_ranks(time.perf_counter() - t0)
+    finally:
+        rt.cudaFreeHost(hptr)
     return {"value": world * hpl_flops(n) / t / 1e12, "unit": UNIT,
             "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": n * 8,
-            "note": "[A|b] from pinned host memory, hplb_pdgesv, x back to the host; wall clock"}
+            "h2d_s": t_h2d, "seconds": t,
+            "note": "[A|b] from pinned host memory (cudaMemcpy), hplb_pdgesv, x back to the "
+                    "host; wall clock"}
 
 
 def main():
