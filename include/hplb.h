@@ -136,6 +136,16 @@ hplb_status hplb_dgemm_sub(hplb_ctx* ctx, int m, int n, int k, const double* dA,
 hplb_status hplb_laswp_trsm(hplb_ctx* ctx, double* dA, int64_t ld, int ia, int jb,
                             int lc, const int* ipiv_host, int c0, int n);
 
+/* Mixed-precision trailing update (tensor cores, tcgen05): C -= sA[i] sB[j]
+ * A16 B16^T on 128 x 256 tiles, FP32 accumulation.  C is m x n FP32
+ * column-major; A16 (m x k) and B16 (n x k) are row-major 16-bit (bf16 != 0:
+ * BF16, else FP16) with leading dimensions that are multiples of 8; sA holds
+ * ceil(m/128) and sB ceil(n/256) FP32 tile scale factors.  The building block of
+ * hplb_pdgesv_mixed; no counterpart in the reference (rocHPL is FP64 only). */
+hplb_status hplb_gemm_lp_sub(hplb_ctx* ctx, int bf16, int m, int n, int k, const void* dA16,
+                             int64_t lda, const void* dB16, int64_t ldb, const float* dsA,
+                             const float* dsB, float* dC, int64_t ldc);
+
 /* Measurement and self-test utilities (no counterpart in the reference).
  *   hplb_fp64_peak          : FP64 tensor-core (DMMA m16n8k8) and FP64 FMA issue
  *                             rates of this GPU in TFLOP/s, the roofline

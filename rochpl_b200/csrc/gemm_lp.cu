@@ -1,0 +1,385 @@
+// Low-precision trailing update of the mixed-precision LU on the 5th-generation
+// tensor cores:   C (fp32) -= sA[tile_m] * sB[tile_n] * (A16 B16^T)
+// with A16 (m x k) and B16 (n x k) BF16 or FP16, both K-major (row-major with
+// k contiguous), and FP32 accumulation in tensor memory.
+//
+// One CTA per SM at a time, 320 threads:
+//   warp 0      TMA producer: k-blocks of 64 (128-byte rows, 128B swizzle) of
+//               A (128 rows) and B (256 rows) into a 4-stage ring.
+//   warp 1      allocates 512 TMEM columns (two 128 x 256 FP32 accumulators)
+//               and one lane issues tcgen05.mma (M=128, N=256, K=16), frees
+//               ring slots and hands finished accumulators over with
+//               tcgen05.commit.
+//   warps 2..9  epilogue: tcgen05.ld of the accumulator rows their TMEM lane
+//               group may read, scale, and C -= in FP32.  Two accumulators let
+//               the epilogue of one tile (HBM-bound: 128 KB read + 128 KB
+//               written) overlap the MMAs of the next.
+// Every mbarrier wait is bounded; on expiry the CTA records the site, the
+// roles leave their loops, TMEM is released and the CTA exits.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "common.cuh"
+#include "internal.h"
+
+namespace hplb {
+
+namespace {
+
+constexpr int LBM = 128, LBN = 256, LBK = 64, LSTAGES = 4;
+constexpr int L_THREADS = 320;
+constexpr int L_EPI_WARPS = 8;
+constexpr int LA_BYTES = LBM * LBK * 2;  // 16 KB
+constexpr int LB_BYTES = LBN * LBK * 2;  // 32 KB
+constexpr int LSTAGE_BYTES = LA_BYTES + LB_BYTES;
+constexpr int L_SMEM = LSTAGES * LSTAGE_BYTES + 1024 + 256;
+constexpr int L_GROUP_N = 8;  // column tiles per group (A and B stay in L2)
+
+HPLB_DEV uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+HPLB_DEV void bar_init(uint64_t* b, int c) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(su32(b)), "r"(c) : "memory");
+}
+HPLB_DEV void bar_expect_tx(uint64_t* b, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(su32(b)),
+               "r"(bytes)
+               : "memory");
+}
+HPLB_DEV void bar_arrive(uint64_t* b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+HPLB_DEV bool bar_try(uint64_t* b, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(su32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+HPLB_DEV bool bar_wait(uint64_t* b, uint32_t parity, volatile int* abort) {
+  if(bar_try(b, parity)) return true;
+  const unsigned long long t0 = globaltimer();
+  while(!bar_try(b, parity)) {
+    if(*abort) return false;
+    if(globaltimer() - t0 > kWaitBudgetNs) return false;
+  }
+  return true;
+}
+HPLB_DEV void tma2d(void* dst, const CUtensorMap* map, uint64_t* bar, int c0, int c1) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%3, %4}], [%2];" ::"r"(su32(dst)),
+      "l"(map), "r"(su32(bar)), "r"(c0), "r"(c1)
+      : "memory");
+}
+
+// Shared-memory matrix descriptor: K-major, 128B swizzle, 8-row atoms of
+// 1024 bytes stacked densely (SBO = 1024 B), descriptor version 1.
+HPLB_DEV uint64_t umma_desc(uint32_t saddr) {
+  uint64_t d = (uint64_t)((saddr >> 4) & 0x3FFFu);
+  d |= (uint64_t)1 << 16;              // leading byte offset (unused for swizzled K-major)
+  d |= (uint64_t)(1024 >> 4) << 32;    // stride byte offset
+  d |= (uint64_t)1 << 46;              // version
+  d |= (uint64_t)2 << 61;              // SWIZZLE_128B
+  return d;
+}
+
+HPLB_DEV void umma_f16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                       uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+HPLB_DEV void umma_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+          su32(bar))
+      : "memory");
+}
+
+HPLB_DEV void tile_of(int t, int tiles_m, int tiles_n, int& tm, int& tn) {
+  const int per = tiles_m * L_GROUP_N;
+  const int grp = t / per;
+  const int r   = t - grp * per;
+  const int gn  = min(L_GROUP_N, tiles_n - grp * L_GROUP_N);
+  tm            = r / gn;
+  tn            = grp * L_GROUP_N + (r - tm * gn);
+}
+
+template <bool BF16>
+__global__ void __launch_bounds__(L_THREADS, 1)
+gemm_lp_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
+               int m, int n, int k, float* __restrict__ C, int64_t ldc,
+               const float* __restrict__ sA, const float* __restrict__ sB, int tiles_m,
+               int tiles_n, int tpc, int* status) {
+  extern __shared__ unsigned char smem_raw[];
+  unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  unsigned char* ringA = base;
+  unsigned char* ringB = base + LSTAGES * LA_BYTES;
+  uint64_t* full  = (uint64_t*)(base + LSTAGES * LSTAGE_BYTES);
+  uint64_t* empty = full + LSTAGES;
+  uint64_t* accf  = empty + LSTAGES;  // accumulator ready (MMA -> epilogue)
+  uint64_t* acce  = accf + 2;         // accumulator drained (epilogue -> MMA)
+  uint64_t* drain = acce + 2;         // every issued MMA finished (abort path)
+  __shared__ uint32_t     s_tmem;
+  __shared__ volatile int s_abort;
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int ntiles  = tiles_m * tiles_n;
+  const int t_begin = blockIdx.x * tpc;
+  const int t_end   = min(ntiles, t_begin + tpc);
+  const int KB      = (k + LBK - 1) / LBK;
+
+  if(threadIdx.x == 0) {
+    for(int s = 0; s < LSTAGES; ++s) {
+      bar_init(&full[s], 1);
+      bar_init(&empty[s], 1);
+    }
+    for(int b = 0; b < 2; ++b) {
+      bar_init(&accf[b], 1);
+      bar_init(&acce[b], L_EPI_WARPS);
+    }
+    bar_init(drain, 1);
+    s_abort = 0;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  }
+  if(warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 512;" ::"r"(
+                     su32(&s_tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tmem = s_tmem;
+
+  if(warp == 0) {
+    // ---------------- TMA producer ----------------
+    if(lane == 0) {
+      int s = 0, issued = 0;
+      uint32_t ph = 0;
+      for(int t = t_begin; t < t_end && !s_abort; ++t) {
+        int tm, tn;
+        tile_of(t, tiles_m, tiles_n, tm, tn);
+        for(int kb = 0; kb < KB; ++kb) {
+          if(!bar_wait(&empty[s], ph ^ 1, &s_abort)) {
+            atomicCAS(status + ST_TIMEOUT, 0, 31);
+            s_abort = 1;
+            break;
+          }
+          bar_expect_tx(&full[s], LSTAGE_BYTES);
+          tma2d(ringA + s * LA_BYTES, &tmA, &full[s], kb * LBK, tm * LBM);
+          tma2d(ringB + s * LB_BYTES, &tmB, &full[s], kb * LBK, tn * LBN);
+          ++issued;
+          if(++s == LSTAGES) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+      }
+      if(s_abort) {
+        // Bounded drain: the last LSTAGES copies are the only ones that can
+        // still be in flight; let them land before the CTA can exit.
+        for(int q = issued > LSTAGES ? issued - LSTAGES : 0; q < issued; ++q) {
+          const unsigned long long t0 = globaltimer();
+          while(!bar_try(&full[q % LSTAGES], (uint32_t)((q / LSTAGES) & 1)) &&
+                globaltimer() - t0 < kWaitBudgetNs) {
+          }
+        }
+      }
+    }
+    __syncwarp();
+  } else if(warp == 1) {
+    // ---------------- MMA issuer ----------------
+    if(lane == 0) {
+      // D = F32 (bits 4-5), A/B = BF16 (1) or F16 (0) (bits 7-12), K-major,
+      // N/8 at bits 17-22, M/16 at bits 24-28.
+      const uint32_t fmt   = BF16 ? 1u : 0u;
+      const uint32_t idesc = (1u << 4) | (fmt << 7) | (fmt << 10) | ((uint32_t)(LBN >> 3) << 17) |
+                             ((uint32_t)(LBM >> 4) << 24);
+      int s = 0;
+      uint32_t ph = 0;
+      int it = 0;
+      for(int t = t_begin; t < t_end && !s_abort; ++t, ++it) {
+        const int      buf = it & 1;
+        const uint32_t d   = tmem + (uint32_t)(buf * LBN);
+        if(!bar_wait(&acce[buf], (uint32_t)(((it >> 1) & 1) ^ 1), &s_abort)) {
+          atomicCAS(status + ST_TIMEOUT, 0, 32);
+          s_abort = 1;
+          break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        bool ok = true;
+        for(int kb = 0; kb < KB; ++kb) {
+          if(!bar_wait(&full[s], ph, &s_abort)) {
+            atomicCAS(status + ST_TIMEOUT, 0, 33);
+            s_abort = 1;
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint32_t a0 = su32(ringA + s * LA_BYTES);
+          const uint32_t b0 = su32(ringB + s * LB_BYTES);
+#pragma unroll
+          for(int kk = 0; kk < LBK / 16; ++kk)
+            umma_f16(d, umma_desc(a0 + kk * 32), umma_desc(b0 + kk * 32), idesc,
+                     (kb | kk) != 0 ? 1u : 0u);
+          umma_commit(&empty[s]);  // slot free once these MMAs have read it
+          if(++s == LSTAGES) {
+            s = 0;
+            ph ^= 1;
+          }
+        }
+        if(!ok) break;
+        umma_commit(&accf[buf]);  // accumulator complete
+      }
+      if(s_abort) {
+        // Bounded wait for every MMA this thread issued before TMEM goes away.
+        umma_commit(drain);
+        const unsigned long long t0 = globaltimer();
+        while(!bar_try(drain, 0) && globaltimer() - t0 < kWaitBudgetNs) {
+        }
+      }
+    }
+    __syncwarp();
+  } else {
+    // ---------------- epilogue ----------------
+    const int ew   = warp - 2;              // 0..7
+    const int sub  = warp & 3;              // TMEM lane group this warp may read
+    const int half = ew >> 2;               // column half of the tile
+    int it = 0;
+    for(int t = t_begin; t < t_end; ++t, ++it) {
+      const int buf = it & 1;
+      if(!bar_wait(&accf[buf], (uint32_t)((it >> 1) & 1), &s_abort)) {
+        if(lane == 0) atomicCAS(status + ST_TIMEOUT, 0, 34);
+        s_abort = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      int tm, tn;
+      tile_of(t, tiles_m, tiles_n, tm, tn);
+      const int   row   = tm * LBM + sub * 32 + lane;
+      const float scale = sA[tm] * sB[tn];
+      for(int c0 = half * (LBN / 2); c0 < (half + 1) * (LBN / 2); c0 += 32) {
+        uint32_t r[32];
+        const uint32_t taddr = tmem + ((uint32_t)(sub * 32) << 16) + (uint32_t)(buf * LBN + c0);
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+            "%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31},"
+            " [%32];"
+            : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+              "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+              "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]),
+              "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+              "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]),
+              "=r"(r[30]), "=r"(r[31])
+            : "r"(taddr));
+        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        if(row < m) {
+          float cv[32];
+          const int col0 = tn * LBN + c0;
+#pragma unroll
+          for(int j = 0; j < 32; ++j)
+            cv[j] = (col0 + j < n) ? C[(size_t)row + (size_t)(col0 + j) * ldc] : 0.f;
+#pragma unroll
+          for(int j = 0; j < 32; ++j)
+            if(col0 + j < n)
+              C[(size_t)row + (size_t)(col0 + j) * ldc] = cv[j] - scale * __uint_as_float(r[j]);
+        }
+      }
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if(lane == 0) bar_arrive(&acce[buf]);
+    }
+  }
+
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if(warp == 1) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 512;" ::"r"(tmem) : "memory");
+  }
+}
+
+PFN_cuTensorMapEncodeTiled_v12000 g_enc = nullptr;
+
+bool lp_encoder() {
+  if(g_enc) return true;
+  cudaDriverEntryPointQueryResult q;
+  void*                           fn = nullptr;
+  if(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) !=
+         cudaSuccess ||
+     q != cudaDriverEntryPointSuccess || !fn) {
+    cudaGetLastError();
+    return false;
+  }
+  g_enc = (PFN_cuTensorMapEncodeTiled_v12000)fn;
+  return true;
+}
+
+}  // namespace
+
+int gemm_lp_tile_m() { return LBM; }
+int gemm_lp_tile_n() { return LBN; }
+
+// A16: m x k, row-major with leading dimension lda (elements, k contiguous);
+// B16: n x k likewise.  sA: tiles_m scale factors, sB: tiles_n.
+cudaError_t launch_gemm_lp(bool bf16, int m, int n, int k, const void* A16, int64_t lda,
+                           const void* B16, int64_t ldb, const float* sA, const float* sB,
+                           float* C, int64_t ldc, int* status, cudaStream_t stream) {
+  if(m <= 0 || n <= 0 || k <= 0) return cudaSuccess;
+  if(!lp_encoder()) return cudaErrorNotSupported;
+  if((uintptr_t)A16 % 16 || (uintptr_t)B16 % 16 || (lda * 2) % 16 || (ldb * 2) % 16)
+    return cudaErrorInvalidValue;
+  const CUtensorMapDataType dt =
+      bf16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16;
+  CUtensorMap mA, mB;
+  {
+    cuuint64_t dims[2]    = {(cuuint64_t)k, (cuuint64_t)m};
+    cuuint64_t strides[1] = {(cuuint64_t)lda * 2};
+    cuuint32_t box[2]     = {LBK, LBM};
+    cuuint32_t es[2]      = {1, 1};
+    if(g_enc(&mA, dt, 2, (void*)A16, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return cudaErrorInvalidValue;
+  }
+  {
+    cuuint64_t dims[2]    = {(cuuint64_t)k, (cuuint64_t)n};
+    cuuint64_t strides[1] = {(cuuint64_t)ldb * 2};
+    cuuint32_t box[2]     = {LBK, LBN};
+    cuuint32_t es[2]      = {1, 1};
+    if(g_enc(&mB, dt, 2, (void*)B16, dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+             CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return cudaErrorInvalidValue;
+  }
+  static bool attr[2] = {false, false};
+  cudaError_t e = cudaSuccess;
+  if(!attr[bf16]) {
+    e = bf16 ? cudaFuncSetAttribute(gemm_lp_kernel<true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM)
+             : cudaFuncSetAttribute(gemm_lp_kernel<false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM);
+    if(e != cudaSuccess) return e;
+    attr[bf16] = true;
+  }
+  const int tiles_m = (m + LBM - 1) / LBM, tiles_n = (n + LBN - 1) / LBN;
+  const long long ntiles = (long long)tiles_m * tiles_n;
+  const int tpc = 8;
+  const long long grid = (ntiles + tpc - 1) / tpc;
+  if(bf16)
+    gemm_lp_kernel<true><<<(unsigned)grid, L_THREADS, L_SMEM, stream>>>(
+        mA, mB, m, n, k, C, ldc, sA, sB, tiles_m, tiles_n, tpc, status);
+  else
+    gemm_lp_kernel<false><<<(unsigned)grid, L_THREADS, L_SMEM, stream>>>(
+        mA, mB, m, n, k, C, ldc, sA, sB, tiles_m, tiles_n, tpc, status);
+  return cudaGetLastError();
+}
+
+}  // namespace hplb

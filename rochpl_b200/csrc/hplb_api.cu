@@ -541,6 +541,21 @@ hplb_status hplb_laswp_trsm(hplb_ctx* ctx, double* dA, int64_t ld, int ia, int j
   return HPLB_OK;
 }
 
+hplb_status hplb_gemm_lp_sub(hplb_ctx* ctx, int bf16, int m, int n, int k, const void* dA16,
+                             int64_t lda, const void* dB16, int64_t ldb, const float* dsA,
+                             const float* dsB, float* dC, int64_t ldc) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(m < 0 || n < 0 || k < 0 || lda < std::max(1, k) || ldb < std::max(1, k) ||
+     ldc < std::max(1, m) || lda % 8 || ldb % 8)
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_gemm_lp_sub: bad sizes or leading dimensions");
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
+  CK(launch_gemm_lp(bf16 != 0, m, n, k, dA16, lda, dB16, ldb, dsA, dsB, dC, ldc, ctx->d_status,
+                    ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return read_status(ctx, nullptr);
+}
+
 hplb_status hplb_fp64_peak(hplb_ctx* ctx, int iters, double* dmma_tflops, double* dfma_tflops) {
   if(!ctx || iters < 1 || !dmma_tflops || !dfma_tflops) return HPLB_ERR_ARG;
   CK(cudaSetDevice(ctx->device));

@@ -67,4 +67,13 @@ cudaError_t fp64_peak(int num_sms, int iters, double* dmma_tflops, double* dfma_
 cudaError_t launch_wait_selftest(const int* flag, int* status, unsigned long long budget_ns,
                                  cudaStream_t stream);
 
+// Mixed-precision trailing update on tcgen05: C (fp32, column-major) -=
+// sA[tile_m] sB[tile_n] A16 B16^T, A16 m x k and B16 n x k row-major 16-bit
+// (BF16 when bf16, else FP16), tiles of gemm_lp_tile_m() x gemm_lp_tile_n().
+int         gemm_lp_tile_m();
+int         gemm_lp_tile_n();
+cudaError_t launch_gemm_lp(bool bf16, int m, int n, int k, const void* A16, int64_t lda,
+                           const void* B16, int64_t ldb, const float* sA, const float* sB,
+                           float* C, int64_t ldc, int* status, cudaStream_t stream);
+
 }  // namespace hplb

@@ -26,6 +26,7 @@ EXPORTS = [
     "hplb_default_ld", "hplb_matgen", "hplb_pdgesv", "hplb_residual",
     "hplb_residual_lcg", "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm",
     "hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_residual_lcg_noalloc",
+    "hplb_gemm_lp_sub",
 ]
 
 
@@ -85,6 +86,8 @@ def load() -> C.CDLL:
     L.hplb_selftest_wait_timeout.argtypes = [vp, u64]
     L.hplb_residual_lcg_noalloc.argtypes = [i32, u64, vp, vp, C.POINTER(hplb_resid)]
     L.hplb_residual_lcg_noalloc.restype = i32
+    L.hplb_gemm_lp_sub.argtypes = [vp, i32, i32, i32, i32, vp, i64, vp, i64, vp, vp, vp, i64]
+    L.hplb_gemm_lp_sub.restype = i32
     for name in ("hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_matgen", "hplb_pdgesv", "hplb_residual", "hplb_residual_lcg",
                  "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm"):
         getattr(L, name).restype = i32
@@ -154,6 +157,10 @@ class Library:
             arr = (C.c_int * len(ipiv_host))(*[int(v) for v in ipiv_host])
         self._check(self.L.hplb_laswp_trsm(self.ctx, A, ld, ia, jb, lc, arr, c0, n))
 
+
+    def gemm_lp_sub(self, bf16, m, n, k, A16, lda, B16, ldb, sA, sB, Cp, ldc):
+        self._check(self.L.hplb_gemm_lp_sub(self.ctx, int(bf16), m, n, k, A16, lda, B16, ldb,
+                                            sA, sB, Cp, ldc))
 
     def fp64_peak(self, iters: int = 20000) -> tuple[float, float]:
         a, b = C.c_double(0), C.c_double(0)
