@@ -136,6 +136,50 @@ hplb_status hplb_dgemm_sub(hplb_ctx* ctx, int m, int n, int k, const double* dA,
 hplb_status hplb_laswp_trsm(hplb_ctx* ctx, double* dA, int64_t ld, int ia, int jb,
                             int lc, const int* ipiv_host, int c0, int n);
 
+/* ------------------------------------------------------------------------
+ * Mixed-precision form (no counterpart in the reference, which is FP64 only).
+ * LU in FP32 storage with the panel in FP32 and the trailing update on the
+ * tensor cores in BF16 or FP16 (per-tile power-of-two scaling, FP32
+ * accumulation), then flexible GMRES iterative refinement in FP64,
+ * preconditioned by the low-precision factors, until the HPL scaled residual
+ * is below target_resid.  FP64 is used only for r = b - A x against the FP64
+ * A, the solution update and the norms.
+ * ------------------------------------------------------------------------ */
+typedef struct hplb_mixed_opts {
+  int    precision;    /* trailing update: 0 = BF16 (default), 1 = FP16, 2 = BF16 x3 and
+                          3 = FP16 x3 (each operand split into high and low 16-bit parts,
+                          three products accumulated in FP32: FP32-accurate factors) */
+  int    restart;      /* GMRES restart length (<= 0: 20) */
+  int    max_outer;    /* refinement steps (<= 0: 20) */
+  double target_resid; /* stop below this HPL scaled residual (<= 0: 16.0) */
+  double gmres_tol;    /* relative residual reduction per GMRES cycle (<= 0: 1e-6) */
+} hplb_mixed_opts;
+
+typedef struct hplb_mixed_report {
+  double resid;        /* final HPL scaled residual */
+  double resid_lu;     /* scaled residual of x = M^-1 b with the low-precision LU alone */
+  int    outer_iters;  /* refinement steps taken */
+  int    gmres_iters;  /* GMRES iterations in total (one preconditioned A-product each) */
+  int    converged;    /* resid < target_resid */
+  int    info;         /* first zero pivot of the FP32 panel (1-based), 0 if none */
+  double lu_ms;        /* low-precision factorisation */
+  double ir_ms;        /* refinement (initial solve included) */
+  double total_ms;     /* time to solution (device events, first to last) */
+  double gemm_ms;      /* tensor-core trailing-update kernel time within lu_ms */
+  double gemm_flops;   /* tensor-core flops of those kernels (x3 counted for the split forms) */
+  double panel_ms;     /* FP32 panel factorisation time (concurrent with the updates) */
+} hplb_mixed_report;
+
+/* Solve the n x n system of [A|b].  dA: the FP64 [A|b] (n x (n+1), leading
+ * dimension ld, not modified), or NULL to use the HPL LCG matrix of `seed`
+ * regenerated on the fly (bit-identical to hplb_matgen; no n x n FP64 buffer
+ * is needed, which is what lets n = 131072 fit beside the FP32 factors).
+ * dX receives x (n doubles, device); ipiv_out (device, may be NULL) the pivots
+ * of the low-precision LU. */
+hplb_status hplb_pdgesv_mixed(hplb_ctx* ctx, const hplb_algo* algo, const hplb_mixed_opts* opts,
+                              int n, const double* dA, int64_t ld, uint64_t seed, double* dX,
+                              int* ipiv_out, hplb_mixed_report* report);
+
 /* Mixed-precision trailing update (tensor cores, tcgen05): C -= sA[i] sB[j]
  * A16 B16^T on 128 x 256 tiles, FP32 accumulation.  C is m x n FP32
  * column-major; A16 (m x k) and B16 (n x k) are row-major 16-bit (bf16 != 0:

@@ -22,87 +22,11 @@
 #include <string>
 #include <vector>
 
-#include "common.cuh"
-#include "internal.h"
+#include "ctx.h"
 
 using namespace hplb;
 
-struct hplb_ctx {
-  int          device  = 0;
-  int          num_sms = 0;
-  cudaStream_t s_upd   = nullptr;
-  cudaStream_t s_pan   = nullptr;
-  std::string  err;
-  hplb_timing  timing{};
-
-  int*    d_status = nullptr;  // ST_COUNT ints
-  int*    d_bar    = nullptr;  // 2 ints
-  double* d_out8   = nullptr;  // residual outputs
-
-  int*    d_ipiv   = nullptr;
-  size_t  ipiv_cap = 0;
-  int*    d_perm[2] = {nullptr, nullptr};
-  double* d_dinv[2] = {nullptr, nullptr};
-  double* d_linv[2] = {nullptr, nullptr};  // L11^-1 per panel set (nb x nb)
-  double* d_dinv_piece = nullptr;
-  double* d_w          = nullptr;  // gathered top rows of the trailing columns (nb x (n+1))
-  size_t  w_cap        = 0;        // doubles
-  int     nb_cap       = 0;
-  double* d_cand       = nullptr;
-  double* d_cur        = nullptr;
-  size_t  cand_cap     = 0;  // doubles
-  double* d_res        = nullptr;
-  size_t  res_cap      = 0;  // doubles
-
-  std::vector<cudaEvent_t> events;  // pool
-  size_t                   ev_next = 0;
-  int                      launches = 0;
-};
-
 namespace {
-
-hplb_status set_err(hplb_ctx* c, hplb_status s, const char* fmt, ...) {
-  char    buf[512];
-  va_list ap;
-  va_start(ap, fmt);
-  vsnprintf(buf, sizeof buf, fmt, ap);
-  va_end(ap);
-  if(c) c->err = buf;
-  return s;
-}
-
-#define CK(expr)                                                                       \
-  do {                                                                                 \
-    cudaError_t e__ = (expr);                                                          \
-    if(e__ != cudaSuccess)                                                             \
-      return set_err(ctx, HPLB_ERR_CUDA, "%s failed: %s (%s:%d)", #expr,               \
-                     cudaGetErrorString(e__), __FILE__, __LINE__);                     \
-  } while(0)
-
-template <class T>
-hplb_status grow(hplb_ctx* ctx, T** p, size_t* cap, size_t need) {
-  if(*cap >= need && *p) return HPLB_OK;
-  if(*p) cudaFree(*p);
-  *p   = nullptr;
-  *cap = 0;
-  if(cudaMalloc((void**)p, need * sizeof(T)) != cudaSuccess) {
-    cudaGetLastError();
-    *p = nullptr;
-    return set_err(ctx, HPLB_ERR_OOM, "workspace allocation of %zu bytes failed",
-                   need * sizeof(T));
-  }
-  *cap = need;
-  return HPLB_OK;
-}
-
-cudaEvent_t next_event(hplb_ctx* ctx) {
-  if(ctx->ev_next == ctx->events.size()) {
-    cudaEvent_t e;
-    cudaEventCreate(&e);
-    ctx->events.push_back(e);
-  }
-  return ctx->events[ctx->ev_next++];
-}
 
 // U12 = L11^-1 (P A12) as a DMMA GEMM (default), or by the blocked
 // substitution kernel (HPLB_TRSM_PATH=substitution, kept for comparison).
@@ -146,11 +70,7 @@ hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
   if(n > 0 && trsm_by_inverse() &&
      (s = grow(ctx, &ctx->d_w, &ctx->w_cap, (size_t)nb * (size_t)(n + 1))) != HPLB_OK)
     return s;
-  const int    gmax = leaf_grid_size(ctx->num_sms, std::max(n, 1));
-  const size_t need = 2 * (size_t)gmax * (2 + std::min(nbmin, kMaxLeaf)) + 2 * kMaxLeaf;
-  if((s = grow(ctx, &ctx->d_cand, &ctx->cand_cap, need)) != HPLB_OK) return s;
-  ctx->d_cur = ctx->d_cand + 2 * (size_t)gmax * (2 + std::min(nbmin, kMaxLeaf));
-  return HPLB_OK;
+  return ensure_leaf_ws(ctx, n, nbmin);
 }
 
 struct Solve {
@@ -277,16 +197,6 @@ struct Solve {
   }
 };
 
-hplb_status read_status(hplb_ctx* ctx, int* info_out) {
-  int st[ST_COUNT];
-  CK(cudaMemcpy(st, ctx->d_status, sizeof st, cudaMemcpyDeviceToHost));
-  if(info_out) *info_out = st[ST_INFO];
-  if(st[ST_TIMEOUT] != 0)
-    return set_err(ctx, HPLB_ERR_TIMEOUT, "a bounded device wait expired (site %d)",
-                   st[ST_TIMEOUT]);
-  return HPLB_OK;
-}
-
 }  // namespace
 
 extern "C" {
@@ -349,7 +259,9 @@ void hplb_destroy(hplb_ctx* ctx) {
   void* bufs[] = {ctx->d_status, ctx->d_bar,      ctx->d_out8,        ctx->d_ipiv,
                   ctx->d_perm[0], ctx->d_perm[1], ctx->d_dinv[0],     ctx->d_dinv[1],
                   ctx->d_dinv_piece, ctx->d_cand, ctx->d_res, ctx->d_linv[0], ctx->d_linv[1],
-                  ctx->d_w};
+                  ctx->d_w,       ctx->m_w,       ctx->m_linv,        ctx->m_uinv,
+                  ctx->m_perm,    ctx->m_g,       ctx->m_l16,         ctx->m_u16,
+                  ctx->m_scale,   ctx->m_small,   ctx->m_vec};
   for(void* b : bufs)
     if(b) cudaFree(b);
   if(ctx->s_upd) cudaStreamDestroy(ctx->s_upd);
@@ -373,27 +285,14 @@ hplb_status hplb_matgen(hplb_ctx* ctx, int m, int n, int nb, uint64_t seed, doub
 hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA, int64_t ld,
                         double* dX, int* ipiv_out, int* info) {
   if(!ctx) return HPLB_ERR_ARG;
-  if(!algo) return set_err(ctx, HPLB_ERR_ARG, "hplb_pdgesv: null algo");
-  if(n < 0) return set_err(ctx, HPLB_ERR_ARG, "Value of N less than 0");
-  if(algo->nb < 1) return set_err(ctx, HPLB_ERR_ARG, "Value of NB less than 1");
-  if(algo->nbmin < 1) return set_err(ctx, HPLB_ERR_ARG, "Value of NBMIN less than 1");
-  if(algo->ndiv < 2) return set_err(ctx, HPLB_ERR_ARG, "Value of NDIV less than 2");
-  if(algo->pfact < 0 || algo->pfact > 2)
-    return set_err(ctx, HPLB_ERR_ARG, "Value of PFACT out of range");
-  if(algo->rfact < 0 || algo->rfact > 2)
-    return set_err(ctx, HPLB_ERR_ARG, "Value of RFACT out of range");
-  if(algo->depth != 1)
-    return set_err(ctx, HPLB_ERR_UNSUPPORTED, "Only lookahead depth 1 is supported");
-  if(algo->nbmin > kMaxLeaf)
-    return set_err(ctx, HPLB_ERR_UNSUPPORTED, "NBMIN above %d is not supported", kMaxLeaf);
-  if(algo->nb > 2048) return set_err(ctx, HPLB_ERR_UNSUPPORTED, "NB above 2048 is not supported");
-  if(ld < std::max(1, n)) return set_err(ctx, HPLB_ERR_ARG, "hplb_pdgesv: ld < max(1,N)");
+  hplb_status s = check_algo(ctx, algo, n, ld, true);
+  if(s != HPLB_OK) return s;
   if(info) *info = 0;
   ctx->timing = hplb_timing{};
   if(n == 0) return HPLB_OK;
   if(!dA || !dX) return set_err(ctx, HPLB_ERR_ARG, "hplb_pdgesv: null matrix or solution");
   CK(cudaSetDevice(ctx->device));
-  hplb_status s = ensure_solve_ws(ctx, n, algo->nb, algo->nbmin);
+  s = ensure_solve_ws(ctx, n, algo->nb, algo->nbmin);
   if(s != HPLB_OK) return s;
 
   ctx->ev_next  = 0;

@@ -31,26 +31,34 @@ cudaError_t launch_dgemm_cpasync(int m, int n, int k, const double* A, int64_t l
                                  bool accumulate, cudaStream_t stream);
 
 int         leaf_grid_size(int num_sms, int rows);
-cudaError_t launch_leaf(double* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
+// The panel kernels exist for double (the FP64 solve) and float (the FP32
+// panel of the mixed-precision solve).
+template <typename T>
+cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
                         double* cand, double* cur, int* bar, int* status, int grid,
                         cudaStream_t stream);
-cudaError_t launch_panel_swap(double* A, int64_t ld, const int* ipiv, int r0, int c0, int w,
-                              int pc, int pw, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_panel_swap(T* A, int64_t ld, const int* ipiv, int r0, int c0, int w, int pc,
+                              int pw, cudaStream_t stream);
 cudaError_t launch_perm(const int* ipiv, int ia, int jb, int* permU, cudaStream_t stream);
-cudaError_t launch_diag_inv(const double* A, int64_t ld, int r0, int c0, int n, double* inv,
+template <typename T>
+cudaError_t launch_diag_inv(const T* A, int64_t ld, int r0, int c0, int n, T* inv,
                             cudaStream_t stream);
 int         trsm_wcol(int jb);
 size_t      trsm_smem_bytes(int jb);
-cudaError_t launch_laswp_trsm(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
-                              const double* dinv, int c0, int n, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_laswp_trsm(T* A, int64_t ld, int ia, int jb, int lc, const int* permU,
+                              const T* dinv, int c0, int n, cudaStream_t stream);
 // Linv (jb x jb, leading dimension ldinv) = L^-1 for the unit-lower L at L
 // (leading dimension ldl), by the blocked substitution applied to the identity.
-cudaError_t launch_unit_lower_inverse(const double* L, int64_t ldl, int jb, const double* dinv,
-                                      double* Linv, int64_t ldinv, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_unit_lower_inverse(const T* L, int64_t ldl, int jb, const T* dinv, T* Linv,
+                                      int64_t ldinv, cudaStream_t stream);
 // Panel interchanges on columns [c0, c0+n): new top rows gathered into W
 // (jb x n, leading dimension ldw), displaced rows written in place.
-cudaError_t launch_laswp_gather(double* A, int64_t ld, int ia, int jb, const int* permU,
-                                double* W, int64_t ldw, int c0, int n, cudaStream_t stream);
+template <typename T>
+cudaError_t launch_laswp_gather(T* A, int64_t ld, int ia, int jb, const int* permU, T* W,
+                                int64_t ldw, int c0, int n, cudaStream_t stream);
 
 // Back-solve U x = y, y = column n of A, x written to X.
 cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* status,
@@ -60,6 +68,47 @@ cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* stat
 size_t      residual_ws_doubles(int n);
 cudaError_t launch_residual(int n, const double* A, int64_t ld, bool lcg, uint64_t seed,
                             const double* X, double* ws, double* out8, cudaStream_t stream);
+
+// y = A x (FP64) and column extraction for [A|b], stored or regenerated from
+// the LCG; ws as for launch_residual.
+cudaError_t launch_gemv_hpl(int n, const double* A, int64_t ld, bool lcg, uint64_t seed,
+                            const double* x, double* y, double* ws, cudaStream_t stream);
+cudaError_t launch_column_hpl(int n, int col, const double* A, int64_t ld, bool lcg,
+                              uint64_t seed, double* out, double* ws, cudaStream_t stream);
+
+// Mixed-precision helpers (mixed.cu, sgemm.cu, matgen.cu).
+cudaError_t launch_sgemm(int m, int n, int k, const float* A, int64_t lda, const float* B,
+                         int64_t ldb, float* C, int64_t ldc, bool accumulate, cudaStream_t stream);
+cudaError_t launch_f64_to_f32(int m, int n, const double* A, int64_t lda, float* W, int64_t ldw,
+                              cudaStream_t st);
+// split: three jb-wide segments per packed row (hi/lo parts, K = 3 jb).
+cudaError_t launch_pack_l(bool bf16, bool split, int m, int jb, const float* L, int64_t ld,
+                          void* out, int64_t ldo, float* sL, cudaStream_t st);
+cudaError_t launch_pack_u(bool bf16, bool split, int jb, int n, const float* U, int64_t ld,
+                          void* out, int64_t ldo, float* sU, cudaStream_t st);
+cudaError_t launch_upper_inverse(int jb, const float* U, int64_t ld, float* Uinv, float* work,
+                                 float* dinv_work, cudaStream_t st);
+cudaError_t launch_perm_vec(double* z, int ia, int jb, const int* permU, cudaStream_t st);
+cudaError_t launch_tri_apply(const float* T, int jb, double* z, int o, cudaStream_t st);
+cudaError_t launch_gemv_sub(int rows, int cols, const float* M, int64_t ld, const double* x,
+                            double* y, cudaStream_t st);
+int         vec_partials();
+cudaError_t launch_dot(int n, const double* a, const double* b, double* part, double* out,
+                       cudaStream_t st);
+cudaError_t launch_amax(int n, const double* a, double* part, double* out, cudaStream_t st);
+// Gram-Schmidt over k <= 64 columns of V (leading dimension ldv):
+// out[i] = V_i . w (part: mdot_partials(k) doubles) and w -= V h (acc += h
+// when acc is not null).
+size_t      mdot_partials(int k);
+cudaError_t launch_mdot(int n, int k, const double* V, int64_t ldv, const double* w,
+                        double* part, double* out, cudaStream_t st);
+cudaError_t launch_mgemv_sub(int n, int k, const double* V, int64_t ldv, const double* h,
+                             double* w, double* acc, cudaStream_t st);
+cudaError_t launch_axpy(int n, double a, const double* x, double* y, cudaStream_t st);
+cudaError_t launch_scal_copy(int n, double a, const double* x, double* y, cudaStream_t st);
+cudaError_t launch_sub(int n, const double* a, const double* b, double* c, cudaStream_t st);
+cudaError_t launch_matgen_f32(int m, int n, uint64_t seed, float* W, int64_t ld,
+                              cudaStream_t stream);
 
 // FP64 issue-rate probes (TFLOP/s) and the bounded-wait self test.
 cudaError_t fp64_peak(int num_sms, int iters, double* dmma_tflops, double* dfma_tflops,

@@ -26,13 +26,14 @@ struct MatgenTables {
   Jump step32;    // jump by 32
 };
 
+template <typename T>
 __global__ void __launch_bounds__(kWarps * 32)
-matgen_kernel(int m, int n, int64_t ld, double* __restrict__ A, uint64_t x1,
-              MatgenTables T) {
+matgen_kernel(int m, int n, int64_t ld, T* __restrict__ A, uint64_t x1,
+              MatgenTables Tab) {
   __shared__ Jump s_pow2[64];
   __shared__ Jump s_lane[32];
-  for(int i = threadIdx.x; i < 64; i += blockDim.x) s_pow2[i] = T.pow2[i];
-  if(threadIdx.x < 32) s_lane[threadIdx.x] = T.lane[threadIdx.x];
+  for(int i = threadIdx.x; i < 64; i += blockDim.x) s_pow2[i] = Tab.pow2[i];
+  if(threadIdx.x < 32) s_lane[threadIdx.x] = Tab.lane[threadIdx.x];
   __syncthreads();
 
   const int lane   = threadIdx.x & 31;
@@ -54,18 +55,18 @@ matgen_kernel(int m, int n, int64_t ld, double* __restrict__ A, uint64_t x1,
   s = __shfl_sync(0xffffffffu, s, 0);
   s = apply(s_lane[lane], s);
 
-  double* col = A + (size_t)j * (size_t)ld;
-  const Jump st = T.step32;
+  T* col = A + (size_t)j * (size_t)ld;
+  const Jump st = Tab.step32;
   if(i0 + kRun <= m) {
 #pragma unroll 4
     for(int r = 0; r < kRowsPerLane; ++r) {
-      col[i0 + r * 32 + lane] = lcg_value(s);
+      col[i0 + r * 32 + lane] = (T)lcg_value(s);
       s = apply(st, s);
     }
   } else {
     for(int r = 0; r < kRowsPerLane; ++r) {
       const int i = i0 + r * 32 + lane;
-      if(i < m) col[i] = lcg_value(s);
+      if(i < m) col[i] = (T)lcg_value(s);
       s = apply(st, s);
     }
   }
@@ -73,8 +74,9 @@ matgen_kernel(int m, int n, int64_t ld, double* __restrict__ A, uint64_t x1,
 
 }  // namespace
 
-cudaError_t launch_matgen(int m, int n, uint64_t seed, double* A, int64_t ld,
-                          cudaStream_t stream) {
+template <typename E>
+static cudaError_t matgen_any(int m, int n, uint64_t seed, E* A, int64_t ld,
+                              cudaStream_t stream) {
   if(m <= 0 || n <= 0) return cudaSuccess;
   MatgenTables T;
   Jump p{kLcgMult, kLcgAdd};
@@ -88,8 +90,19 @@ cudaError_t launch_matgen(int m, int n, uint64_t seed, double* A, int64_t ld,
   const int64_t runs  = (m + kRun - 1) / kRun;
   const int64_t warps = runs * (int64_t)n;
   const int64_t grid  = (warps + kWarps - 1) / kWarps;
-  matgen_kernel<<<(unsigned)grid, kWarps * 32, 0, stream>>>(m, n, ld, A, x1, T);
+  matgen_kernel<E><<<(unsigned)grid, kWarps * 32, 0, stream>>>(m, n, ld, A, x1, T);
   return cudaGetLastError();
+}
+
+cudaError_t launch_matgen(int m, int n, uint64_t seed, double* A, int64_t ld,
+                          cudaStream_t stream) {
+  return matgen_any<double>(m, n, seed, A, ld, stream);
+}
+
+// The same matrix rounded to FP32 (the working copy of the mixed-precision solve).
+cudaError_t launch_matgen_f32(int m, int n, uint64_t seed, float* W, int64_t ld,
+                              cudaStream_t stream) {
+  return matgen_any<float>(m, n, seed, W, ld, stream);
 }
 
 }  // namespace hplb

@@ -81,8 +81,9 @@ HPLB_DEV void block_argmax(double& v, int& r, double* s_v, int* s_r) {
   __syncthreads();
 }
 
+template <typename T>
 struct LeafParams {
-  double* A;
+  T*      A;
   int64_t ld;
   int     r0, end;  // leaf rows [r0, end)
   int     c0, w;    // leaf columns [c0, c0 + w), w <= kMaxLeaf
@@ -96,12 +97,13 @@ struct LeafParams {
 
 // Publish this block's pivot candidate for leaf column k (its rows >= d) and,
 // when it owns row d, the diagonal row itself.
-HPLB_DEV void leaf_publish(const LeafParams& P, int k, int par, double* s_v, int* s_r) {
+template <typename T>
+HPLB_DEV void leaf_publish(const LeafParams<T>& P, int k, int par, double* s_v, int* s_r) {
   const int d   = P.r0 + k;
   const int lo  = P.r0 + blockIdx.x * P.rpb;
   const int hi  = min(P.end, lo + P.rpb);
   const int beg = max(lo, d);
-  const double* colk = P.A + (size_t)(P.c0 + k) * P.ld;
+  const T* colk = P.A + (size_t)(P.c0 + k) * P.ld;
   double v = 0.0;
   int    r = -1;
   for(int i = beg + threadIdx.x; i < hi; i += blockDim.x) {
@@ -125,7 +127,8 @@ HPLB_DEV void leaf_publish(const LeafParams& P, int k, int par, double* s_v, int
       P.cur[par * P.w + c] = P.A[(size_t)d + (size_t)(P.c0 + c) * P.ld];
 }
 
-__global__ void __launch_bounds__(kLeafThreads) leaf_kernel(LeafParams P) {
+template <typename T>
+__global__ void __launch_bounds__(kLeafThreads) leaf_kernel(LeafParams<T> P) {
   __shared__ double s_v[32];
   __shared__ int    s_r[32];
   __shared__ double s_u[kMaxLeaf];    // pivot row (leaf columns)
@@ -187,30 +190,30 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(LeafParams P) {
       }
     }
     __syncthreads();
-    const double piv = s_piv;
-    const int    p   = s_p;
+    const T   piv = (T)s_piv;
+    const int p   = s_p;
     if(blockIdx.x == 0 && threadIdx.x == 0) {
       P.ipiv[c] = p;
-      if(piv == 0.0) record_info(P.status, c + 1);
+      if(piv == (T)0) record_info(P.status, c + 1);
     }
     // Interchange rows d and p over the leaf columns.
     if(p != d && p >= lo && p < hi)
       for(int cc = threadIdx.x; cc < P.w; cc += blockDim.x)
-        P.A[(size_t)p + (size_t)(P.c0 + cc) * ld] = s_cur[cc];
+        P.A[(size_t)p + (size_t)(P.c0 + cc) * ld] = (T)s_cur[cc];
     if(d >= lo && d < hi)
       for(int cc = threadIdx.x; cc < P.w; cc += blockDim.x)
-        P.A[(size_t)d + (size_t)(P.c0 + cc) * ld] = s_u[cc];
+        P.A[(size_t)d + (size_t)(P.c0 + cc) * ld] = (T)s_u[cc];
     __syncthreads();
     // Scale column c below the diagonal (division, as the reference does at
     // src/pfact/HPL_pdpanrlT_device.cpp:232) and apply the rank-1 update to the
     // remaining leaf columns.
-    double* colc = P.A + (size_t)c * ld;
+    T* colc = P.A + (size_t)c * ld;
     for(int i = max(lo, d + 1) + threadIdx.x; i < hi; i += blockDim.x) {
-      const double l = colc[i] / piv;
-      colc[i]        = l;
+      const T l = colc[i] / piv;
+      colc[i]   = l;
       for(int cc = k + 1; cc < P.w; ++cc) {
-        double* a = P.A + (size_t)i + (size_t)(P.c0 + cc) * ld;
-        *a        = *a - l * s_u[cc];
+        T* a = P.A + (size_t)i + (size_t)(P.c0 + cc) * ld;
+        *a   = *a - l * (T)s_u[cc];
       }
     }
     if(k + 1 == P.w) break;
@@ -222,16 +225,17 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(LeafParams P) {
 
 // Apply the w interchanges of leaf columns [c0, c0+w) to the panel columns
 // outside the leaf, in order.  One thread per column.
-__global__ void panel_swap_kernel(double* A, int64_t ld, const int* ipiv, int r0, int c0,
+template <typename T>
+__global__ void panel_swap_kernel(T* A, int64_t ld, const int* ipiv, int r0, int c0,
                                   int w, int pc, int pw) {
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
   if(j >= pw - w) return;
   const int col = (pc + j < c0) ? pc + j : pc + j + w;
-  double*   a   = A + (size_t)col * ld;
+  T*        a   = A + (size_t)col * ld;
   for(int k = 0; k < w; ++k) {
     const int d = r0 + k, p = ipiv[c0 + k];
     if(p != d) {
-      const double t = a[d];
+      const T t = a[d];
       a[d]           = a[p];
       a[p]           = t;
     }
@@ -266,26 +270,26 @@ __global__ void perm_kernel(const int* ipiv, int ia, int jb, int* permU) {
 // Inverses of the unit-lower kTri x kTri diagonal blocks of L (n x n at
 // (r0, c0)); block b's inverse goes to inv[b * kTri * kTri], column-major.
 // A partial last block is padded with the identity.
-__global__ void diag_inv_kernel(const double* A, int64_t ld, int r0, int c0, int n,
-                                double* inv) {
-  __shared__ double L[kTri][kTri + 1];
+template <typename T>
+__global__ void diag_inv_kernel(const T* A, int64_t ld, int r0, int c0, int n, T* inv) {
+  __shared__ T L[kTri][kTri + 1];
   const int b = blockIdx.x, lane = threadIdx.x;
   const int base = b * kTri;
   for(int c = 0; c < kTri; ++c) {
     const bool in = (base + lane < n) && (base + c < n);
-    L[lane][c] = in ? A[(size_t)(r0 + base + lane) + (size_t)(c0 + base + c) * ld] : 0.0;
+    L[lane][c] = in ? A[(size_t)(r0 + base + lane) + (size_t)(c0 + base + c) * ld] : (T)0;
   }
   __syncwarp();
   // Column `lane` of L^-1: forward substitution with the unit diagonal.
-  double x[kTri];
+  T x[kTri];
 #pragma unroll
   for(int i = 0; i < kTri; ++i) {
-    double s = (i == lane) ? 1.0 : 0.0;
+    T s = (i == lane) ? (T)1 : (T)0;
 #pragma unroll
     for(int k = 0; k < i; ++k) s -= L[i][k] * x[k];
-    x[i] = (i < lane) ? 0.0 : s;
+    x[i] = (i < lane) ? (T)0 : s;
   }
-  double* out = inv + (size_t)b * kTri * kTri + (size_t)lane * kTri;
+  T* out = inv + (size_t)b * kTri * kTri + (size_t)lane * kTri;
 #pragma unroll
   for(int i = 0; i < kTri; ++i) out[i] = x[i];
 }
@@ -296,11 +300,12 @@ __global__ void diag_inv_kernel(const double* A, int64_t ld, int r0, int c0, int
 //   semantics: gather the new top rows, send displaced top rows down).
 //   Then X := L^-1 X with L the unit-lower jb x jb block at (ia, lc), blocked
 //   by kTri rows: X_b = Dinv_b (X_b - L(b, 0:b) X(0:b)).
-template <int WCOL>
+template <int WCOL, typename T>
 __global__ void __launch_bounds__(256)
-laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, const double* L, int64_t ldl,
-                  const int* permU, const double* dinv, int c0, int n) {
-  extern __shared__ double sx[];  // [WCOL][jb + 1] column-major, padded
+laswp_trsm_kernel(T* A, int64_t ld, int ia, int jb, const T* L, int64_t ldl,
+                  const int* permU, const T* dinv, int c0, int n) {
+  extern __shared__ __align__(16) unsigned char sx_raw[];
+  T* sx = (T*)sx_raw;  // [WCOL][jb + 1] column-major, padded
   const int ldx = jb + 1;
   const int cb  = c0 + blockIdx.x * WCOL;
   const int nc  = min(WCOL, c0 + n - cb);
@@ -334,24 +339,24 @@ laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, const double* L, int64_
   const int nblk = (jb + kTri - 1) / kTri;
   for(int b = 0; b < nblk; ++b) {
     const int row0 = b * kTri;
-    double acc[CPT];
+    T acc[CPT];
 #pragma unroll
-    for(int q = 0; q < CPT; ++q) acc[q] = 0.0;
+    for(int q = 0; q < CPT; ++q) acc[q] = (T)0;
     const int gr = row0 + r;
     if(gr < jb) {
-      const double* Lrow = L + (size_t)gr;
+      const T* Lrow = L + (size_t)gr;
       for(int kk = 0; kk < row0; ++kk) {
-        const double l = Lrow[(size_t)kk * (size_t)ldl];
+        const T l = Lrow[(size_t)kk * (size_t)ldl];
 #pragma unroll
         for(int q = 0; q < CPT; ++q) acc[q] += l * sx[(size_t)(cg * CPT + q) * ldx + kk];
       }
     }
     // R = X_b - acc, kept in registers; then X_b = Dinv_b R via shared memory.
-    double rv[CPT];
+    T rv[CPT];
 #pragma unroll
     for(int q = 0; q < CPT; ++q) {
       const int c = cg * CPT + q;
-      rv[q] = (gr < jb) ? sx[(size_t)c * ldx + gr] - acc[q] : 0.0;
+      rv[q] = (gr < jb) ? sx[(size_t)c * ldx + gr] - acc[q] : (T)0;
     }
     __syncthreads();
 #pragma unroll
@@ -360,11 +365,11 @@ laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, const double* L, int64_
       if(gr < jb) sx[(size_t)c * ldx + gr] = rv[q];
     }
     __syncthreads();
-    const double* D = dinv + (size_t)b * kTri * kTri;
+    const T* D = dinv + (size_t)b * kTri * kTri;
 #pragma unroll
-    for(int q = 0; q < CPT; ++q) acc[q] = 0.0;
+    for(int q = 0; q < CPT; ++q) acc[q] = (T)0;
     for(int kk = 0; kk < kTri && row0 + kk < jb; ++kk) {
-      const double dv = D[(size_t)kk * kTri + r];
+      const T dv = D[(size_t)kk * kTri + r];
 #pragma unroll
       for(int q = 0; q < CPT; ++q) acc[q] += dv * sx[(size_t)(cg * CPT + q) * ldx + row0 + kk];
     }
@@ -390,9 +395,10 @@ laswp_trsm_kernel(double* A, int64_t ld, int ia, int jb, const double* L, int64_
 // CTA owns kGatherCols columns; its gathers from rows >= jb read exactly the
 // rows its displaced writes overwrite, hence the barrier between the two.
 constexpr int kGatherCols = 8;
+template <typename T>
 __global__ void __launch_bounds__(256)
-laswp_gather_kernel(double* A, int64_t ld, int ia, int jb, const int* __restrict__ permU,
-                    double* __restrict__ W, int64_t ldw, int c0, int n) {
+laswp_gather_kernel(T* A, int64_t ld, int ia, int jb, const int* __restrict__ permU,
+                    T* __restrict__ W, int64_t ldw, int c0, int n) {
   const int cb = c0 + blockIdx.x * kGatherCols;
   const int nc = min(kGatherCols, c0 + n - cb);
   for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
@@ -410,9 +416,11 @@ laswp_gather_kernel(double* A, int64_t ld, int ia, int jb, const int* __restrict
 }
 
 // Writes the jb x jb identity into X (leading dimension ldx).
-__global__ void identity_kernel(double* X, int64_t ldx, int jb) {
+template <typename T>
+__global__ void identity_kernel(T* X, int64_t ldx, int jb) {
   const int c = blockIdx.x;
-  for(int r = threadIdx.x; r < jb; r += blockDim.x) X[(size_t)r + (size_t)c * ldx] = (r == c);
+  for(int r = threadIdx.x; r < jb; r += blockDim.x)
+    X[(size_t)r + (size_t)c * ldx] = (r == c) ? (T)1 : (T)0;
 }
 
 }  // namespace
@@ -423,7 +431,7 @@ __global__ void identity_kernel(double* X, int64_t ldx, int jb) {
 
 int leaf_grid_size(int num_sms, int rows) {
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_kernel, kLeafThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, leaf_kernel<double>, kLeafThreads, 0);
   if(per_sm < 1) per_sm = 1;
   const int max_grid = num_sms * per_sm;
   // At least ~256 rows per block so the barrier count is worth the parallelism.
@@ -433,10 +441,11 @@ int leaf_grid_size(int num_sms, int rows) {
   return g;
 }
 
-cudaError_t launch_leaf(double* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
+template <typename T>
+cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
                         double* cand, double* cur, int* bar, int* status, int grid,
                         cudaStream_t stream) {
-  LeafParams P;
+  LeafParams<T> P;
   P.A = A;
   P.ld = ld;
   P.r0 = r0;
@@ -452,15 +461,16 @@ cudaError_t launch_leaf(double* A, int64_t ld, int r0, int end, int c0, int w, i
   cudaError_t e = cudaMemsetAsync(bar, 0, 2 * sizeof(int), stream);
   if(e != cudaSuccess) return e;
   void* args[] = {&P};
-  return cudaLaunchCooperativeKernel((const void*)leaf_kernel, dim3(grid), dim3(kLeafThreads),
-                                     args, 0, stream);
+  return cudaLaunchCooperativeKernel((const void*)leaf_kernel<T>, dim3(grid),
+                                     dim3(kLeafThreads), args, 0, stream);
 }
 
-cudaError_t launch_panel_swap(double* A, int64_t ld, const int* ipiv, int r0, int c0, int w,
-                              int pc, int pw, cudaStream_t stream) {
+template <typename T>
+cudaError_t launch_panel_swap(T* A, int64_t ld, const int* ipiv, int r0, int c0, int w, int pc,
+                              int pw, cudaStream_t stream) {
   const int ncols = pw - w;
   if(ncols <= 0) return cudaSuccess;
-  panel_swap_kernel<<<(ncols + 127) / 128, 128, 0, stream>>>(A, ld, ipiv, r0, c0, w, pc, pw);
+  panel_swap_kernel<T><<<(ncols + 127) / 128, 128, 0, stream>>>(A, ld, ipiv, r0, c0, w, pc, pw);
   return cudaGetLastError();
 }
 
@@ -470,10 +480,11 @@ cudaError_t launch_perm(const int* ipiv, int ia, int jb, int* permU, cudaStream_
   return cudaGetLastError();
 }
 
-cudaError_t launch_diag_inv(const double* A, int64_t ld, int r0, int c0, int n, double* inv,
+template <typename T>
+cudaError_t launch_diag_inv(const T* A, int64_t ld, int r0, int c0, int n, T* inv,
                             cudaStream_t stream) {
   if(n <= 0) return cudaSuccess;
-  diag_inv_kernel<<<(n + kTri - 1) / kTri, kTri, 0, stream>>>(A, ld, r0, c0, n, inv);
+  diag_inv_kernel<T><<<(n + kTri - 1) / kTri, kTri, 0, stream>>>(A, ld, r0, c0, n, inv);
   return cudaGetLastError();
 }
 
@@ -484,62 +495,75 @@ size_t trsm_smem_bytes(int jb) {
   return (size_t)w * (jb + 1) * 8;
 }
 
-static cudaError_t launch_trsm_any(double* X, int64_t ldx, int ia, int jb, const double* L,
-                                   int64_t ldl, const int* permU, const double* dinv, int c0,
-                                   int n, cudaStream_t stream) {
+template <int W, typename T>
+static cudaError_t launch_trsm_w(int grid, size_t smem, T* X, int64_t ldx, int ia, int jb,
+                                 const T* L, int64_t ldl, const int* permU, const T* dinv,
+                                 int c0, int n, cudaStream_t stream) {
+  cudaError_t e = cudaFuncSetAttribute(laswp_trsm_kernel<W, T>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if(e != cudaSuccess) return e;
+  laswp_trsm_kernel<W, T><<<grid, 256, smem, stream>>>(X, ldx, ia, jb, L, ldl, permU, dinv, c0,
+                                                       n);
+  return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t launch_trsm_any(T* X, int64_t ldx, int ia, int jb, const T* L, int64_t ldl,
+                                   const int* permU, const T* dinv, int c0, int n,
+                                   cudaStream_t stream) {
   if(n <= 0 || jb <= 0) return cudaSuccess;
   const int    w    = trsm_wcol(jb);
-  const size_t smem = trsm_smem_bytes(jb);
+  const size_t smem = trsm_smem_bytes(jb);  // sized for double; ample for float
   const int    grid = (n + w - 1) / w;
-  cudaError_t  e    = cudaSuccess;
   switch(w) {
     case 32:
-      e = cudaFuncSetAttribute(laswp_trsm_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-      if(e == cudaSuccess)
-        laswp_trsm_kernel<32><<<grid, 256, smem, stream>>>(X, ldx, ia, jb, L, ldl, permU, dinv,
-                                                           c0, n);
-      break;
+      return launch_trsm_w<32, T>(grid, smem, X, ldx, ia, jb, L, ldl, permU, dinv, c0, n, stream);
     case 16:
-      e = cudaFuncSetAttribute(laswp_trsm_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-      if(e == cudaSuccess)
-        laswp_trsm_kernel<16><<<grid, 256, smem, stream>>>(X, ldx, ia, jb, L, ldl, permU, dinv,
-                                                           c0, n);
-      break;
+      return launch_trsm_w<16, T>(grid, smem, X, ldx, ia, jb, L, ldl, permU, dinv, c0, n, stream);
     default:
-      e = cudaFuncSetAttribute(laswp_trsm_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem);
-      if(e == cudaSuccess)
-        laswp_trsm_kernel<8><<<grid, 256, smem, stream>>>(X, ldx, ia, jb, L, ldl, permU, dinv,
-                                                          c0, n);
-      break;
+      return launch_trsm_w<8, T>(grid, smem, X, ldx, ia, jb, L, ldl, permU, dinv, c0, n, stream);
   }
-  if(e != cudaSuccess) return e;
-  return cudaGetLastError();
 }
 
-cudaError_t launch_laswp_trsm(double* A, int64_t ld, int ia, int jb, int lc, const int* permU,
-                              const double* dinv, int c0, int n, cudaStream_t stream) {
-  return launch_trsm_any(A, ld, ia, jb, A + (size_t)ia + (size_t)lc * ld, ld, permU, dinv, c0, n,
-                         stream);
+template <typename T>
+cudaError_t launch_laswp_trsm(T* A, int64_t ld, int ia, int jb, int lc, const int* permU,
+                              const T* dinv, int c0, int n, cudaStream_t stream) {
+  return launch_trsm_any<T>(A, ld, ia, jb, A + (size_t)ia + (size_t)lc * ld, ld, permU, dinv, c0,
+                            n, stream);
 }
 
-cudaError_t launch_unit_lower_inverse(const double* L, int64_t ldl, int jb, const double* dinv,
-                                      double* Linv, int64_t ldinv, cudaStream_t stream) {
+template <typename T>
+cudaError_t launch_unit_lower_inverse(const T* L, int64_t ldl, int jb, const T* dinv, T* Linv,
+                                      int64_t ldinv, cudaStream_t stream) {
   if(jb <= 0) return cudaSuccess;
-  identity_kernel<<<jb, 128, 0, stream>>>(Linv, ldinv, jb);
+  identity_kernel<T><<<jb, 128, 0, stream>>>(Linv, ldinv, jb);
   cudaError_t e = cudaGetLastError();
   if(e != cudaSuccess) return e;
-  return launch_trsm_any(Linv, ldinv, 0, jb, L, ldl, nullptr, dinv, 0, jb, stream);
+  return launch_trsm_any<T>(Linv, ldinv, 0, jb, L, ldl, nullptr, dinv, 0, jb, stream);
 }
 
-cudaError_t launch_laswp_gather(double* A, int64_t ld, int ia, int jb, const int* permU,
-                                double* W, int64_t ldw, int c0, int n, cudaStream_t stream) {
+template <typename T>
+cudaError_t launch_laswp_gather(T* A, int64_t ld, int ia, int jb, const int* permU, T* W,
+                                int64_t ldw, int c0, int n, cudaStream_t stream) {
   if(n <= 0 || jb <= 0) return cudaSuccess;
-  laswp_gather_kernel<<<(n + kGatherCols - 1) / kGatherCols, 256, 0, stream>>>(A, ld, ia, jb,
-                                                                              permU, W, ldw, c0, n);
+  laswp_gather_kernel<T><<<(n + kGatherCols - 1) / kGatherCols, 256, 0, stream>>>(
+      A, ld, ia, jb, permU, W, ldw, c0, n);
   return cudaGetLastError();
 }
+
+#define HPLB_PANEL_INSTANTIATE(T)                                                              \
+  template cudaError_t launch_leaf<T>(T*, int64_t, int, int, int, int, int*, double*, double*, \
+                                      int*, int*, int, cudaStream_t);                          \
+  template cudaError_t launch_panel_swap<T>(T*, int64_t, const int*, int, int, int, int, int,  \
+                                            cudaStream_t);                                     \
+  template cudaError_t launch_diag_inv<T>(const T*, int64_t, int, int, int, T*, cudaStream_t); \
+  template cudaError_t launch_laswp_trsm<T>(T*, int64_t, int, int, int, const int*, const T*,  \
+                                            int, int, cudaStream_t);                           \
+  template cudaError_t launch_unit_lower_inverse<T>(const T*, int64_t, int, const T*, T*,      \
+                                                    int64_t, cudaStream_t);                    \
+  template cudaError_t launch_laswp_gather<T>(T*, int64_t, int, int, const int*, T*, int64_t,  \
+                                              int, int, cudaStream_t);
+HPLB_PANEL_INSTANTIATE(double)
+HPLB_PANEL_INSTANTIATE(float)
 
 }  // namespace hplb

@@ -245,6 +245,83 @@ cudaError_t launch_residual(int n, const double* A, int64_t ld, bool lcg, uint64
   return cudaGetLastError();
 }
 
+namespace {
+
+// y[i] = sum of the per-chunk partials of row i (fixed order).
+__global__ void rows_sum(int n, int nch, const double* __restrict__ part, double* __restrict__ y) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  double acc = 0.0;
+  for(int c = 0; c < nch; ++c) acc += part[(size_t)c * n + i];
+  y[i] = acc;
+}
+
+// out[i] = A(i, col), from the stored matrix or regenerated from the LCG.
+template <bool LCG>
+__global__ void column_of(int n, int col, const double* __restrict__ A, int64_t ld,
+                          const ResTabs* __restrict__ T, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if(i >= n) return;
+  if(LCG)
+    out[i] = lcg_value(state_of(*T, (uint64_t)i + (uint64_t)col * (uint64_t)n));
+  else
+    out[i] = A[(size_t)i + (size_t)col * ld];
+}
+
+cudaError_t upload_tabs(int n, uint64_t seed, ResTabs* dT, cudaStream_t stream) {
+  ResTabs T;
+  Jump p{kLcgMult, kLcgAdd};
+  for(int b = 0; b < 64; ++b) {
+    T.pow2[b] = p;
+    p         = compose(p, p);
+  }
+  T.col    = jump_by((uint64_t)n);
+  T.step32 = jump_by(32);
+  T.x1     = kLcgMult * seed + kLcgAdd;
+  cudaError_t e = cudaMemcpyAsync(dT, &T, sizeof(T), cudaMemcpyHostToDevice, stream);
+  if(e != cudaSuccess) return e;
+  return cudaStreamSynchronize(stream);  // T lives on this stack frame
+}
+
+}  // namespace
+
+// y = A x for the n x n part of [A|b], FP64, from the stored matrix or the LCG.
+// ws: residual_ws_doubles(n) doubles.
+cudaError_t launch_gemv_hpl(int n, const double* A, int64_t ld, bool lcg, uint64_t seed,
+                            const double* x, double* y, double* ws, cudaStream_t stream) {
+  if(n <= 0) return cudaSuccess;
+  const int nch = (n + kChunk - 1) / kChunk;
+  const int nrb = (n + kRowThreads - 1) / kRowThreads;
+  double*   part_r = ws;
+  double*   part_a = part_r + (size_t)nch * n;
+  ResTabs*  dT = reinterpret_cast<ResTabs*>(((uintptr_t)(part_a + (size_t)nch * n) + 63) &
+                                            ~(uintptr_t)63);
+  cudaError_t e = upload_tabs(n, seed, dT, stream);
+  if(e != cudaSuccess) return e;
+  dim3 g1(nrb, nch);
+  if(lcg)
+    rows_partial<true><<<g1, kRowThreads, 0, stream>>>(n, A, ld, x, dT, part_r, part_a);
+  else
+    rows_partial<false><<<g1, kRowThreads, 0, stream>>>(n, A, ld, x, dT, part_r, part_a);
+  rows_sum<<<nrb, kRowThreads, 0, stream>>>(n, nch, part_r, y);
+  return cudaGetLastError();
+}
+
+// out = column col of [A|b] (col = n gives b).
+cudaError_t launch_column_hpl(int n, int col, const double* A, int64_t ld, bool lcg,
+                              uint64_t seed, double* out, double* ws, cudaStream_t stream) {
+  if(n <= 0) return cudaSuccess;
+  ResTabs* dT = reinterpret_cast<ResTabs*>(((uintptr_t)ws + 63) & ~(uintptr_t)63);
+  cudaError_t e = upload_tabs(n, seed, dT, stream);
+  if(e != cudaSuccess) return e;
+  const int nrb = (n + kRowThreads - 1) / kRowThreads;
+  if(lcg)
+    column_of<true><<<nrb, kRowThreads, 0, stream>>>(n, col, A, ld, dT, out);
+  else
+    column_of<false><<<nrb, kRowThreads, 0, stream>>>(n, col, A, ld, dT, out);
+  return cudaGetLastError();
+}
+
 }  // namespace hplb
 
 // ---------------------------------------------------------------------------

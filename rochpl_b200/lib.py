@@ -26,7 +26,7 @@ EXPORTS = [
     "hplb_default_ld", "hplb_matgen", "hplb_pdgesv", "hplb_residual",
     "hplb_residual_lcg", "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm",
     "hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_residual_lcg_noalloc",
-    "hplb_gemm_lp_sub",
+    "hplb_gemm_lp_sub", "hplb_pdgesv_mixed",
 ]
 
 
@@ -44,6 +44,22 @@ class hplb_timing(C.Structure):
     _fields_ = [("total_ms", C.c_double), ("lu_ms", C.c_double), ("trsv_ms", C.c_double),
                 ("gemm_ms", C.c_double), ("gemm_flops", C.c_double), ("panel_ms", C.c_double),
                 ("gemm_launches", C.c_int), ("kernel_launches", C.c_int)]
+
+
+class hplb_mixed_opts(C.Structure):
+    _fields_ = [("precision", C.c_int), ("restart", C.c_int), ("max_outer", C.c_int),
+                ("target_resid", C.c_double), ("gmres_tol", C.c_double)]
+
+
+class hplb_mixed_report(C.Structure):
+    _fields_ = [("resid", C.c_double), ("resid_lu", C.c_double), ("outer_iters", C.c_int),
+                ("gmres_iters", C.c_int), ("converged", C.c_int), ("info", C.c_int),
+                ("lu_ms", C.c_double), ("ir_ms", C.c_double), ("total_ms", C.c_double),
+                ("gemm_ms", C.c_double), ("gemm_flops", C.c_double), ("panel_ms", C.c_double)]
+
+
+# hplb_mixed_opts.precision values
+PREC_BF16, PREC_FP16, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2, 3
 
 
 class HplError(RuntimeError):
@@ -88,6 +104,9 @@ def load() -> C.CDLL:
     L.hplb_residual_lcg_noalloc.restype = i32
     L.hplb_gemm_lp_sub.argtypes = [vp, i32, i32, i32, i32, vp, i64, vp, i64, vp, vp, vp, i64]
     L.hplb_gemm_lp_sub.restype = i32
+    L.hplb_pdgesv_mixed.argtypes = [vp, C.POINTER(hplb_algo), C.POINTER(hplb_mixed_opts), i32, vp,
+                                    i64, u64, vp, vp, C.POINTER(hplb_mixed_report)]
+    L.hplb_pdgesv_mixed.restype = i32
     for name in ("hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_matgen", "hplb_pdgesv", "hplb_residual", "hplb_residual_lcg",
                  "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm"):
         getattr(L, name).restype = i32
@@ -132,6 +151,23 @@ class Library:
                                 C.byref(info))
         self._check(st, allow=(HPLB_OK, HPLB_ERR_SINGULAR))
         return info.value
+
+    def pdgesv_mixed(self, algo: hplb_algo, n: int, X: int, seed: int = 100, A: int | None = None,
+                     ld: int = 0, precision: int = PREC_BF16X3, restart: int = 20,
+                     max_outer: int = 20, target_resid: float = 16.0, gmres_tol: float = 1e-6,
+                     ipiv: int | None = None) -> dict:
+        """hplb_pdgesv_mixed: low-precision LU + GMRES refinement.  A None
+        solves the LCG system of `seed` without a stored FP64 matrix.  Returns
+        the report as a dict (plus "status"); a zero pivot is reported, not
+        raised."""
+        o = hplb_mixed_opts(precision, restart, max_outer, target_resid, gmres_tol)
+        r = hplb_mixed_report()
+        st = self.L.hplb_pdgesv_mixed(self.ctx, C.byref(algo), C.byref(o), n, A or None, ld,
+                                      seed, X, ipiv or None, C.byref(r))
+        self._check(st, allow=(HPLB_OK, HPLB_ERR_SINGULAR))
+        out = {k: getattr(r, k) for k, _ in hplb_mixed_report._fields_}
+        out["status"] = st
+        return out
 
     def residual(self, n: int, A: int, ld: int, X: int) -> dict:
         r = hplb_resid()
