@@ -105,7 +105,7 @@ def test_mixed_pivots_match_fp32_lu_of_oracle_order(hlib, oracle):
                             ipiv=dP.data_ptr())
     p = dP.cpu().numpy()
     assert np.all(p >= np.arange(n)) and np.all(p < n)
-    assert rep["resid_lu"] > rep["resid"] and rep["converged"] == 1
+    assert rep["resid_lu"] >= rep["resid"] and rep["converged"] == 1
 
 
 def test_mixed_bad_arguments(hlib):
