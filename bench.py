@@ -11,6 +11,11 @@ repeats.  Timing is CUDA events on the launching streams, max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+After the FP64 steps the same system is solved in the mixed-precision form
+(16-bit tensor-core LU, BF16 x3 and FP16 x3, + FP64 GMRES refinement to the
+same residual threshold); its time to solution, speed-up over the FP64 solve,
+iteration counts and distance to the FP64 x go under "mixed" in the line.
+
 Multi-GPU runs are replicas (each rank solves its own system; P = Q = 1 has
 no inter-GPU data path), reported as weak scaling.
 
@@ -234,6 +239,13 @@ def run_ours(args):
     if not args.no_e2e:
         e2e = end_to_end(lib, algo, n, ld, seed, dA, dX, barrier, max_over_ranks, world)
 
+    mixed = None
+    if not args.no_mixed:
+        x64 = dX.double().cpu().numpy()
+        dA = None  # the FP64 [A|b] cannot stay beside the FP32 factors at this N
+        torch.cuda.empty_cache()
+        mixed = mixed_leg(lib, algo, n, seed, x64, solve_ms, args, barrier, max_over_ranks)
+
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_baseline(args.cpu_n, nb)
@@ -273,12 +285,72 @@ def run_ours(args):
         }
         if e2e is not None:
             line["e2e"] = e2e
+        if mixed is not None:
+            line["mixed"] = mixed
         if cb is not None:
             line["cpu_baseline"] = cb
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()
     return 0
+
+
+def _measured_peaks() -> dict:
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def mixed_leg(lib, algo, n, seed, x64, fp64_ms, args, barrier, max_over_ranks):
+    """The mixed-precision form on the same system: low-precision LU + GMRES
+    refinement to the HPL residual threshold, timed on the device (first to
+    last event of hplb_pdgesv_mixed), against the FP64 solve just timed.  A is
+    regenerated from the LCG for r = b - A x (bit-identical to the stored FP64
+    A, which does not fit in HBM beside the FP32 factors at N = 131072)."""
+    import numpy as np
+    import torch
+
+    from rochpl_b200.lib import PREC_BF16X3, PREC_FP16X3
+
+    peaks = _measured_peaks()
+    bf16_peak = peaks.get("bf16_tflops_sustained") or 1394.6
+    src = "MEASURED_PEAKS.json bf16_tflops_sustained" if peaks else "fallback 1394.6"
+    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+    out = {"note": "time to HPL scaled residual < 16 (target 16.0); value = (2/3N^3+2N^2)/t, "
+                   "the HPL-equivalent rate; speedup = FP64 solve time / mixed time; "
+                   "GMRES-IR in FP64, A regenerated from the LCG for r = b - Ax",
+           "bf16_peak_tflops": bf16_peak, "bf16_peak_source": src}
+    for name, prec in (("bf16x3", PREC_BF16X3), ("fp16x3", PREC_FP16X3)):
+        for _ in range(max(1, args.mixed_warmup)):
+            lib.pdgesv_mixed(algo.c(), n, dX.data_ptr(), seed=seed, precision=prec)
+        reps = []
+        for _ in range(args.mixed_steps):
+            torch.cuda.synchronize()
+            barrier()
+            reps.append(lib.pdgesv_mixed(algo.c(), n, dX.data_ptr(), seed=seed, precision=prec))
+        tm = lib.last_timing()
+        ms = max_over_ranks(statistics.mean(r["total_ms"] for r in reps))
+        r = reps[-1]
+        chk = lib.residual_lcg(n, seed, dX.data_ptr())
+        x = dX.cpu().numpy()
+        gemm_tf = r["gemm_flops"] / (r["gemm_ms"] * 1e-3) / 1e12 if r["gemm_ms"] > 0 else 0.0
+        out[name] = {
+            "time_to_solution_ms": ms, "speedup_vs_fp64": fp64_ms / ms,
+            "value": hpl_flops(n) / (ms * 1e-3) / 1e12, "unit": UNIT,
+            "resid": chk["resid"], "resid_passed": chk["resid"] < 16.0,
+            "resid_lu_only": r["resid_lu"], "outer_iters": r["outer_iters"],
+            "gmres_iters": r["gmres_iters"],
+            "rel_err_vs_fp64_x": float(np.max(np.abs(x - x64)) / np.max(np.abs(x64))),
+            "lu_ms": r["lu_ms"], "ir_ms": r["ir_ms"], "panel_ms": r["panel_ms"],
+            "roofline": {"kernel": "gemm_lp_kernel (tcgen05 16-bit trailing update, x3 split)",
+                         "bound": "tensor", "achieved": gemm_tf, "peak": bf16_peak,
+                         "unit": "TFLOP/s", "frac": gemm_tf / bf16_peak,
+                         "gemm_ms": r["gemm_ms"], "gemm_flops": r["gemm_flops"]},
+            "gpu_launches": tm["kernel_launches"], "steps": args.mixed_steps,
+        }
+    return out
 
 
 def _cudart():
@@ -368,6 +440,10 @@ def main():
                     help="host sample size for the CPU baseline / reference arm")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision (16-bit LU + GMRES-IR) leg")
+    ap.add_argument("--mixed-steps", type=int, default=2)
+    ap.add_argument("--mixed-warmup", type=int, default=1)
     ap.add_argument("--gemm-traffic", type=float, default=None,
                     help="DRAM bytes per DGEMM launch from an ncu capture, if known")
     args = ap.parse_args()
