@@ -108,6 +108,29 @@ hplb_status hplb_matgen(hplb_ctx* ctx, int m, int n, int nb, uint64_t seed,
 hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA,
                         int64_t ld, double* dX, int* ipiv_out, int* info);
 
+/* The factorisation of hplb_pdgesv on the n x n A alone (no right-hand side
+ * column, no back-solve): the same panels, pivots and layout, for use with
+ * hplb_getrs.  No counterpart in the reference (HPL_pdgesv always carries b). */
+hplb_status hplb_getrf(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA, int64_t ld,
+                       int* ipiv_out, int* info);
+
+/* Solve op(A) X = B with the factors hplb_pdgesv / hplb_getrf left in dLU
+ * (leading dimension ld) and their pivots d_ipiv (device, n ints, each
+ * ipiv[i] in [i, n)); nb must be the NB of that factorisation.  trans = 0:
+ * A X = B; trans = 1: A^T X = B (this form also takes an n x n workspace).  B
+ * (device, n x nrhs, leading dimension ldb) is overwritten by X.  The
+ * solve-side building block of the differentiable solve; no counterpart in the
+ * reference. */
+hplb_status hplb_getrs(hplb_ctx* ctx, int trans, int n, int nb, int nrhs, const double* dLU,
+                       int64_t ld, const int* d_ipiv, double* dB, int64_t ldb);
+
+/* C = alpha A B^T (accumulate = 0) or C += alpha A B^T (accumulate != 0) in one
+ * fused kernel: A m x k, B n x k, C m x n, all column-major FP64 on the device,
+ * k <= 64.  The adjoint's Abar = -Bbar X^T. */
+hplb_status hplb_rank_k(hplb_ctx* ctx, int m, int n, int k, double alpha, const double* dA,
+                        int64_t lda, const double* dB, int64_t ldb, double* dC, int64_t ldc,
+                        int accumulate);
+
 /* The HPL residual check: dA must hold the regenerated [A|b] (hplb_matgen with
  * the seed of the solve), dX the solution.  Results go to *out (host). */
 hplb_status hplb_residual(hplb_ctx* ctx, int n, const double* dA, int64_t ld,

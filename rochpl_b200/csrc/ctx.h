@@ -47,6 +47,11 @@ struct hplb_ctx {
   float*          m_small = nullptr;  size_t m_small_cap = 0;  // inverses' scratch
   double*         m_vec   = nullptr;  size_t m_vec_cap   = 0;  // FP64 vectors
 
+  // Multi-RHS solve workspaces (hplb_getrs).
+  double* r_t    = nullptr;  size_t r_t_cap    = 0;  // transposed factors (trans = 1)
+  double* r_ws   = nullptr;  size_t r_ws_cap   = 0;  // block copies and inverses
+  int*    r_perm = nullptr;  size_t r_perm_cap = 0;  // one panel's row map
+
   std::vector<cudaEvent_t> events;  // pool
   size_t                   ev_next = 0;
   int                      launches = 0;

@@ -261,7 +261,8 @@ void hplb_destroy(hplb_ctx* ctx) {
                   ctx->d_dinv_piece, ctx->d_cand, ctx->d_res, ctx->d_linv[0], ctx->d_linv[1],
                   ctx->d_w,       ctx->m_w,       ctx->m_linv,        ctx->m_uinv,
                   ctx->m_perm,    ctx->m_g,       ctx->m_l16,         ctx->m_u16,
-                  ctx->m_scale,   ctx->m_small,   ctx->m_vec};
+                  ctx->m_scale,   ctx->m_small,   ctx->m_vec,         ctx->r_t,
+                  ctx->r_ws,      ctx->r_perm};
   for(void* b : bufs)
     if(b) cudaFree(b);
   if(ctx->s_upd) cudaStreamDestroy(ctx->s_upd);
@@ -282,15 +283,20 @@ hplb_status hplb_matgen(hplb_ctx* ctx, int m, int n, int nb, uint64_t seed, doub
   return HPLB_OK;
 }
 
-hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA, int64_t ld,
-                        double* dX, int* ipiv_out, int* info) {
+}  // extern "C"
+
+// The factorisation loop shared by hplb_pdgesv (rhs: column n of A is b,
+// carried through the updates, then the back-solve into dX) and hplb_getrf
+// (A alone, no back-solve).
+static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA,
+                                 int64_t ld, double* dX, int* ipiv_out, int* info, bool rhs) {
   if(!ctx) return HPLB_ERR_ARG;
   hplb_status s = check_algo(ctx, algo, n, ld, true);
   if(s != HPLB_OK) return s;
   if(info) *info = 0;
   ctx->timing = hplb_timing{};
   if(n == 0) return HPLB_OK;
-  if(!dA || !dX) return set_err(ctx, HPLB_ERR_ARG, "hplb_pdgesv: null matrix or solution");
+  if(!dA || (rhs && !dX)) return set_err(ctx, HPLB_ERR_ARG, "null matrix or solution");
   CK(cudaSetDevice(ctx->device));
   s = ensure_solve_ws(ctx, n, algo->nb, algo->nbmin);
   if(s != HPLB_OK) return s;
@@ -319,10 +325,10 @@ hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA,
       CK(cudaStreamWaitEvent(ctx->s_pan, ev_la, 0));
       if((s = S.panel(c1, set ^ 1, ev_panel[set ^ 1])) != HPLB_OK) return s;
     }
-    if((s = S.update(j, set, c1 + la, n + 1 - (c1 + la))) != HPLB_OK) return s;
+    if((s = S.update(j, set, c1 + la, n + (rhs ? 1 : 0) - (c1 + la))) != HPLB_OK) return s;
   }
   CK(cudaEventRecord(ev_lu, ctx->s_upd));
-  CK(launch_trsv(dA, ld, n, dX, ctx->d_status, ctx->s_upd, &ctx->launches));
+  if(rhs) CK(launch_trsv(dA, ld, n, dX, ctx->d_status, ctx->s_upd, &ctx->launches));
   if(ipiv_out)
     CK(cudaMemcpyAsync(ipiv_out, ctx->d_ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice,
                        ctx->s_upd));
@@ -359,6 +365,18 @@ hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA,
   if(s != HPLB_OK) return s;
   if(inf != 0) return set_err(ctx, HPLB_ERR_SINGULAR, "zero pivot in column %d", inf);
   return HPLB_OK;
+}
+
+extern "C" {
+
+hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA, int64_t ld,
+                        double* dX, int* ipiv_out, int* info) {
+  return factor_driver(ctx, algo, n, dA, ld, dX, ipiv_out, info, true);
+}
+
+hplb_status hplb_getrf(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA, int64_t ld,
+                       int* ipiv_out, int* info) {
+  return factor_driver(ctx, algo, n, dA, ld, nullptr, ipiv_out, info, false);
 }
 
 static hplb_status residual_common(hplb_ctx* ctx, int n, const double* dA, int64_t ld, bool lcg,

@@ -86,8 +86,11 @@ cudaError_t launch_pack_l(bool bf16, bool split, int m, int jb, const float* L, 
                           void* out, int64_t ldo, float* sL, cudaStream_t st);
 cudaError_t launch_pack_u(bool bf16, bool split, int jb, int n, const float* U, int64_t ld,
                           void* out, int64_t ldo, float* sU, cudaStream_t st);
-cudaError_t launch_upper_inverse(int jb, const float* U, int64_t ld, float* Uinv, float* work,
-                                 float* dinv_work, cudaStream_t st);
+// Uinv = U^-1 for the upper-triangular U (jb x jb at U, leading dimension
+// ld); work: 2 jb^2 + jb elements, dinv_work: (jb/32 + 1) * 1024.
+template <typename T>
+cudaError_t launch_upper_inverse(int jb, const T* U, int64_t ld, T* Uinv, T* work, T* dinv_work,
+                                 cudaStream_t st);
 cudaError_t launch_perm_vec(double* z, int ia, int jb, const int* permU, cudaStream_t st);
 cudaError_t launch_tri_apply(const float* T, int jb, double* z, int o, cudaStream_t st);
 cudaError_t launch_gemv_sub(int rows, int cols, const float* M, int64_t ld, const double* x,
@@ -109,6 +112,21 @@ cudaError_t launch_scal_copy(int n, double a, const double* x, double* y, cudaSt
 cudaError_t launch_sub(int n, const double* a, const double* b, double* c, cudaStream_t st);
 cudaError_t launch_matgen_f32(int m, int n, uint64_t seed, float* W, int64_t ld,
                               cudaStream_t stream);
+
+// Multi-RHS solve pieces (rhs.cu).
+template <typename T>
+cudaError_t launch_transpose(int m, int n, const T* src, int64_t lds, T* dst, int64_t ldd,
+                             cudaStream_t st);
+// Inverse of a panel's row map on columns [0, n) of B: rows moved back to where
+// the forward interchanges took them from.
+cudaError_t launch_laswp_inverse(double* B, int64_t ldb, int ia, int jb, const int* permU, int n,
+                                 cudaStream_t st);
+// C = alpha A B^T (+ C when accumulate); A m x k, B n x k, k <= 64.
+cudaError_t launch_rank_k(int m, int n, int k, double alpha, const double* A, int64_t lda,
+                          const double* B, int64_t ldb, double* C, int64_t ldc, bool accumulate,
+                          cudaStream_t st);
+// status[ST_INFO] = first i (1-based) with ipiv[i] outside [i, n), else untouched.
+cudaError_t launch_check_ipiv(int n, const int* ipiv, int* status, cudaStream_t st);
 
 // FP64 issue-rate probes (TFLOP/s) and the bounded-wait self test.
 cudaError_t fp64_peak(int num_sms, int iters, double* dmma_tflops, double* dfma_tflops,

@@ -150,12 +150,13 @@ pack_u_kernel(int jb, int n, const float* __restrict__ U, int64_t ld,
 
 // Lf = J (D^-1 U) J for the jb x jb upper block U (leading dimension ld):
 // unit lower, leading dimension jb.  d[i] = U(i, i).
-__global__ void upper_flip_in_kernel(int jb, const float* __restrict__ U, int64_t ld,
-                                     float* __restrict__ Lf, float* __restrict__ d) {
+template <typename T>
+__global__ void upper_flip_in_kernel(int jb, const T* __restrict__ U, int64_t ld,
+                                     T* __restrict__ Lf, T* __restrict__ d) {
   const int c = blockIdx.x;  // column of Lf
   for(int r = threadIdx.x; r < jb; r += blockDim.x) {
     const int ur = jb - 1 - r, uc = jb - 1 - c;
-    float v = 0.f;
+    T v = T(0);
     if(r >= c) v = U[(size_t)ur + (size_t)uc * ld] / U[(size_t)ur + (size_t)ur * ld];
     Lf[(size_t)r + (size_t)c * jb] = v;
   }
@@ -164,12 +165,13 @@ __global__ void upper_flip_in_kernel(int jb, const float* __restrict__ U, int64_
 }
 
 // Uinv = J Lfinv J D^-1 (all jb x jb, leading dimension jb).
-__global__ void upper_flip_out_kernel(int jb, const float* __restrict__ Lfinv,
-                                      const float* __restrict__ d, float* __restrict__ Uinv) {
+template <typename T>
+__global__ void upper_flip_out_kernel(int jb, const T* __restrict__ Lfinv,
+                                      const T* __restrict__ d, T* __restrict__ Uinv) {
   const int c = blockIdx.x;
   for(int r = threadIdx.x; r < jb; r += blockDim.x)
     Uinv[(size_t)r + (size_t)c * jb] =
-        (r <= c) ? Lfinv[(size_t)(jb - 1 - r) + (size_t)(jb - 1 - c) * jb] / d[c] : 0.f;
+        (r <= c) ? Lfinv[(size_t)(jb - 1 - r) + (size_t)(jb - 1 - c) * jb] / d[c] : T(0);
 }
 
 // Apply a panel's row map to a vector: z[ia + x] <- z[ia + permU[x]] for the
@@ -381,22 +383,27 @@ cudaError_t launch_pack_u(bool bf16, bool split, int jb, int n, const float* U, 
   return cudaGetLastError();
 }
 
-cudaError_t launch_upper_inverse(int jb, const float* U, int64_t ld, float* Uinv, float* work,
-                                 float* dinv_work, cudaStream_t st) {
+template <typename T>
+cudaError_t launch_upper_inverse(int jb, const T* U, int64_t ld, T* Uinv, T* work, T* dinv_work,
+                                 cudaStream_t st) {
   if(jb <= 0) return cudaSuccess;
   // work: jb*jb (flipped unit lower) + jb*jb (its inverse) + jb (diagonal).
-  float* Lf    = work;
-  float* Lfinv = work + (size_t)jb * jb;
-  float* d     = Lfinv + (size_t)jb * jb;
-  upper_flip_in_kernel<<<jb, 128, 0, st>>>(jb, U, ld, Lf, d);
+  T* Lf    = work;
+  T* Lfinv = work + (size_t)jb * jb;
+  T* d     = Lfinv + (size_t)jb * jb;
+  upper_flip_in_kernel<T><<<jb, 128, 0, st>>>(jb, U, ld, Lf, d);
   cudaError_t e = cudaGetLastError();
   if(e != cudaSuccess) return e;
-  if((e = launch_diag_inv<float>(Lf, jb, 0, 0, jb, dinv_work, st)) != cudaSuccess) return e;
-  if((e = launch_unit_lower_inverse<float>(Lf, jb, jb, dinv_work, Lfinv, jb, st)) != cudaSuccess)
+  if((e = launch_diag_inv<T>(Lf, jb, 0, 0, jb, dinv_work, st)) != cudaSuccess) return e;
+  if((e = launch_unit_lower_inverse<T>(Lf, jb, jb, dinv_work, Lfinv, jb, st)) != cudaSuccess)
     return e;
-  upper_flip_out_kernel<<<jb, 128, 0, st>>>(jb, Lfinv, d, Uinv);
+  upper_flip_out_kernel<T><<<jb, 128, 0, st>>>(jb, Lfinv, d, Uinv);
   return cudaGetLastError();
 }
+template cudaError_t launch_upper_inverse<float>(int, const float*, int64_t, float*, float*,
+                                                 float*, cudaStream_t);
+template cudaError_t launch_upper_inverse<double>(int, const double*, int64_t, double*, double*,
+                                                  double*, cudaStream_t);
 
 cudaError_t launch_perm_vec(double* z, int ia, int jb, const int* permU, cudaStream_t st) {
   if(jb <= 0) return cudaSuccess;

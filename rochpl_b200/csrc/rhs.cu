@@ -1,0 +1,154 @@
+// Kernels for solves with the stored HPL factors and many right-hand sides
+// (hplb_getrs) and for the fused rank-k product of the solve's adjoint
+// (hplb_rank_k).  No counterpart in the reference (its solve carries a single
+// b through the factorisation, src/pgesv/HPL_pdgesv.cpp).
+//
+//   transpose      dst = src^T, 32 x 32 tiles through shared memory
+//   laswp_inverse  P^T applied to columns of B: the inverse of a panel's row
+//                  map (new row x came from permU[x]; old top row s went to
+//                  permU[jb + s] or stayed in the top block when that is -1)
+//   rank_k         C = alpha A B^T (+ C), k <= 64: 64 x 64 output tiles, A and B
+//                  slices in shared memory, streaming stores (C is written once)
+//   check_ipiv     pivots in range before any kernel indexes with them
+#include "common.cuh"
+#include "internal.h"
+
+namespace hplb {
+
+namespace {
+
+template <typename T>
+__global__ void transpose_kernel(int m, int n, const T* __restrict__ src, int64_t lds,
+                                 T* __restrict__ dst, int64_t ldd) {
+  __shared__ T tile[32][33];
+  const int r0 = blockIdx.x * 32, c0 = blockIdx.y * 32;
+  for(int q = threadIdx.y; q < 32; q += blockDim.y) {
+    const int r = r0 + threadIdx.x, c = c0 + q;
+    if(r < m && c < n) tile[q][threadIdx.x] = src[(size_t)r + (size_t)c * lds];
+  }
+  __syncthreads();
+  for(int q = threadIdx.y; q < 32; q += blockDim.y) {
+    const int r = r0 + q, c = c0 + threadIdx.x;  // dst(c, r) = src(r, c)
+    if(r < m && c < n) dst[(size_t)c + (size_t)r * ldd] = tile[threadIdx.x][q];
+  }
+}
+
+// One column of B per block; all reads land in shared memory before any write,
+// so the permutation is applied in place.
+__global__ void laswp_inverse_kernel(double* B, int64_t ldb, int ia, int jb,
+                                     const int* __restrict__ permU) {
+  extern __shared__ double sm[];
+  double* t_new = sm;       // B(ia + x) for the top rows (new order)
+  double* t_dis = sm + jb;  // the row each displaced old top row moved to
+  double* col   = B + (size_t)blockIdx.x * ldb + ia;
+  for(int x = threadIdx.x; x < jb; x += blockDim.x) {
+    t_new[x]    = col[x];
+    const int d = permU[jb + x];
+    t_dis[x]    = d >= 0 ? col[d] : 0.0;
+  }
+  __syncthreads();
+  for(int x = threadIdx.x; x < jb; x += blockDim.x) col[permU[x]] = t_new[x];
+  for(int x = threadIdx.x; x < jb; x += blockDim.x)
+    if(permU[jb + x] >= 0) col[x] = t_dis[x];
+}
+
+constexpr int RK_T = 64, RK_K = 32;
+
+template <bool ACCUM>
+__global__ void __launch_bounds__(256)
+rank_k_kernel(int m, int n, int k, double alpha, const double* __restrict__ A, int64_t lda,
+              const double* __restrict__ B, int64_t ldb, double* __restrict__ C, int64_t ldc) {
+  __shared__ double As[RK_K][RK_T];
+  __shared__ double Bs[RK_K][RK_T];
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int m0 = blockIdx.x * RK_T, n0 = blockIdx.y * RK_T;
+  double acc[4][4] = {};
+  for(int k0 = 0; k0 < k; k0 += RK_K) {
+    const int kc = min(RK_K, k - k0);
+    for(int idx = tid; idx < RK_K * RK_T; idx += 256) {
+      const int r = idx & (RK_T - 1), kk = idx >> 6;
+      As[kk][r] = (kk < kc && m0 + r < m) ? A[(size_t)(m0 + r) + (size_t)(k0 + kk) * lda] : 0.0;
+      Bs[kk][r] = (kk < kc && n0 + r < n) ? B[(size_t)(n0 + r) + (size_t)(k0 + kk) * ldb] : 0.0;
+    }
+    __syncthreads();
+    for(int kk = 0; kk < kc; ++kk) {
+      double a[4], b[4];
+#pragma unroll
+      for(int i = 0; i < 4; ++i) a[i] = As[kk][tx + 16 * i];
+#pragma unroll
+      for(int j = 0; j < 4; ++j) b[j] = Bs[kk][ty + 16 * j];
+#pragma unroll
+      for(int i = 0; i < 4; ++i)
+#pragma unroll
+        for(int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for(int j = 0; j < 4; ++j) {
+    const int c = n0 + ty + 16 * j;
+    if(c >= n) continue;
+#pragma unroll
+    for(int i = 0; i < 4; ++i) {
+      const int r = m0 + tx + 16 * i;
+      if(r >= m) continue;
+      double* p = C + (size_t)r + (size_t)c * ldc;
+      if(ACCUM)
+        *p += alpha * acc[i][j];
+      else
+        __stcs(p, alpha * acc[i][j]);
+    }
+  }
+}
+
+__global__ void check_ipiv_kernel(int n, const int* __restrict__ ipiv, int* status) {
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    if(ipiv[i] < i || ipiv[i] >= n) record_info(status, i + 1);
+}
+
+}  // namespace
+
+template <typename T>
+cudaError_t launch_transpose(int m, int n, const T* src, int64_t lds, T* dst, int64_t ldd,
+                             cudaStream_t st) {
+  if(m <= 0 || n <= 0) return cudaSuccess;
+  dim3 grid((m + 31) / 32, (n + 31) / 32);
+  if(grid.y > 65535) return cudaErrorInvalidValue;
+  transpose_kernel<T><<<grid, dim3(32, 8), 0, st>>>(m, n, src, lds, dst, ldd);
+  return cudaGetLastError();
+}
+template cudaError_t launch_transpose<double>(int, int, const double*, int64_t, double*, int64_t,
+                                              cudaStream_t);
+template cudaError_t launch_transpose<float>(int, int, const float*, int64_t, float*, int64_t,
+                                             cudaStream_t);
+
+cudaError_t launch_laswp_inverse(double* B, int64_t ldb, int ia, int jb, const int* permU, int n,
+                                 cudaStream_t st) {
+  if(jb <= 0 || n <= 0) return cudaSuccess;
+  if(jb > 2048 || n > 65535) return cudaErrorInvalidValue;
+  laswp_inverse_kernel<<<n, 256, 2 * jb * sizeof(double), st>>>(B, ldb, ia, jb, permU);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rank_k(int m, int n, int k, double alpha, const double* A, int64_t lda,
+                          const double* B, int64_t ldb, double* C, int64_t ldc, bool accumulate,
+                          cudaStream_t st) {
+  if(m <= 0 || n <= 0) return cudaSuccess;
+  if(k < 0 || k > 64) return cudaErrorInvalidValue;
+  dim3 grid((m + RK_T - 1) / RK_T, (n + RK_T - 1) / RK_T);
+  if(grid.y > 65535) return cudaErrorInvalidValue;
+  if(accumulate)
+    rank_k_kernel<true><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, C, ldc);
+  else
+    rank_k_kernel<false><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, C, ldc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_check_ipiv(int n, const int* ipiv, int* status, cudaStream_t st) {
+  if(n <= 0) return cudaSuccess;
+  check_ipiv_kernel<<<(n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024, 256, 0, st>>>(n, ipiv,
+                                                                                     status);
+  return cudaGetLastError();
+}
+
+}  // namespace hplb

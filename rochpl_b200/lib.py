@@ -26,7 +26,7 @@ EXPORTS = [
     "hplb_default_ld", "hplb_matgen", "hplb_pdgesv", "hplb_residual",
     "hplb_residual_lcg", "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm",
     "hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_residual_lcg_noalloc",
-    "hplb_gemm_lp_sub", "hplb_pdgesv_mixed",
+    "hplb_gemm_lp_sub", "hplb_pdgesv_mixed", "hplb_getrf", "hplb_getrs", "hplb_rank_k",
 ]
 
 
@@ -107,6 +107,12 @@ def load() -> C.CDLL:
     L.hplb_pdgesv_mixed.argtypes = [vp, C.POINTER(hplb_algo), C.POINTER(hplb_mixed_opts), i32, vp,
                                     i64, u64, vp, vp, C.POINTER(hplb_mixed_report)]
     L.hplb_pdgesv_mixed.restype = i32
+    L.hplb_getrf.argtypes = [vp, C.POINTER(hplb_algo), i32, vp, i64, vp, C.POINTER(C.c_int)]
+    L.hplb_getrf.restype = i32
+    L.hplb_getrs.argtypes = [vp, i32, i32, i32, i32, vp, i64, vp, vp, i64]
+    L.hplb_getrs.restype = i32
+    L.hplb_rank_k.argtypes = [vp, i32, i32, i32, C.c_double, vp, i64, vp, i64, vp, i64, i32]
+    L.hplb_rank_k.restype = i32
     for name in ("hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_matgen", "hplb_pdgesv", "hplb_residual", "hplb_residual_lcg",
                  "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm"):
         getattr(L, name).restype = i32
@@ -168,6 +174,22 @@ class Library:
         out = {k: getattr(r, k) for k, _ in hplb_mixed_report._fields_}
         out["status"] = st
         return out
+
+    def getrf(self, algo: hplb_algo, n: int, A: int, ld: int, ipiv: int | None = None) -> int:
+        """hplb_getrf: factor A alone; returns info (0, or the first zero pivot)."""
+        info = C.c_int(0)
+        st = self.L.hplb_getrf(self.ctx, C.byref(algo), n, A, ld, ipiv or None, C.byref(info))
+        self._check(st, allow=(HPLB_OK, HPLB_ERR_SINGULAR))
+        return info.value
+
+    def getrs(self, trans: int, n: int, nb: int, nrhs: int, LU: int, ld: int, ipiv: int, B: int,
+              ldb: int):
+        self._check(self.L.hplb_getrs(self.ctx, int(trans), n, nb, nrhs, LU, ld, ipiv, B, ldb))
+
+    def rank_k(self, m: int, n: int, k: int, alpha: float, A: int, lda: int, B: int, ldb: int,
+               Cp: int, ldc: int, accumulate: bool = False):
+        self._check(self.L.hplb_rank_k(self.ctx, m, n, k, float(alpha), A, lda, B, ldb, Cp, ldc,
+                                       int(bool(accumulate))))
 
     def residual(self, n: int, A: int, ld: int, X: int) -> dict:
         r = hplb_resid()
