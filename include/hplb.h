@@ -82,6 +82,13 @@ typedef struct hplb_timing {
 hplb_ctx* hplb_create(int device, hplb_status* status);
 void      hplb_destroy(hplb_ctx* ctx);
 
+/* Inputs of every later call on ctx are read only after the work queued on
+ * `stream` (a cudaStream_t) before that call has finished; NULL (the default)
+ * means the legacy default stream.  Calls still return with their own work
+ * complete.  (The reference is synchronous per call, with no stream
+ * parameter.) */
+hplb_status hplb_set_stream(hplb_ctx* ctx, void* stream);
+
 const char* hplb_status_string(hplb_status s);
 /* Message of the last failing call on this context (never NULL). */
 const char* hplb_last_error(const hplb_ctx* ctx);

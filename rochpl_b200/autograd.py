@@ -42,6 +42,7 @@ class HplSolve(torch.autograd.Function):
             raise ValueError(f"shapes {tuple(A.shape)} and {tuple(B.shape)} do not form A X = B")
         n, nrhs = A.shape[0], B.shape[1]
         lib = library(A.device.index or 0)
+        lib.set_stream(torch.cuda.current_stream(A.device).cuda_stream)
         nbe = max(1, min(nb, max(n, 1)))
         LU = _colmajor(A.detach())
         ipiv = torch.zeros(max(n, 1), dtype=torch.int32, device=A.device)
@@ -61,6 +62,7 @@ class HplSolve(torch.autograd.Function):
         LU, ipiv, Xc = ctx.saved_tensors
         n, nrhs = Xc.shape[1], Xc.shape[0]
         lib = library(LU.device.index or 0)
+        lib.set_stream(torch.cuda.current_stream(LU.device).cuda_stream)
         Bc = _colmajor(Xbar.to(torch.float64))
         lib.getrs(1, n, ctx.nb, nrhs, LU.data_ptr(), max(n, 1), ipiv.data_ptr(), Bc.data_ptr(),
                   max(n, 1))

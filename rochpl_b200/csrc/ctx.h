@@ -52,6 +52,9 @@ struct hplb_ctx {
   double* r_ws   = nullptr;  size_t r_ws_cap   = 0;  // block copies and inverses
   int*    r_perm = nullptr;  size_t r_perm_cap = 0;  // one panel's row map
 
+  cudaStream_t caller   = nullptr;  // hplb_set_stream (null: the legacy default stream)
+  cudaEvent_t  ev_enter = nullptr;  // recorded on `caller` at every entry
+
   std::vector<cudaEvent_t> events;  // pool
   size_t                   ev_next = 0;
   int                      launches = 0;
@@ -134,6 +137,23 @@ inline cudaEvent_t next_event(hplb_ctx* ctx) {
   }
   return ctx->events[ctx->ev_next++];
 }
+
+// Every entry point starts here: the library's streams wait for the work the
+// caller queued on its stream before the call (inputs written by the caller's
+// kernels are complete before any kernel of the call reads them).
+inline hplb_status enter(hplb_ctx* ctx) {
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaEventRecord(ctx->ev_enter, ctx->caller));
+  CK(cudaStreamWaitEvent(ctx->s_upd, ctx->ev_enter, 0));
+  CK(cudaStreamWaitEvent(ctx->s_pan, ctx->ev_enter, 0));
+  return HPLB_OK;
+}
+
+#define ENTER(ctx)                          \
+  do {                                      \
+    hplb_status e__ = hplb::enter(ctx);     \
+    if(e__ != HPLB_OK) return e__;          \
+  } while(0)
 
 inline hplb_status read_status(hplb_ctx* ctx, int* info_out) {
   int st[ST_COUNT];

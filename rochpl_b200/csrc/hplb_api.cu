@@ -216,6 +216,12 @@ const char* hplb_status_string(hplb_status s) {
 
 const char* hplb_last_error(const hplb_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
 
+hplb_status hplb_set_stream(hplb_ctx* ctx, void* stream) {
+  if(!ctx) return HPLB_ERR_ARG;
+  ctx->caller = static_cast<cudaStream_t>(stream);
+  return HPLB_OK;
+}
+
 int64_t hplb_default_ld(int n) { return ((int64_t)std::max(1, n) + 95) / 128 * 128 + 32; }
 
 hplb_ctx* hplb_create(int device, hplb_status* status) {
@@ -236,6 +242,7 @@ hplb_ctx* hplb_create(int device, hplb_status* status) {
   cudaDeviceGetStreamPriorityRange(&lo, &hi);
   bool ok = cudaStreamCreateWithPriority(&ctx->s_upd, cudaStreamNonBlocking, lo) == cudaSuccess &&
             cudaStreamCreateWithPriority(&ctx->s_pan, cudaStreamNonBlocking, hi) == cudaSuccess &&
+            cudaEventCreateWithFlags(&ctx->ev_enter, cudaEventDisableTiming) == cudaSuccess &&
             cudaMalloc(&ctx->d_status, ST_COUNT * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&ctx->d_bar, 2 * sizeof(int)) == cudaSuccess &&
             cudaMalloc(&ctx->d_out8, 8 * sizeof(double)) == cudaSuccess;
@@ -256,6 +263,7 @@ void hplb_destroy(hplb_ctx* ctx) {
   if(ctx->s_upd) cudaStreamSynchronize(ctx->s_upd);
   if(ctx->s_pan) cudaStreamSynchronize(ctx->s_pan);
   for(auto e : ctx->events) cudaEventDestroy(e);
+  if(ctx->ev_enter) cudaEventDestroy(ctx->ev_enter);
   void* bufs[] = {ctx->d_status, ctx->d_bar,      ctx->d_out8,        ctx->d_ipiv,
                   ctx->d_perm[0], ctx->d_perm[1], ctx->d_dinv[0],     ctx->d_dinv[1],
                   ctx->d_dinv_piece, ctx->d_cand, ctx->d_res, ctx->d_linv[0], ctx->d_linv[1],
@@ -277,7 +285,7 @@ hplb_status hplb_matgen(hplb_ctx* ctx, int m, int n, int nb, uint64_t seed, doub
   if(m < 0 || n < 0) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen: negative size");
   if(ld < std::max(1, m)) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen: ld < max(1,m)");
   if(m > 0 && n > 0 && !dA) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen: null matrix");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   CK(launch_matgen(m, n, seed, dA, ld, ctx->s_upd));
   CK(cudaStreamSynchronize(ctx->s_upd));
   return HPLB_OK;
@@ -297,7 +305,7 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
   ctx->timing = hplb_timing{};
   if(n == 0) return HPLB_OK;
   if(!dA || (rhs && !dX)) return set_err(ctx, HPLB_ERR_ARG, "null matrix or solution");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   s = ensure_solve_ws(ctx, n, algo->nb, algo->nbmin);
   if(s != HPLB_OK) return s;
 
@@ -385,7 +393,7 @@ static hplb_status residual_common(hplb_ctx* ctx, int n, const double* dA, int64
   if(n < 0 || !out) return set_err(ctx, HPLB_ERR_ARG, "hplb_residual: bad argument");
   if(!lcg && n > 0 && (!dA || ld < n)) return set_err(ctx, HPLB_ERR_ARG, "hplb_residual: bad matrix");
   if(n > 0 && !dX) return set_err(ctx, HPLB_ERR_ARG, "hplb_residual: null solution");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   hplb_status s = grow(ctx, &ctx->d_res, &ctx->res_cap, residual_ws_doubles(std::max(n, 1)));
   if(s != HPLB_OK) return s;
   CK(launch_residual(n, dA, ld, lcg, seed, dX, ctx->d_res, ctx->d_out8, ctx->s_upd));
@@ -425,7 +433,7 @@ hplb_status hplb_dgemm_sub(hplb_ctx* ctx, int m, int n, int k, const double* dA,
   if(m < 0 || n < 0 || k < 0) return set_err(ctx, HPLB_ERR_ARG, "hplb_dgemm_sub: negative size");
   if(lda < std::max(1, m) || ldb < std::max(1, k) || ldc < std::max(1, m))
     return set_err(ctx, HPLB_ERR_ARG, "hplb_dgemm_sub: leading dimension too small");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
   CK(launch_dgemm_sub(m, n, k, dA, lda, dB, ldb, dC, ldc, ctx->d_status, ctx->s_upd));
   CK(cudaStreamSynchronize(ctx->s_upd));
@@ -438,7 +446,7 @@ hplb_status hplb_laswp_trsm(hplb_ctx* ctx, double* dA, int64_t ld, int ia, int j
   if(jb < 0 || jb > 2048 || n < 0 || ia < 0 || lc < 0 || c0 < 0)
     return set_err(ctx, HPLB_ERR_ARG, "hplb_laswp_trsm: bad argument");
   if(jb == 0 || n == 0) return HPLB_OK;
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   hplb_status s = ensure_solve_ws(ctx, ia + jb, std::max(jb, 1), 1);
   if(s != HPLB_OK) return s;
   const int* perm = nullptr;
@@ -465,7 +473,7 @@ hplb_status hplb_gemm_lp_sub(hplb_ctx* ctx, int bf16, int m, int n, int k, const
   if(m < 0 || n < 0 || k < 0 || lda < std::max(1, k) || ldb < std::max(1, k) ||
      ldc < std::max(1, m) || lda % 8 || ldb % 8)
     return set_err(ctx, HPLB_ERR_ARG, "hplb_gemm_lp_sub: bad sizes or leading dimensions");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
   CK(launch_gemm_lp(bf16 != 0, m, n, k, dA16, lda, dB16, ldb, dsA, dsB, dC, ldc, ctx->d_status,
                     ctx->s_upd));
@@ -475,7 +483,7 @@ hplb_status hplb_gemm_lp_sub(hplb_ctx* ctx, int bf16, int m, int n, int k, const
 
 hplb_status hplb_fp64_peak(hplb_ctx* ctx, int iters, double* dmma_tflops, double* dfma_tflops) {
   if(!ctx || iters < 1 || !dmma_tflops || !dfma_tflops) return HPLB_ERR_ARG;
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   CK(fp64_peak(ctx->num_sms, iters, dmma_tflops, dfma_tflops, ctx->s_upd));
   return HPLB_OK;
 }
@@ -484,7 +492,7 @@ hplb_status hplb_selftest_wait_timeout(hplb_ctx* ctx, uint64_t budget_ns) {
   if(!ctx) return HPLB_ERR_ARG;
   if(budget_ns > 10000000000ull)
     return set_err(ctx, HPLB_ERR_ARG, "hplb_selftest_wait_timeout: budget above 10 s");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
   // d_bar[0] is the flag: zeroed and never set.
   CK(cudaMemsetAsync(ctx->d_bar, 0, 2 * sizeof(int), ctx->s_upd));

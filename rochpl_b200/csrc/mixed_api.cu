@@ -352,7 +352,7 @@ extern "C" hplb_status hplb_pdgesv_mixed(hplb_ctx* ctx, const hplb_algo* algo,
   ctx->timing = hplb_timing{};
   if(n == 0) return HPLB_OK;
   if(!dX) return set_err(ctx, HPLB_ERR_ARG, "hplb_pdgesv_mixed: null solution");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
 
   Mixed M{};
   M.ctx   = ctx;

@@ -148,7 +148,7 @@ hplb_status hplb_getrs(hplb_ctx* ctx, int trans, int n, int nb, int nrhs, const 
   ctx->timing = hplb_timing{};
   if(n == 0 || nrhs == 0) return HPLB_OK;
   if(!dLU || !d_ipiv || !dB) return set_err(ctx, HPLB_ERR_ARG, "hplb_getrs: null pointer");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   Rhs R{};
   R.ctx  = ctx;
   R.n    = n;
@@ -208,7 +208,7 @@ hplb_status hplb_rank_k(hplb_ctx* ctx, int m, int n, int k, double alpha, const 
   if(m == 0 || n == 0) return HPLB_OK;
   if(!dC || (k > 0 && (!dA || !dB))) return set_err(ctx, HPLB_ERR_ARG, "hplb_rank_k: null pointer");
   if((n + 63) / 64 > 65535) return set_err(ctx, HPLB_ERR_UNSUPPORTED, "hplb_rank_k: n too large");
-  CK(cudaSetDevice(ctx->device));
+  ENTER(ctx);
   ctx->ev_next   = 0;
   cudaEvent_t e0 = next_event(ctx), e1 = next_event(ctx);
   CK(cudaEventRecord(e0, ctx->s_upd));

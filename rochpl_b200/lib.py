@@ -27,6 +27,7 @@ EXPORTS = [
     "hplb_residual_lcg", "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm",
     "hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_residual_lcg_noalloc",
     "hplb_gemm_lp_sub", "hplb_pdgesv_mixed", "hplb_getrf", "hplb_getrs", "hplb_rank_k",
+    "hplb_set_stream",
 ]
 
 
@@ -107,6 +108,8 @@ def load() -> C.CDLL:
     L.hplb_pdgesv_mixed.argtypes = [vp, C.POINTER(hplb_algo), C.POINTER(hplb_mixed_opts), i32, vp,
                                     i64, u64, vp, vp, C.POINTER(hplb_mixed_report)]
     L.hplb_pdgesv_mixed.restype = i32
+    L.hplb_set_stream.argtypes = [vp, vp]
+    L.hplb_set_stream.restype = i32
     L.hplb_getrf.argtypes = [vp, C.POINTER(hplb_algo), i32, vp, i64, vp, C.POINTER(C.c_int)]
     L.hplb_getrf.restype = i32
     L.hplb_getrs.argtypes = [vp, i32, i32, i32, i32, vp, i64, vp, vp, i64]
@@ -174,6 +177,11 @@ class Library:
         out = {k: getattr(r, k) for k, _ in hplb_mixed_report._fields_}
         out["status"] = st
         return out
+
+    def set_stream(self, stream: int | None):
+        """Order later calls after the work queued on `stream` (a raw
+        cudaStream_t, e.g. torch.cuda.current_stream().cuda_stream)."""
+        self._check(self.L.hplb_set_stream(self.ctx, stream or None))
 
     def getrf(self, algo: hplb_algo, n: int, A: int, ld: int, ipiv: int | None = None) -> int:
         """hplb_getrf: factor A alone; returns info (0, or the first zero pivot)."""
