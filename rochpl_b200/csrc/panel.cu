@@ -17,6 +17,8 @@
 //                      (rocblas_dtrsm, src/pgesv/HPL_pdupdateTT.cpp:95-106)
 //                      over a block of columns held in shared memory.
 #include <cooperative_groups.h>
+#include <cstdlib>
+#include <cstring>
 
 #include "common.cuh"
 #include "internal.h"
@@ -221,6 +223,152 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(LeafParams<T> P) {
     leaf_publish(P, k + 1, par ^ 1, s_v, s_r);
     if(!grid_sync(P.bar, G, P.status, 12)) return;
   }
+}
+
+// Leaf with the block's rows resident in shared memory (w <= kSmemLeafW).
+//
+// Each block loads its rpb x w slice of the leaf once, runs all w column steps
+// on it, and writes it back once; only the pivot candidates, the pivot row and
+// the old diagonal row cross global memory (the same exchange and bounded grid
+// barrier as leaf_kernel).  The arithmetic is that of leaf_kernel, operation
+// for operation (division by the pivot, then a_cc - l * u_cc per entry), so
+// the two kernels give identical bits; this one just never waits on L2
+// latency inside a column step.  The slice is column-major in shared memory,
+// sm[cc * rpb + i], so the pivot search and the update read consecutive words.
+constexpr int kSmemLeafW       = 32;
+constexpr int kSmemLeafThreads = 256;
+
+template <typename T>
+HPLB_DEV void leaf_smem_publish(const LeafParams<T>& P, const T* sm, int lo, int nr, int k,
+                                int par, double* s_v, int* s_r) {
+  const int d   = P.r0 + k;
+  const T*  col = sm + (size_t)k * P.rpb;
+  double    v   = 0.0;
+  int       r   = -1;
+  for(int i = max(0, d - lo) + threadIdx.x; i < nr; i += blockDim.x) {
+    const double a = col[i];
+    if(better(a, lo + i, v, r)) {
+      v = a;
+      r = lo + i;
+    }
+  }
+  block_argmax(v, r, s_v, s_r);
+  double* slot = P.cand + ((size_t)par * gridDim.x + blockIdx.x) * (2 + P.w);
+  if(threadIdx.x == 0) {
+    slot[0] = v;
+    slot[1] = (double)r;
+  }
+  if(r >= 0)
+    for(int c = threadIdx.x; c < P.w; c += blockDim.x)
+      slot[2 + c] = sm[(size_t)c * P.rpb + (r - lo)];
+  if(d >= lo && d < lo + nr)
+    for(int c = threadIdx.x; c < P.w; c += blockDim.x)
+      P.cur[par * P.w + c] = sm[(size_t)c * P.rpb + (d - lo)];
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kSmemLeafThreads) leaf_smem_kernel(LeafParams<T> P) {
+  extern __shared__ __align__(16) unsigned char leaf_raw[];
+  T* sm = reinterpret_cast<T*>(leaf_raw);
+  __shared__ double s_v[32];
+  __shared__ int    s_r[32];
+  __shared__ double s_u[kSmemLeafW];
+  __shared__ double s_cur[kSmemLeafW];
+  __shared__ double s_piv;
+  __shared__ int    s_p;
+
+  const int    G  = gridDim.x;
+  const int    R  = P.rpb;
+  const int    lo = P.r0 + blockIdx.x * R;
+  const int    nr = max(0, min(P.end, lo + R) - lo);
+  const size_t ld = (size_t)P.ld;
+
+  for(int c = 0; c < P.w; ++c)
+    for(int i = threadIdx.x; i < nr; i += blockDim.x)
+      sm[(size_t)c * R + i] = P.A[(size_t)(lo + i) + (size_t)(P.c0 + c) * ld];
+  __syncthreads();
+
+  leaf_smem_publish(P, sm, lo, nr, 0, 0, s_v, s_r);
+  if(!grid_sync(P.bar, G, P.status, 13)) return;
+
+  for(int k = 0; k < P.w; ++k) {
+    const int par = k & 1;
+    const int d   = P.r0 + k;
+    if(threadIdx.x < 32) {
+      double v = 0.0;
+      int    r = -1, slot = -1;
+      for(int b = threadIdx.x; b < G; b += 32) {
+        const double* sl = P.cand + ((size_t)par * G + b) * (2 + P.w);
+        const double  sv = __ldcg(sl);
+        const int     sr = (int)__ldcg(sl + 1);
+        if(better(sv, sr, v, r)) {
+          v    = sv;
+          r    = sr;
+          slot = b;
+        }
+      }
+#pragma unroll
+      for(int off = 16; off > 0; off >>= 1) {
+        const double ov   = __shfl_down_sync(0xffffffffu, v, off);
+        const int    orow = __shfl_down_sync(0xffffffffu, r, off);
+        const int    os   = __shfl_down_sync(0xffffffffu, slot, off);
+        if(better(ov, orow, v, r)) {
+          v    = ov;
+          r    = orow;
+          slot = os;
+        }
+      }
+      slot = __shfl_sync(0xffffffffu, slot, 0);
+      if(slot < 0) {  // unreachable while the leaf has rows >= d; keeps reads in bounds
+        slot = 0;
+        v    = 0.0;
+        r    = d;
+      }
+      if(threadIdx.x == 0) {
+        s_piv = v;
+        s_p   = r;
+      }
+      const double* sl = P.cand + ((size_t)par * G + slot) * (2 + P.w);
+      if(threadIdx.x < P.w) {
+        s_u[threadIdx.x]   = __ldcg(sl + 2 + threadIdx.x);
+        s_cur[threadIdx.x] = __ldcg(P.cur + par * P.w + threadIdx.x);
+      }
+    }
+    __syncthreads();
+    const T   piv = (T)s_piv;
+    const int p   = s_p;
+    if(blockIdx.x == 0 && threadIdx.x == 0) {
+      P.ipiv[P.c0 + k] = p;
+      if(piv == (T)0) record_info(P.status, P.c0 + k + 1);
+    }
+    if(p != d && p >= lo && p < lo + nr && threadIdx.x < P.w)
+      sm[(size_t)threadIdx.x * R + (p - lo)] = (T)s_cur[threadIdx.x];
+    if(d >= lo && d < lo + nr && threadIdx.x < P.w)
+      sm[(size_t)threadIdx.x * R + (d - lo)] = (T)s_u[threadIdx.x];
+    __syncthreads();
+    // Scale the column below the diagonal and update the remaining columns.
+    // The row's values are loaded before any is stored, so the loads issue
+    // back to back.
+    for(int i = max(0, d + 1 - lo) + threadIdx.x; i < nr; i += blockDim.x) {
+      const T l = sm[(size_t)k * R + i] / piv;
+      sm[(size_t)k * R + i] = l;
+      T x[kSmemLeafW];
+#pragma unroll
+      for(int cc = 0; cc < kSmemLeafW; ++cc)
+        if(cc > k && cc < P.w) x[cc] = sm[(size_t)cc * R + i];
+#pragma unroll
+      for(int cc = 0; cc < kSmemLeafW; ++cc)
+        if(cc > k && cc < P.w) sm[(size_t)cc * R + i] = x[cc] - l * (T)s_u[cc];
+    }
+    if(k + 1 == P.w) break;
+    __syncthreads();
+    leaf_smem_publish(P, sm, lo, nr, k + 1, par ^ 1, s_v, s_r);
+    if(!grid_sync(P.bar, G, P.status, 14)) return;
+  }
+  __syncthreads();
+  for(int c = 0; c < P.w; ++c)
+    for(int i = threadIdx.x; i < nr; i += blockDim.x)
+      P.A[(size_t)(lo + i) + (size_t)(P.c0 + c) * ld] = sm[(size_t)c * R + i];
 }
 
 // Apply the w interchanges of leaf columns [c0, c0+w) to the panel columns
@@ -441,10 +589,76 @@ int leaf_grid_size(int num_sms, int rows) {
   return g;
 }
 
+// Largest dynamic shared memory the resident-slice leaf may take (bytes), set
+// once per element type.
+template <typename T>
+static int leaf_smem_budget() {
+  static int budget = -1;
+  if(budget < 0) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, leaf_smem_kernel<T>);
+    int b = optin - (int)fa.sharedSizeBytes - 1024;
+    if(b < 0 ||
+       cudaFuncSetAttribute(leaf_smem_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, b) !=
+           cudaSuccess) {
+      cudaGetLastError();
+      b = 0;
+    }
+    budget = b;
+  }
+  return budget;
+}
+
+static bool leaf_smem_disabled() {
+  static const bool off = [] {
+    const char* e = getenv("HPLB_LEAF");
+    return e && strcmp(e, "global") == 0;
+  }();
+  return off;
+}
+
 template <typename T>
 cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
                         double* cand, double* cur, int* bar, int* status, int grid,
                         cudaStream_t stream) {
+  const int rows = end - r0;
+  // Resident-slice leaf: as few blocks as hold the leaf in shared memory (one
+  // per SM at most), so the barrier is short and the kernel leaves most SMs
+  // to the trailing update running beside it.
+  if(w <= kSmemLeafW && rows > 0 && !leaf_smem_disabled()) {
+    const int budget = leaf_smem_budget<T>();
+    const int rmax   = budget / (w * (int)sizeof(T));
+    int       dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if(rmax >= 32) {
+      const int g = (rows + rmax - 1) / rmax;
+      if(g <= sms && g <= grid) {
+        LeafParams<T> P;
+        P.A      = A;
+        P.ld     = ld;
+        P.r0     = r0;
+        P.end    = end;
+        P.c0     = c0;
+        P.w      = w;
+        P.rpb    = (rows + g - 1) / g;
+        P.ipiv   = ipiv;
+        P.cand   = cand;
+        P.cur    = cur;
+        P.bar    = bar;
+        P.status = status;
+        cudaError_t e = cudaMemsetAsync(bar, 0, 2 * sizeof(int), stream);
+        if(e != cudaSuccess) return e;
+        void* args[] = {&P};
+        return cudaLaunchCooperativeKernel((const void*)leaf_smem_kernel<T>, dim3(g),
+                                           dim3(kSmemLeafThreads), args,
+                                           (size_t)P.rpb * w * sizeof(T), stream);
+      }
+    }
+  }
   LeafParams<T> P;
   P.A = A;
   P.ld = ld;

@@ -36,7 +36,8 @@ def _factor(hlib, A, nb, nbmin=16):
 
 
 @pytest.mark.parametrize("n,nb,nrhs", [(1, 1, 1), (100, 32, 1), (300, 64, 7), (1000, 128, 32),
-                                       (1005, 100, 3), (2048, 256, 64), (777, 96, 16)])
+                                       (1005, 100, 3), (2048, 256, 64), (777, 96, 16),
+                                       (64, 16, 4), (64, 8, 4), (200, 16, 3)])
 @pytest.mark.parametrize("trans", [0, 1])
 def test_getrs_matches_numpy(hlib, oracle, n, nb, nrhs, trans):
     A, B = _lcg_system(oracle, n, nrhs)
