@@ -24,8 +24,12 @@ __all__ = ["HplSolve", "hpl_solve"]
 
 def _colmajor(M: torch.Tensor) -> torch.Tensor:
     """Column-major copy of a 2-D tensor: returns T with T[j, i] = M[i, j],
-    i.e. M stored column by column with leading dimension M.shape[0]."""
-    return M.t().contiguous()
+    i.e. M stored column by column with leading dimension M.shape[0].  Always
+    a new buffer (the solve overwrites it): for an M that is already
+    column-major, M.t().contiguous() would return M's own storage."""
+    out = torch.empty((M.shape[1], M.shape[0]), dtype=M.dtype, device=M.device)
+    out.copy_(M.t())
+    return out
 
 
 class HplSolve(torch.autograd.Function):

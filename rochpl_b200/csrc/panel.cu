@@ -144,7 +144,7 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(LeafParams<T> P) {
   const size_t ld = (size_t)P.ld;
 
   leaf_publish(P, 0, 0, s_v, s_r);
-  if(!grid_sync(P.bar, G, P.status, 11)) return;
+  if(!grid_sync(P.bar, G, 1, P.status, 11)) return;
 
   for(int k = 0; k < P.w; ++k) {
     const int par = k & 1;
@@ -221,7 +221,7 @@ __global__ void __launch_bounds__(kLeafThreads) leaf_kernel(LeafParams<T> P) {
     if(k + 1 == P.w) break;
     __syncthreads();
     leaf_publish(P, k + 1, par ^ 1, s_v, s_r);
-    if(!grid_sync(P.bar, G, P.status, 12)) return;
+    if(!grid_sync(P.bar, G, k + 2, P.status, 12)) return;
   }
 }
 
@@ -289,7 +289,7 @@ __global__ void __launch_bounds__(kSmemLeafThreads) leaf_smem_kernel(LeafParams<
   __syncthreads();
 
   leaf_smem_publish(P, sm, lo, nr, 0, 0, s_v, s_r);
-  if(!grid_sync(P.bar, G, P.status, 13)) return;
+  if(!grid_sync(P.bar, G, 1, P.status, 13)) return;
 
   for(int k = 0; k < P.w; ++k) {
     const int par = k & 1;
@@ -363,7 +363,7 @@ __global__ void __launch_bounds__(kSmemLeafThreads) leaf_smem_kernel(LeafParams<
     if(k + 1 == P.w) break;
     __syncthreads();
     leaf_smem_publish(P, sm, lo, nr, k + 1, par ^ 1, s_v, s_r);
-    if(!grid_sync(P.bar, G, P.status, 14)) return;
+    if(!grid_sync(P.bar, G, k + 2, P.status, 14)) return;
   }
   __syncthreads();
   for(int c = 0; c < P.w; ++c)

@@ -182,3 +182,23 @@ def test_hpl_solve_vector_rhs_and_errors(hlib, oracle):
         hpl_solve(tA.float(), torch.tensor(B, device="cuda").float())
     with pytest.raises(ValueError):
         hpl_solve(tA.cpu(), torch.tensor(B))
+
+
+def test_hpl_solve_leaves_column_major_inputs_untouched(hlib, oracle):
+    """A and B that are already column-major (strides (1, n), as a tensor made
+    from a Fortran-ordered array is) must be copied, not solved in place."""
+    import torch
+
+    from rochpl_b200.autograd import hpl_solve
+
+    n = 80
+    A, B = _lcg_system(oracle, n, 3)
+    tA = torch.tensor(np.asfortranarray(A), device="cuda")
+    tB = torch.tensor(np.asfortranarray(B), device="cuda")
+    assert tB.stride() == (1, n) and tA.stride() == (1, n)
+    A0, B0 = tA.clone(), tB.clone()
+    ref = np.linalg.solve(A, B)
+    for _ in range(2):
+        X = hpl_solve(tA, tB, nb=16)
+        assert torch.equal(tA, A0) and torch.equal(tB, B0)
+        assert np.allclose(X.cpu().numpy(), ref, rtol=1e-10, atol=1e-12)
