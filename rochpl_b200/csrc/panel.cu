@@ -371,6 +371,148 @@ __global__ void __launch_bounds__(kSmemLeafThreads) leaf_smem_kernel(LeafParams<
       P.A[(size_t)(lo + i) + (size_t)(P.c0 + c) * ld] = sm[(size_t)c * R + i];
 }
 
+// Leaf with every row in registers: thread t of block b owns rows
+// r0 + b * rpb + t + q * blockDim.x (q < RPT) across all w <= 32 leaf
+// columns.  The column loop is unrolled, so step k updates exactly columns
+// k+1 .. w-1 of the thread's rows without shared-memory traffic; a column
+// step costs the pivot search, one bounded grid barrier and two 32-word
+// reads (pivot row, old diagonal row).  Arithmetic identical to leaf_kernel
+// (division by the pivot, a_cc - l * u_cc), hence identical bits.
+constexpr int kRegLeafW       = 32;
+constexpr int kRegLeafThreads = 256;
+
+template <typename T, int RPT>
+__global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams<T> P) {
+  __shared__ double s_v[32];
+  __shared__ int    s_r[32];
+  __shared__ double s_u[kRegLeafW];
+  __shared__ double s_cur[kRegLeafW];
+  __shared__ double s_piv;
+  __shared__ int    s_p;
+
+  const int    G  = gridDim.x;
+  const int    lo = P.r0 + blockIdx.x * P.rpb;
+  const size_t ld = (size_t)P.ld;
+  const int    w  = P.w;
+
+  T   x[RPT][kRegLeafW];
+  int row[RPT];
+#pragma unroll
+  for(int q = 0; q < RPT; ++q) {
+    row[q]         = lo + threadIdx.x + q * blockDim.x;
+    const bool in  = row[q] < P.end && threadIdx.x + q * blockDim.x < P.rpb;
+    if(!in) row[q] = -1;
+#pragma unroll
+    for(int c = 0; c < kRegLeafW; ++c)
+      x[q][c] = (in && c < w) ? P.A[(size_t)row[q] + (size_t)(P.c0 + c) * ld] : (T)0;
+  }
+
+#pragma unroll
+  for(int k = 0; k < kRegLeafW; ++k) {
+    if(k >= w) break;
+    const int par = k & 1;
+    const int d   = P.r0 + k;
+    // This block's candidate among its rows >= d, and the rows it must publish.
+    double v = 0.0;
+    int    r = -1;
+#pragma unroll
+    for(int q = 0; q < RPT; ++q)
+      if(row[q] >= d && better((double)x[q][k], row[q], v, r)) {
+        v = x[q][k];
+        r = row[q];
+      }
+    block_argmax(v, r, s_v, s_r);
+    double* slot = P.cand + ((size_t)par * G + blockIdx.x) * (2 + w);
+    if(threadIdx.x == 0) {
+      slot[0] = v;
+      slot[1] = (double)r;
+    }
+#pragma unroll
+    for(int q = 0; q < RPT; ++q) {
+      if(r >= 0 && row[q] == r)
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c)
+          if(c < w) slot[2 + c] = x[q][c];
+      if(row[q] == d)
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c)
+          if(c < w) P.cur[par * w + c] = x[q][c];
+    }
+    if(!grid_sync(P.bar, G, k + 1, P.status, 15)) return;
+
+    if(threadIdx.x < 32) {
+      double bv = 0.0;
+      int    br = -1, bs = -1;
+      for(int b = threadIdx.x; b < G; b += 32) {
+        const double* sl = P.cand + ((size_t)par * G + b) * (2 + w);
+        const double  sv = __ldcg(sl);
+        const int     sr = (int)__ldcg(sl + 1);
+        if(better(sv, sr, bv, br)) {
+          bv = sv;
+          br = sr;
+          bs = b;
+        }
+      }
+#pragma unroll
+      for(int off = 16; off > 0; off >>= 1) {
+        const double ov   = __shfl_down_sync(0xffffffffu, bv, off);
+        const int    orow = __shfl_down_sync(0xffffffffu, br, off);
+        const int    os   = __shfl_down_sync(0xffffffffu, bs, off);
+        if(better(ov, orow, bv, br)) {
+          bv = ov;
+          br = orow;
+          bs = os;
+        }
+      }
+      bs = __shfl_sync(0xffffffffu, bs, 0);
+      if(bs < 0) {  // unreachable while the leaf has rows >= d; keeps reads in bounds
+        bs = 0;
+        bv = 0.0;
+        br = d;
+      }
+      if(threadIdx.x == 0) {
+        s_piv = bv;
+        s_p   = br;
+      }
+      const double* sl = P.cand + ((size_t)par * G + bs) * (2 + w);
+      if(threadIdx.x < w) {
+        s_u[threadIdx.x]   = __ldcg(sl + 2 + threadIdx.x);
+        s_cur[threadIdx.x] = __ldcg(P.cur + par * w + threadIdx.x);
+      }
+    }
+    __syncthreads();
+    const T   piv = (T)s_piv;
+    const int p   = s_p;
+    if(blockIdx.x == 0 && threadIdx.x == 0) {
+      P.ipiv[P.c0 + k] = p;
+      if(piv == (T)0) record_info(P.status, P.c0 + k + 1);
+    }
+#pragma unroll
+    for(int q = 0; q < RPT; ++q) {
+      if(row[q] == d) {
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_u[c];
+      } else if(row[q] == p) {
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_cur[c];
+      }
+      if(row[q] > d) {
+        const T l = x[q][k] / piv;
+        x[q][k]   = l;
+#pragma unroll
+        for(int cc = k + 1; cc < kRegLeafW; ++cc) x[q][cc] = x[q][cc] - l * (T)s_u[cc];
+      }
+    }
+  }
+
+#pragma unroll
+  for(int q = 0; q < RPT; ++q)
+    if(row[q] >= 0)
+#pragma unroll
+      for(int c = 0; c < kRegLeafW; ++c)
+        if(c < w) P.A[(size_t)row[q] + (size_t)(P.c0 + c) * ld] = x[q][c];
+}
+
 // Apply the w interchanges of leaf columns [c0, c0+w) to the panel columns
 // outside the leaf, in order.  One thread per column.
 template <typename T>
@@ -612,12 +754,50 @@ static int leaf_smem_budget() {
   return budget;
 }
 
-static bool leaf_smem_disabled() {
-  static const bool off = [] {
+// Leaf kernel choice: registers (default), "smem" or "global" (HPLB_LEAF), the
+// latter two kept for comparison; each falls through to the next when the
+// leaf does not fit.
+static int leaf_mode() {
+  static const int mode = [] {
     const char* e = getenv("HPLB_LEAF");
-    return e && strcmp(e, "global") == 0;
+    if(e && strcmp(e, "global") == 0) return 2;
+    if(e && strcmp(e, "smem") == 0) return 1;
+    return 0;
   }();
-  return off;
+  return mode;
+}
+
+template <typename T, int RPT>
+static cudaError_t launch_leaf_reg(LeafParams<T> P, int g, cudaStream_t stream) {
+  P.rpb         = RPT * kRegLeafThreads;
+  cudaError_t e = cudaMemsetAsync(P.bar, 0, 2 * sizeof(int), stream);
+  if(e != cudaSuccess) return e;
+  void* args[] = {&P};
+  return cudaLaunchCooperativeKernel((const void*)leaf_reg_kernel<T, RPT>, dim3(g),
+                                     dim3(kRegLeafThreads), args, 0, stream);
+}
+
+// Rows per thread the register leaf is built for: the smallest that puts the
+// leaf on at most one block per SM (3 x 32 doubles or 4 x 32 floats per
+// thread fill the register file of a 256-thread block without spilling).
+template <typename T>
+static cudaError_t try_leaf_reg(const LeafParams<T>& P, int rows, int sms, int grid,
+                                cudaStream_t stream, bool* done) {
+  constexpr int kMaxRpt = sizeof(T) == 8 ? 3 : 4;
+  *done                 = false;
+  for(int rpt = 1; rpt <= kMaxRpt; ++rpt) {
+    const int cap = rpt * kRegLeafThreads;
+    const int g   = (rows + cap - 1) / cap;
+    if(g > sms || g > grid) continue;
+    *done = true;
+    switch(rpt) {
+      case 1: return launch_leaf_reg<T, 1>(P, g, stream);
+      case 2: return launch_leaf_reg<T, 2>(P, g, stream);
+      case 3: return launch_leaf_reg<T, 3>(P, g, stream);
+      default: return launch_leaf_reg<T, kMaxRpt>(P, g, stream);
+    }
+  }
+  return cudaSuccess;
 }
 
 template <typename T>
@@ -625,15 +805,32 @@ cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* i
                         double* cand, double* cur, int* bar, int* status, int grid,
                         cudaStream_t stream) {
   const int rows = end - r0;
+  int       dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if(w <= kRegLeafW && rows > 0 && leaf_mode() == 0) {
+    LeafParams<T> P;
+    P.A      = A;
+    P.ld     = ld;
+    P.r0     = r0;
+    P.end    = end;
+    P.c0     = c0;
+    P.w      = w;
+    P.rpb    = 0;
+    P.ipiv   = ipiv;
+    P.cand   = cand;
+    P.cur    = cur;
+    P.bar    = bar;
+    P.status = status;
+    bool              done = false;
+    const cudaError_t e    = try_leaf_reg<T>(P, rows, sms, grid, stream, &done);
+    if(done) return e;
+  }
   // Resident-slice leaf: as few blocks as hold the leaf in shared memory (one
-  // per SM at most), so the barrier is short and the kernel leaves most SMs
-  // to the trailing update running beside it.
-  if(w <= kSmemLeafW && rows > 0 && !leaf_smem_disabled()) {
+  // per SM at most).
+  if(w <= kSmemLeafW && rows > 0 && leaf_mode() <= 1) {
     const int budget = leaf_smem_budget<T>();
     const int rmax   = budget / (w * (int)sizeof(T));
-    int       dev = 0, sms = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if(rmax >= 32) {
       const int g = (rows + rmax - 1) / rmax;
       if(g <= sms && g <= grid) {
