@@ -138,6 +138,61 @@ hplb_status hplb_rank_k(hplb_ctx* ctx, int m, int n, int k, double alpha, const 
                         int64_t lda, const double* dB, int64_t ldb, double* dC, int64_t ldc,
                         int accumulate);
 
+/* ---------------------------------------------------------------------------
+ * Batched form (no counterpart in the reference, which solves one system per
+ * run).  Many independent systems of uneven size, system i being n[i] x n[i]
+ * with nrhs[i] right-hand sides, solved in one persistent, graph-captured
+ * launch: one CTA per system at a time, largest first, right-looking blocked
+ * LU with partial pivoting (full-row interchanges, as LAPACK's getrf, so P A =
+ * L U), the panel width from the system's size class.
+ *
+ * Layout (device pools, all column-major, packed in system order): A_i at
+ * a_off[i] with leading dimension n[i]; B_i (n[i] x nrhs[i]) at b_off[i] with
+ * leading dimension n[i]; pivots at p_off[i] (n[i] ints, 0-based row swapped
+ * into each row, as LAPACK's ipiv minus one).
+ * ------------------------------------------------------------------------ */
+#define HPLB_BATCH_CLASSES 6   /* size classes: n < 48, < 96, < 192, < 384, < 768, >= 768 */
+#define HPLB_BATCH_MAX_N 2048
+
+typedef struct hplb_batch hplb_batch;
+
+/* Plan a batch (host arrays n, nrhs of length count).  nb_by_class: panel
+ * width (8, 16 or 32) per size class, e.g. from hplb_batch_tune; NULL for the
+ * built-in table.  Widths are lowered where a panel would not fit in shared
+ * memory. */
+hplb_status hplb_batch_create(hplb_ctx* ctx, int count, const int* n, const int* nrhs,
+                              const int* nb_by_class, hplb_batch** out);
+void        hplb_batch_destroy(hplb_batch* b);
+/* Pool sizes (elements) and, when the arrays are not NULL, every system's
+ * offsets and panel width (host arrays of length count). */
+hplb_status hplb_batch_layout(const hplb_batch* b, int64_t* a_elems, int64_t* b_elems,
+                              int64_t* p_elems, int64_t* a_off, int64_t* b_off, int64_t* p_off,
+                              int* nb);
+/* [A_i | B_i] = the HPL LCG matrix of seeds[i] (host array), n[i] x (n[i] +
+ * nrhs[i]) with n[i] rows: the first n[i] columns go to A_i, the rest to B_i. */
+hplb_status hplb_batch_matgen(hplb_batch* b, const uint64_t* seeds, double* dA, double* dB);
+/* Factor every A_i in place (L and U), overwrite B_i with X_i = A_i^-1 B_i,
+ * pivots to dipiv, first zero pivot (1-based, 0 if none) to dinfo[i]. */
+hplb_status hplb_batch_gesv(hplb_batch* b, double* dA, double* dB, int* dipiv, int* dinfo);
+/* With the factors and pivots of hplb_batch_gesv: B_i <- A_i^-1 B_i (trans = 0)
+ * or A_i^-T B_i (trans = 1). */
+hplb_status hplb_batch_getrs(hplb_batch* b, int trans, const double* dLU, const int* dipiv,
+                             double* dB);
+/* C_i = alpha X_i Y_i^T (X_i, Y_i in the B layout, C_i in the A layout). */
+hplb_status hplb_batch_rank_k(hplb_batch* b, double alpha, const double* dX, const double* dY,
+                              double* dC);
+/* dresid[i] (device) = the HPL scaled residual of X_i against the regenerated
+ * LCG system of seeds[i], the largest over its right-hand sides. */
+hplb_status hplb_batch_residual(hplb_batch* b, const uint64_t* seeds, const double* dX,
+                                double* dresid);
+/* Device time of the last batch call (ms). */
+hplb_status hplb_batch_last_ms(const hplb_batch* b, double* ms);
+/* The autotuner: times panel widths 8 / 16 / 32 on a batch of each size class
+ * (2 x SM-count systems, nrhs right-hand sides) and writes the fastest to
+ * nb_by_class; ms_table (6 x 3, may be NULL) receives every timing, -1 where a
+ * width does not fit. */
+hplb_status hplb_batch_tune(hplb_ctx* ctx, int nrhs, int* nb_by_class, double* ms_table);
+
 /* The HPL residual check: dA must hold the regenerated [A|b] (hplb_matgen with
  * the seed of the solve), dX the solution.  Results go to *out (host). */
 hplb_status hplb_residual(hplb_ctx* ctx, int n, const double* dA, int64_t ld,

@@ -1,0 +1,816 @@
+// Batched FP64 LU + solve of many independent systems of uneven size in one
+// persistent launch (no counterpart in the reference, whose solve is a single
+// system; the per-system algorithm is the right-looking blocked LU with
+// partial pivoting of HPL_pdgesv, with LAPACK's full-row interchanges so that
+// the right-hand sides ride along as extra columns).
+//
+// One CTA (kBT threads) owns one system at a time and takes the next one from
+// a work counter; the plan orders systems by descending cost so the large ones
+// start first.  Per panel of nb columns (nb from the plan's size class):
+//   panel      the m x kb panel is factored in shared memory (pivot search by
+//              warp shuffles and a block reduction, division by the pivot, rank-1
+//              updates inside the panel), then written back;
+//   swaps      the panel's interchanges applied to the other columns of A and to B;
+//   trsm       U12 = L11^-1 A12 (and B's rows), one column per thread;
+//   update     A22 -= L21 U12 and B2 -= L21 U12_B on the FP64 tensor cores
+//              (DMMA m16n8k8) from 64 x 64 tiles staged in shared memory.
+// Then U X = B by blocks (substitution on the diagonal blocks, DMMA updates).
+// The stored-factor solves (plain and transposed), the batched rank-k product
+// of the adjoint, the per-system LCG generator and the per-system HPL residual
+// use the same CTA-per-system loop.
+#include "common.cuh"
+#include "internal.h"
+#include "lcg.cuh"
+
+namespace hplb {
+
+namespace {
+
+constexpr int kBT    = 512;  // threads per CTA
+constexpr int kBW    = kBT / 32;
+constexpr int kNbMax = 32;   // widest panel
+constexpr int kTile  = 64;   // output tile of the block updates
+constexpr int kLdT   = kTile + 4;
+
+struct Sys {
+  int       n, nrhs, nb, pad;
+  long long a_off, b_off, p_off;
+};
+
+struct Args {
+  double*       A;      // A pool (factored in place), or null
+  const double* LU;     // stored factors (solve-only modes)
+  double*       B;      // B pool (overwritten by X)
+  int*          ipiv;   // pivot pool (global row within the system, 0-based)
+  const int*    ipivc;  // stored pivots (solve-only modes)
+  int*          info;   // per system: first zero pivot (1-based) or 0
+  const Sys*    sys;    // descriptors
+  const int*    order;  // work order
+  int           count;
+  int*          counter;
+  double        alpha;  // rank-k scale
+  const double* X;      // rank-k operands (B-pool layout)
+  const double* Y;
+  double*       C;      // rank-k output (A-pool layout)
+  const unsigned long long* seeds;  // generator / residual
+  double*       resid;  // per system HPL scaled residual (max over its RHS)
+};
+
+// Shared scratch of every mode.  The panel P is [kb][ldp] column-major.
+struct Smem {
+  double red_v[kBW];
+  int    red_r[kBW];
+  int    piv[kNbMax];
+  int    src[kNbMax];  // new top row x came from row src[x] (panel-local)
+  int    dst[kNbMax];  // old top row x went to row dst[x], or -1 if it stayed on top
+  int    next;
+  int    info;
+  double As[kNbMax][kLdT];  // A tile: k x rows
+  double Bs[kTile][kNbMax + 2];  // B tile: cols x k
+  double D[kNbMax][kNbMax + 1];  // a diagonal block
+};
+
+HPLB_DEV bool better_b(double av, int ar, double bv, int br) {
+  if(br < 0) return ar >= 0;
+  if(ar < 0) return false;
+  const double fa = fabs(av), fb = fabs(bv);
+  if(fa > fb) return true;
+  if(fa < fb) return false;
+  return ar < br;
+}
+
+HPLB_DEV void argmax_block(double& v, int& r, Smem& S) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for(int off = 16; off > 0; off >>= 1) {
+    const double ov = __shfl_down_sync(0xffffffffu, v, off);
+    const int    orr = __shfl_down_sync(0xffffffffu, r, off);
+    if(better_b(ov, orr, v, r)) {
+      v = ov;
+      r = orr;
+    }
+  }
+  __syncthreads();
+  if(lane == 0) {
+    S.red_v[warp] = v;
+    S.red_r[warp] = r;
+  }
+  __syncthreads();
+  if(warp == 0) {
+    v = lane < kBW ? S.red_v[lane] : 0.0;
+    r = lane < kBW ? S.red_r[lane] : -1;
+#pragma unroll
+    for(int off = 16; off > 0; off >>= 1) {
+      const double ov = __shfl_down_sync(0xffffffffu, v, off);
+      const int    orr = __shfl_down_sync(0xffffffffu, r, off);
+      if(better_b(ov, orr, v, r)) {
+        v = ov;
+        r = orr;
+      }
+    }
+    if(lane == 0) {
+      S.red_v[0] = v;
+      S.red_r[0] = r;
+    }
+  }
+  __syncthreads();
+  v = S.red_v[0];
+  r = S.red_r[0];
+  __syncthreads();
+}
+
+HPLB_DEV void dmma(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 "
+      "{%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+      : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+      : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b[0]), "d"(b[1]));
+}
+
+// C (m x n) -= A (m x k) B (k x n), k <= kNbMax, all column-major in global
+// memory, by 64 x 64 tiles: A and B slices staged in shared memory (zero
+// padded to a multiple of 8 in k), C accumulated in DMMA fragments.  16 warps:
+// 4 x 4, each 16 rows x 16 columns (two m16n8 tiles).  Fragment layout
+// (g = lane / 4, t = lane % 4): A a0 (g, t) a1 (g+8, t) a2 (g, t+4)
+// a3 (g+8, t+4); B b0 (t, g) b1 (t+4, g); C c0 (g, 2t) c1 (g, 2t+1)
+// c2 (g+8, 2t) c3 (g+8, 2t+1).
+HPLB_DEV void tile_gemm_sub(int m, int n, int k, const double* A, int64_t lda, const double* B,
+                            int64_t ldb, double* C, int64_t ldc, Smem& S) {
+  if(m <= 0 || n <= 0 || k <= 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 3) * 16, wn = (warp >> 2) * 16;
+  const int k8 = (k + 7) & ~7;
+  const int tm = (m + kTile - 1) / kTile, tn = (n + kTile - 1) / kTile;
+  for(int tile = 0; tile < tm * tn; ++tile) {
+    const int m0 = (tile % tm) * kTile, n0 = (tile / tm) * kTile;
+    __syncthreads();
+    for(int idx = threadIdx.x; idx < k8 * kTile; idx += kBT) {
+      const int r = idx % kTile, kk = idx / kTile;
+      S.As[kk][r] = (kk < k && m0 + r < m) ? A[(size_t)(m0 + r) + (size_t)kk * lda] : 0.0;
+      const int c = idx / k8, k2 = idx % k8;
+      S.Bs[c][k2] = (k2 < k && n0 + c < n) ? B[(size_t)k2 + (size_t)(n0 + c) * ldb] : 0.0;
+    }
+    __syncthreads();
+    double acc[2][4];
+#pragma unroll
+    for(int j = 0; j < 2; ++j)
+#pragma unroll
+      for(int q = 0; q < 4; ++q) acc[j][q] = 0.0;
+    for(int kk = 0; kk < k8; kk += 8) {
+      double af[4], bf[2][2];
+      af[0] = S.As[kk + t][wm + g];
+      af[1] = S.As[kk + t][wm + g + 8];
+      af[2] = S.As[kk + t + 4][wm + g];
+      af[3] = S.As[kk + t + 4][wm + g + 8];
+#pragma unroll
+      for(int j = 0; j < 2; ++j) {
+        bf[j][0] = S.Bs[wn + j * 8 + g][kk + t];
+        bf[j][1] = S.Bs[wn + j * 8 + g][kk + t + 4];
+      }
+#pragma unroll
+      for(int j = 0; j < 2; ++j) dmma(acc[j], af, bf[j]);
+    }
+#pragma unroll
+    for(int j = 0; j < 2; ++j)
+#pragma unroll
+      for(int q = 0; q < 4; ++q) {
+        const int r = m0 + wm + g + (q >> 1) * 8;
+        const int c = n0 + wn + j * 8 + 2 * t + (q & 1);
+        if(r < m && c < n) {
+          double* p = C + (size_t)r + (size_t)c * ldc;
+          *p -= acc[j][q];
+        }
+      }
+  }
+  __syncthreads();
+}
+
+// C (m x n) -= A^T B with A (k x m), B (k x n), m <= kNbMax, n arbitrary:
+// k-chunks of 64 of A and of B staged in shared memory; thread (i, c) keeps its
+// outputs in registers across the chunks.  For the transposed solves.
+HPLB_DEV void tile_gemm_tn_sub(int m, int n, int k, const double* A, int64_t lda,
+                               const double* B, int64_t ldb, double* C, int64_t ldc, Smem& S) {
+  if(m <= 0 || n <= 0 || k <= 0) return;
+  for(int n0 = 0; n0 < n; n0 += kTile) {
+    const int nc = min(kTile, n - n0);
+    // thread -> (i = idx % m, c = idx / m) for idx = threadIdx.x + s * kBT
+    double acc[4] = {0.0, 0.0, 0.0, 0.0};
+    for(int k0 = 0; k0 < k; k0 += kTile) {
+      const int kc = min(kTile, k - k0);
+      __syncthreads();
+      // As[i][kk] (i < m <= 32, kk < 64) reuses As as [kNbMax][kLdT]
+      for(int idx = threadIdx.x; idx < kNbMax * kTile; idx += kBT) {
+        const int i = idx / kTile, kk = idx % kTile;
+        S.As[i][kk] = (i < m && kk < kc) ? A[(size_t)(k0 + kk) + (size_t)i * lda] : 0.0;
+      }
+      // Bs[c][kk] for c < 64, kk < 32: two halves of the 64-long chunk
+      for(int half = 0; half < 2; ++half) {
+        __syncthreads();
+        for(int idx = threadIdx.x; idx < kTile * kNbMax; idx += kBT) {
+          const int c = idx / kNbMax, kk = idx % kNbMax;
+          const int kg = half * kNbMax + kk;
+          S.Bs[c][kk] = (c < nc && kg < kc) ? B[(size_t)(k0 + kg) + (size_t)(n0 + c) * ldb] : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for(int s = 0; s < 4; ++s) {
+          const int idx = threadIdx.x + s * kBT;
+          const int i = idx % kNbMax, c = idx / kNbMax;
+          if(i < m && c < nc) {
+            double a = acc[s];
+            for(int kk = 0; kk < kNbMax; ++kk) a += S.As[i][half * kNbMax + kk] * S.Bs[c][kk];
+            acc[s] = a;
+          }
+        }
+      }
+    }
+#pragma unroll
+    for(int s = 0; s < 4; ++s) {
+      const int idx = threadIdx.x + s * kBT;
+      const int i = idx % kNbMax, c = idx / kNbMax;
+      if(i < m && c < nc) C[(size_t)i + (size_t)(n0 + c) * ldc] -= acc[s];
+    }
+  }
+  __syncthreads();
+}
+
+// S.D <- the kb x kb diagonal block at A (leading dimension lda).
+HPLB_DEV void load_diag(const double* A, int64_t lda, int kb, Smem& S) {
+  __syncthreads();
+  for(int idx = threadIdx.x; idx < kb * kb; idx += kBT) {
+    const int r = idx % kb, c = idx / kb;
+    S.D[r][c] = A[(size_t)r + (size_t)c * lda];
+  }
+  __syncthreads();
+}
+
+// Substitution with S.D on n columns of X (kb rows, leading dimension ldx),
+// one column per thread:
+//   LOWER_UNIT:      X <- L^-1 X     (unit lower, forward)
+//   UPPER:           X <- U^-1 X     (backward)
+//   UPPER_T:         X <- U^-T X     (U^T lower, forward)
+//   LOWER_UNIT_T:    X <- L^-T X     (L^T unit upper, backward)
+enum { LOWER_UNIT = 0, UPPER = 1, UPPER_T = 2, LOWER_UNIT_T = 3 };
+template <int KIND>
+HPLB_DEV void diag_solve(int kb, double* X, int64_t ldx, int n, const Smem& S) {
+  for(int c = threadIdx.x; c < n; c += kBT) {
+    double  x[kNbMax];
+    double* col = X + (size_t)c * ldx;
+#pragma unroll
+    for(int r = 0; r < kNbMax; ++r) x[r] = r < kb ? col[r] : 0.0;
+    if(KIND == LOWER_UNIT || KIND == UPPER_T) {
+#pragma unroll
+      for(int r = 0; r < kNbMax; ++r) {
+        if(r < kb) {
+          double s = x[r];
+#pragma unroll
+          for(int q = 0; q < r; ++q) s -= (KIND == LOWER_UNIT ? S.D[r][q] : S.D[q][r]) * x[q];
+          x[r] = KIND == UPPER_T ? s / S.D[r][r] : s;
+        }
+      }
+    } else {
+#pragma unroll
+      for(int r = kNbMax - 1; r >= 0; --r) {
+        if(r < kb) {
+          double s = x[r];
+#pragma unroll
+          for(int q = r + 1; q < kNbMax; ++q)
+            if(q < kb) s -= (KIND == UPPER ? S.D[r][q] : S.D[q][r]) * x[q];
+          x[r] = KIND == UPPER ? s / S.D[r][r] : s;
+        }
+      }
+    }
+#pragma unroll
+    for(int r = 0; r < kNbMax; ++r)
+      if(r < kb) col[r] = x[r];
+  }
+  __syncthreads();
+}
+
+// Take the next system index (or -1), in the plan's order.
+HPLB_DEV int next_system(const Args& a, Smem& S) {
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    const int s = atomicAdd(a.counter, 1);
+    S.next      = s < a.count ? a.order[s] : -1;
+  }
+  __syncthreads();
+  return S.next;
+}
+
+// Factor one system (A n x n, lda = n) and solve for its B (n x nrhs, ldb = n).
+HPLB_DEV void solve_system(const Args& a, const Sys& y, double* P, Smem& S) {
+  const int n = y.n, nrhs = y.nrhs, nb = y.nb;
+  const int ldp = n;
+  double*   A  = a.A + y.a_off;
+  double*   B  = a.B + y.b_off;
+  int*      ip = a.ipiv + y.p_off;
+  if(threadIdx.x == 0) S.info = 0;
+  for(int k0 = 0; k0 < n; k0 += nb) {
+    const int kb = min(nb, n - k0), m = n - k0;
+    // Panel to shared memory.
+    __syncthreads();
+    for(int idx = threadIdx.x; idx < kb * m; idx += kBT) {
+      const int c = idx / m, i = idx % m;
+      P[(size_t)c * ldp + i] = A[(size_t)(k0 + i) + (size_t)(k0 + c) * n];
+    }
+    __syncthreads();
+    for(int j = 0; j < kb; ++j) {
+      double* col = P + (size_t)j * ldp;
+      double  v   = 0.0;
+      int     r   = -1;
+      for(int i = j + threadIdx.x; i < m; i += kBT)
+        if(better_b(col[i], i, v, r)) {
+          v = col[i];
+          r = i;
+        }
+      argmax_block(v, r, S);
+      if(threadIdx.x == 0) {
+        S.piv[j] = r;
+        ip[k0 + j] = k0 + r;
+        if(v == 0.0 && S.info == 0) S.info = k0 + j + 1;
+      }
+      if(r != j && threadIdx.x < kb) {
+        double* pc = P + (size_t)threadIdx.x * ldp;
+        const double tmp = pc[j];
+        pc[j]            = pc[r];
+        pc[r]            = tmp;
+      }
+      __syncthreads();
+      if(v != 0.0)
+        for(int i = j + 1 + threadIdx.x; i < m; i += kBT) {
+          const double l = col[i] / v;
+          col[i]         = l;
+          for(int c = j + 1; c < kb; ++c) {
+            double* pc = P + (size_t)c * ldp;
+            pc[i]      = pc[i] - l * pc[j];
+          }
+        }
+      __syncthreads();
+    }
+    for(int idx = threadIdx.x; idx < kb * m; idx += kBT) {
+      const int c = idx / m, i = idx % m;
+      A[(size_t)(k0 + i) + (size_t)(k0 + c) * n] = P[(size_t)c * ldp + i];
+    }
+    // The panel's interchanges as a row map (each thread x < kb traces one
+    // position through the kb swaps).
+    if(threadIdx.x < kb) {
+      const int x = threadIdx.x;
+      int       pos = x;
+      for(int i = kb - 1; i >= 0; --i) {
+        const int p = S.piv[i];
+        pos         = (pos == i) ? p : (pos == p ? i : pos);
+      }
+      S.src[x] = pos;
+      pos      = x;
+      for(int i = 0; i < kb; ++i) {
+        const int p = S.piv[i];
+        pos         = (pos == i) ? p : (pos == p ? i : pos);
+      }
+      S.dst[x] = pos >= kb ? pos : -1;
+    }
+    load_diag(A + k0 + (size_t)k0 * n, n, kb, S);
+    // Interchanges on every other column of A and on B, and on the columns
+    // right of the panel (and B) the unit-lower solve with L11, fused: each
+    // thread gathers its column's new top rows and displaced rows into
+    // registers before it stores anything.
+    const int rest = n - k0 - kb;
+    const int ncol = k0 + rest + nrhs;
+    for(int q = threadIdx.x; q < ncol; q += kBT) {
+      double* col = q < k0 ? A + (size_t)q * n
+                           : (q < k0 + rest ? A + (size_t)(q + kb) * n : B + (size_t)(q - k0 - rest) * n);
+      col += k0;
+      double x[kNbMax], o[kNbMax];
+#pragma unroll
+      for(int r = 0; r < kNbMax; ++r)
+        if(r < kb) {
+          x[r] = col[S.src[r]];
+          o[r] = S.dst[r] >= 0 ? col[r] : 0.0;
+        }
+#pragma unroll
+      for(int r = 0; r < kNbMax; ++r)
+        if(r < kb && S.dst[r] >= 0) col[S.dst[r]] = o[r];
+      if(q >= k0) {
+#pragma unroll
+        for(int r = 0; r < kNbMax; ++r)
+          if(r < kb) {
+            double t = x[r];
+#pragma unroll
+            for(int c = 0; c < r; ++c) t -= S.D[r][c] * x[c];
+            x[r] = t;
+          }
+      }
+#pragma unroll
+      for(int r = 0; r < kNbMax; ++r)
+        if(r < kb) col[r] = x[r];
+    }
+    __syncthreads();
+    if(rest + nrhs > 0) {
+      // A22 -= L21 U12, B2 -= L21 B1.
+      tile_gemm_sub(rest, rest, kb, A + (k0 + kb) + (size_t)k0 * n, n,
+                    A + k0 + (size_t)(k0 + kb) * n, n, A + (k0 + kb) + (size_t)(k0 + kb) * n, n,
+                    S);
+      tile_gemm_sub(rest, nrhs, kb, A + (k0 + kb) + (size_t)k0 * n, n, B + k0, n, B + (k0 + kb),
+                    n, S);
+    }
+  }
+  // U X = B.
+  for(int k0 = (n - 1) / nb * nb; k0 >= 0; k0 -= nb) {
+    const int kb = min(nb, n - k0);
+    load_diag(A + k0 + (size_t)k0 * n, n, kb, S);
+    diag_solve<UPPER>(kb, B + k0, n, nrhs, S);
+    tile_gemm_sub(k0, nrhs, kb, A + (size_t)k0 * n, n, B + k0, n, B, n, S);
+  }
+  if(threadIdx.x == 0) a.info[&y - a.sys] = S.info;
+}
+
+__global__ void __launch_bounds__(kBT, 1) batch_gesv_kernel(const Args* pa) {
+  extern __shared__ __align__(16) double panel_smem[];
+  __shared__ Smem S;
+  const Args a = *pa;
+  for(;;) {
+    const int s = next_system(a, S);
+    if(s < 0) break;
+    solve_system(a, a.sys[s], panel_smem, S);
+  }
+}
+
+// ---- solves with stored factors ----
+
+// Rows of B (n x nrhs, leading dimension n) permuted by the pivots: forward,
+// B <- P B (the swaps j = 0 .. n-1 in order), or inverse, B <- P^T B.  The
+// permutation is traced once on an index array in shared memory (idx[i] =
+// original row now at position i), then applied as a gather through shared
+// memory, kPermCols columns at a time.
+constexpr int kPermCols = 8;
+HPLB_DEV void permute_rows(const int* ip, int n, double* B, int nrhs, bool inverse, int* idx,
+                           double* T) {
+  for(int i = threadIdx.x; i < n; i += kBT) idx[i] = ip[i];
+  __syncthreads();
+  if(threadIdx.x == 0) {
+    // idx[] holds the pivots; trace positions in place with a second pass.
+    int* pv = idx;
+    // positions are rebuilt into the upper half of the same buffer
+    int* pos = idx + n;
+    for(int i = 0; i < n; ++i) pos[i] = i;
+    for(int j = 0; j < n; ++j) {
+      const int r = pv[j];
+      if(r != j) {
+        const int t = pos[j];
+        pos[j]      = pos[r];
+        pos[r]      = t;
+      }
+    }
+  }
+  __syncthreads();
+  const int* pos = idx + n;
+  for(int c0 = 0; c0 < nrhs; c0 += kPermCols) {
+    const int nc = min(kPermCols, nrhs - c0);
+    for(int e = threadIdx.x; e < nc * n; e += kBT) {
+      const int c = e / n, i = e % n;
+      const double* col = B + (size_t)(c0 + c) * n;
+      if(!inverse)
+        T[(size_t)c * n + i] = col[pos[i]];
+      else
+        T[(size_t)c * n + pos[i]] = col[i];
+    }
+    __syncthreads();
+    for(int e = threadIdx.x; e < nc * n; e += kBT) {
+      const int c = e / n, i = e % n;
+      B[(size_t)i + (size_t)(c0 + c) * n] = T[(size_t)c * n + i];
+    }
+    __syncthreads();
+  }
+}
+
+template <bool TRANS>
+__global__ void __launch_bounds__(kBT, 1) batch_getrs_kernel(const Args* pa) {
+  extern __shared__ __align__(16) double perm_smem[];
+  __shared__ Smem S;
+  const Args a = *pa;
+  for(;;) {
+    const int s = next_system(a, S);
+    if(s < 0) break;
+    const Sys&    y = a.sys[s];
+    const int     n = y.n, nrhs = y.nrhs, nb = y.nb;
+    const double* L = a.LU + y.a_off;
+    double*       B = a.B + y.b_off;
+    const int*    ip = a.ipivc + y.p_off;
+    int*          idx = reinterpret_cast<int*>(perm_smem);
+    double*       T   = perm_smem + n;  // after 2n ints
+    if(!TRANS) {
+      // x = U^-1 L^-1 P b
+      permute_rows(ip, n, B, nrhs, false, idx, T);
+      for(int k0 = 0; k0 < n; k0 += nb) {
+        const int kb = min(nb, n - k0);
+        load_diag(L + k0 + (size_t)k0 * n, n, kb, S);
+        diag_solve<LOWER_UNIT>(kb, B + k0, n, nrhs, S);
+        tile_gemm_sub(n - k0 - kb, nrhs, kb, L + (k0 + kb) + (size_t)k0 * n, n, B + k0, n,
+                      B + k0 + kb, n, S);
+      }
+      for(int k0 = (n - 1) / nb * nb; k0 >= 0; k0 -= nb) {
+        const int kb = min(nb, n - k0);
+        load_diag(L + k0 + (size_t)k0 * n, n, kb, S);
+        diag_solve<UPPER>(kb, B + k0, n, nrhs, S);
+        tile_gemm_sub(k0, nrhs, kb, L + (size_t)k0 * n, n, B + k0, n, B, n, S);
+      }
+    } else {
+      // x = P^T L^-T U^-T b
+      for(int k0 = 0; k0 < n; k0 += nb) {
+        const int kb = min(nb, n - k0);
+        tile_gemm_tn_sub(kb, nrhs, k0, L + (size_t)k0 * n, n, B, n, B + k0, n, S);
+        load_diag(L + k0 + (size_t)k0 * n, n, kb, S);
+        diag_solve<UPPER_T>(kb, B + k0, n, nrhs, S);
+      }
+      for(int k0 = (n - 1) / nb * nb; k0 >= 0; k0 -= nb) {
+        const int kb = min(nb, n - k0);
+        tile_gemm_tn_sub(kb, nrhs, n - k0 - kb, L + (k0 + kb) + (size_t)k0 * n, n, B + k0 + kb,
+                         n, B + k0, n, S);
+        load_diag(L + k0 + (size_t)k0 * n, n, kb, S);
+        diag_solve<LOWER_UNIT_T>(kb, B + k0, n, nrhs, S);
+      }
+      permute_rows(ip, n, B, nrhs, true, idx, T);
+    }
+  }
+}
+
+
+// C_i = alpha X_i Y_i^T for every system (X_i, Y_i n_i x nrhs_i in the B-pool
+// layout, C_i n_i x n_i in the A-pool layout): 64 x 64 output tiles, the
+// nrhs-long slices of X and Y staged in shared memory (k <= 64 in two halves),
+// each thread 2 x 4 outputs, streaming stores.
+__global__ void __launch_bounds__(kBT, 1) batch_rank_k_kernel(const Args* pa) {
+  __shared__ Smem S;
+  const Args a = *pa;
+  const int  tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // rows tx + 32 i, cols ty + 16 j
+  for(;;) {
+    const int s = next_system(a, S);
+    if(s < 0) break;
+    const Sys&    y = a.sys[s];
+    const int     n = y.n, k = y.nrhs;
+    const double* X = a.X + y.b_off;
+    const double* Yp = a.Y + y.b_off;
+    double*       C = a.C + y.a_off;
+    const int     tn = (n + kTile - 1) / kTile;
+    for(int tile = 0; tile < tn * tn; ++tile) {
+      const int m0 = (tile % tn) * kTile, n0 = (tile / tn) * kTile;
+      double acc[2][4] = {};
+      for(int k0 = 0; k0 < k; k0 += kNbMax) {
+        const int kc = min(kNbMax, k - k0);
+        __syncthreads();
+        for(int idx = threadIdx.x; idx < kNbMax * kTile; idx += kBT) {
+          const int r = idx % kTile, kk = idx / kTile;
+          S.As[kk][r] = (kk < kc && m0 + r < n) ? X[(size_t)(m0 + r) + (size_t)(k0 + kk) * n] : 0.0;
+          S.Bs[r][kk] = (kk < kc && n0 + r < n) ? Yp[(size_t)(n0 + r) + (size_t)(k0 + kk) * n] : 0.0;
+        }
+        __syncthreads();
+        for(int kk = 0; kk < kc; ++kk) {
+          double xa[2], yb[4];
+#pragma unroll
+          for(int i = 0; i < 2; ++i) xa[i] = S.As[kk][tx + 32 * i];
+#pragma unroll
+          for(int j = 0; j < 4; ++j) yb[j] = S.Bs[ty + 16 * j][kk];
+#pragma unroll
+          for(int i = 0; i < 2; ++i)
+#pragma unroll
+            for(int j = 0; j < 4; ++j) acc[i][j] = fma(xa[i], yb[j], acc[i][j]);
+        }
+      }
+#pragma unroll
+      for(int j = 0; j < 4; ++j) {
+        const int c = n0 + ty + 16 * j;
+#pragma unroll
+        for(int i = 0; i < 2; ++i) {
+          const int r = m0 + tx + 32 * i;
+          if(r < n && c < n) __stcs(C + (size_t)r + (size_t)c * n, a.alpha * acc[i][j]);
+        }
+      }
+    }
+  }
+}
+
+// LCG of one system: [A_i | B_i] = HPL_pdrandmat(n_i, n_i + nrhs_i, seed_i)
+// with m = n_i rows, i.e. entry (r, c) is X(1 + r + c n_i); columns >= n_i are
+// B_i.  Thread per row: the row's first state by the binary jump table, then a
+// jump of n_i per column.
+HPLB_DEV uint64_t state_of(uint64_t x1, uint64_t k, const Jump* pow2) {
+  Jump acc{1, 0};
+  for(int b = 0; k; ++b, k >>= 1)
+    if(k & 1) acc = compose(acc, pow2[b]);
+  return apply(acc, x1);
+}
+
+__global__ void __launch_bounds__(kBT, 1) batch_matgen_kernel(const Args* pa) {
+  __shared__ Smem S;
+  __shared__ Jump pow2[64];
+  __shared__ Jump jn;
+  const Args a = *pa;
+  if(threadIdx.x == 0) {
+    Jump p{kLcgMult, kLcgAdd};
+    for(int b = 0; b < 64; ++b) {
+      pow2[b] = p;
+      p       = compose(p, p);
+    }
+  }
+  for(;;) {
+    const int s = next_system(a, S);
+    if(s < 0) break;
+    const Sys& y = a.sys[s];
+    const int  n = y.n;
+    if(threadIdx.x == 0) jn = jump_by((uint64_t)n);
+    __syncthreads();
+    const uint64_t x1 = kLcgMult * a.seeds[s] + kLcgAdd;
+    double*        A  = a.A + y.a_off;
+    double*        B  = a.B + y.b_off;
+    for(int r = threadIdx.x; r < n; r += kBT) {
+      uint64_t st = state_of(x1, (uint64_t)r, pow2);
+      for(int c = 0; c < n + y.nrhs; ++c) {
+        const double v = lcg_value(st);
+        if(c < n)
+          A[(size_t)r + (size_t)c * n] = v;
+        else
+          B[(size_t)r + (size_t)(c - n) * n] = v;
+        st = apply(jn, st);
+      }
+    }
+  }
+}
+
+// HPL scaled residual of every system against its regenerated [A_i | B_i]:
+// per right-hand side c, ||B_c - A X_c||oo / (eps (||A||oo ||X_c||oo +
+// ||B_c||oo) n) with eps = 2^-53 (src/HPL_pdtest.cpp:330-438); resid[i] is the
+// largest over the system's right-hand sides.  X_c is staged in shared memory
+// kPermCols columns at a time; A is regenerated for each group.
+__global__ void __launch_bounds__(kBT, 1) batch_residual_kernel(const Args* pa) {
+  extern __shared__ __align__(16) double xs[];
+  __shared__ Smem S;
+  __shared__ Jump pow2[64];
+  __shared__ Jump jn;
+  __shared__ double s_worst;
+  const Args a = *pa;
+  if(threadIdx.x == 0) {
+    Jump p{kLcgMult, kLcgAdd};
+    for(int b = 0; b < 64; ++b) {
+      pow2[b] = p;
+      p       = compose(p, p);
+    }
+  }
+  for(;;) {
+    const int s = next_system(a, S);
+    if(s < 0) break;
+    const Sys&    y = a.sys[s];
+    const int     n = y.n, nrhs = y.nrhs;
+    const double* X = a.X + y.b_off;
+    if(threadIdx.x == 0) {
+      jn      = jump_by((uint64_t)n);
+      s_worst = 0.0;
+    }
+    __syncthreads();
+    const uint64_t x1 = kLcgMult * a.seeds[s] + kLcgAdd;
+    for(int c0 = 0; c0 < nrhs; c0 += kPermCols) {
+      const int nc = min(kPermCols, nrhs - c0);
+      for(int e = threadIdx.x; e < nc * n; e += kBT) xs[e] = X[(size_t)c0 * n + e];
+      __syncthreads();
+      double rmax[kPermCols], bmax[kPermCols], xmax[kPermCols], amax = 0.0;
+#pragma unroll
+      for(int c = 0; c < kPermCols; ++c) rmax[c] = bmax[c] = xmax[c] = 0.0;
+      for(int r = threadIdx.x; r < n; r += kBT) {
+        uint64_t st = state_of(x1, (uint64_t)r, pow2);
+        double   dot[kPermCols], rs = 0.0;
+#pragma unroll
+        for(int c = 0; c < kPermCols; ++c) dot[c] = 0.0;
+        for(int j = 0; j < n; ++j) {
+          const double v = lcg_value(st);
+          rs += fabs(v);
+#pragma unroll
+          for(int c = 0; c < kPermCols; ++c)
+            if(c < nc) dot[c] = fma(v, xs[(size_t)c * n + j], dot[c]);
+          st = apply(jn, st);
+        }
+        amax = fmax(amax, rs);
+        // skip to the right-hand side columns c0 ..
+        uint64_t sb = state_of(x1, (uint64_t)r + (uint64_t)(n + c0) * (uint64_t)n, pow2);
+#pragma unroll
+        for(int c = 0; c < kPermCols; ++c)
+          if(c < nc) {
+            const double b = lcg_value(sb);
+            rmax[c]        = fmax(rmax[c], fabs(b - dot[c]));
+            bmax[c]        = fmax(bmax[c], fabs(b));
+            xmax[c]        = fmax(xmax[c], fabs(xs[(size_t)c * n + r]));
+            sb             = apply(jn, sb);
+          }
+      }
+      // Block maxima (row sums, then per column r, b, x).
+      double v = amax;
+      for(int off = 16; off > 0; off >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, off));
+      __syncthreads();
+      if((threadIdx.x & 31) == 0) S.red_v[threadIdx.x >> 5] = v;
+      __syncthreads();
+      double an = 0.0;
+      for(int w = 0; w < kBW; ++w) an = fmax(an, S.red_v[w]);
+      for(int c = 0; c < nc; ++c) {
+        double m3[3] = {rmax[c], bmax[c], xmax[c]};
+        double out[3];
+        for(int q = 0; q < 3; ++q) {
+          double t = m3[q];
+          for(int off = 16; off > 0; off >>= 1) t = fmax(t, __shfl_down_sync(0xffffffffu, t, off));
+          __syncthreads();
+          if((threadIdx.x & 31) == 0) S.red_v[threadIdx.x >> 5] = t;
+          __syncthreads();
+          double u = 0.0;
+          for(int w = 0; w < kBW; ++w) u = fmax(u, S.red_v[w]);
+          out[q] = u;
+        }
+        if(threadIdx.x == 0) {
+          const double eps = 0x1p-53;
+          const double res = out[0] / (eps * (an * out[2] + out[1]) * (double)n);
+          s_worst          = fmax(s_worst, res);
+        }
+      }
+      __syncthreads();
+    }
+    if(threadIdx.x == 0) a.resid[s] = s_worst;
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Launchers (the plan in batch_api.cu sizes the shared memory and the grid).
+// ---------------------------------------------------------------------------
+
+size_t batch_static_smem() { return sizeof(Smem); }
+int    batch_threads() { return kBT; }
+int    batch_nb_max() { return kNbMax; }
+
+cudaError_t batch_set_smem(size_t dyn_bytes) {
+  cudaError_t e = cudaFuncSetAttribute(batch_gesv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)dyn_bytes);
+  if(e == cudaSuccess)
+    e = cudaFuncSetAttribute(batch_getrs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dyn_bytes);
+  if(e == cudaSuccess)
+    e = cudaFuncSetAttribute(batch_getrs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dyn_bytes);
+  if(e == cudaSuccess)
+    e = cudaFuncSetAttribute(batch_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)dyn_bytes);
+  return e;
+}
+
+// mode: 0 gesv, 1 getrs, 2 getrs transposed, 3 rank-k, 4 matgen, 5 residual.
+cudaError_t launch_batch(int mode, const void* d_args, int grid, size_t dyn_bytes,
+                         cudaStream_t st) {
+  const Args* pa = static_cast<const Args*>(d_args);
+  switch(mode) {
+    case 0: batch_gesv_kernel<<<grid, kBT, dyn_bytes, st>>>(pa); break;
+    case 1: batch_getrs_kernel<false><<<grid, kBT, dyn_bytes, st>>>(pa); break;
+    case 2: batch_getrs_kernel<true><<<grid, kBT, dyn_bytes, st>>>(pa); break;
+    case 3: batch_rank_k_kernel<<<grid, kBT, 0, st>>>(pa); break;
+    case 4: batch_matgen_kernel<<<grid, kBT, 0, st>>>(pa); break;
+    case 5: batch_residual_kernel<<<grid, kBT, dyn_bytes, st>>>(pa); break;
+    default: return cudaErrorInvalidValue;
+  }
+  return cudaGetLastError();
+}
+
+size_t batch_args_bytes() { return sizeof(Args); }
+
+void batch_fill_args(void* host_args, double* A, const double* LU, double* B, int* ipiv,
+                     const int* ipivc, int* info, const void* sys, const int* order, int count,
+                     int* counter, double alpha, const double* X, const double* Y, double* C,
+                     const unsigned long long* seeds, double* resid) {
+  Args* a    = static_cast<Args*>(host_args);
+  a->A       = A;
+  a->LU      = LU;
+  a->B       = B;
+  a->ipiv    = ipiv;
+  a->ipivc   = ipivc;
+  a->info    = info;
+  a->sys     = static_cast<const Sys*>(sys);
+  a->order   = order;
+  a->count   = count;
+  a->counter = counter;
+  a->alpha   = alpha;
+  a->X       = X;
+  a->Y       = Y;
+  a->C       = C;
+  a->seeds   = seeds;
+  a->resid   = resid;
+}
+
+size_t batch_sys_bytes() { return sizeof(Sys); }
+void   batch_fill_sys(void* dst, int i, int n, int nrhs, int nb, long long a_off, long long b_off,
+                      long long p_off) {
+  Sys* y   = static_cast<Sys*>(dst) + i;
+  y->n     = n;
+  y->nrhs  = nrhs;
+  y->nb    = nb;
+  y->pad   = 0;
+  y->a_off = a_off;
+  y->b_off = b_off;
+  y->p_off = p_off;
+}
+
+}  // namespace hplb

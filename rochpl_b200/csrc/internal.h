@@ -128,6 +128,24 @@ cudaError_t launch_rank_k(int m, int n, int k, double alpha, const double* A, in
 // status[ST_INFO] = first i (1-based) with ipiv[i] outside [i, n), else untouched.
 cudaError_t launch_check_ipiv(int n, const int* ipiv, int* status, cudaStream_t st);
 
+// Batched solver kernels (batch.cu); the plan and C ABI are in batch_api.cu.
+size_t      batch_static_smem();
+int         batch_threads();
+int         batch_nb_max();
+cudaError_t batch_set_smem(size_t dyn_bytes);
+// mode: 0 gesv, 1 getrs, 2 getrs transposed, 3 rank-k, 4 matgen, 5 residual.
+cudaError_t launch_batch(int mode, const void* d_args, int grid, size_t dyn_bytes,
+                         cudaStream_t st);
+size_t      batch_args_bytes();
+void        batch_fill_args(void* host_args, double* A, const double* LU, double* B, int* ipiv,
+                            const int* ipivc, int* info, const void* sys, const int* order,
+                            int count, int* counter, double alpha, const double* X,
+                            const double* Y, double* C, const unsigned long long* seeds,
+                            double* resid);
+size_t      batch_sys_bytes();
+void        batch_fill_sys(void* dst, int i, int n, int nrhs, int nb, long long a_off,
+                           long long b_off, long long p_off);
+
 // FP64 issue-rate probes (TFLOP/s) and the bounded-wait self test.
 cudaError_t fp64_peak(int num_sms, int iters, double* dmma_tflops, double* dfma_tflops,
                       cudaStream_t stream);

@@ -27,8 +27,13 @@ EXPORTS = [
     "hplb_residual_lcg", "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm",
     "hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_residual_lcg_noalloc",
     "hplb_gemm_lp_sub", "hplb_pdgesv_mixed", "hplb_getrf", "hplb_getrs", "hplb_rank_k",
-    "hplb_set_stream",
+    "hplb_set_stream", "hplb_batch_create", "hplb_batch_destroy", "hplb_batch_layout",
+    "hplb_batch_matgen", "hplb_batch_gesv", "hplb_batch_getrs", "hplb_batch_rank_k",
+    "hplb_batch_residual", "hplb_batch_last_ms", "hplb_batch_tune",
 ]
+
+HPLB_BATCH_CLASSES = 6
+HPLB_BATCH_MAX_N = 2048
 
 
 class hplb_algo(C.Structure):
@@ -108,6 +113,23 @@ def load() -> C.CDLL:
     L.hplb_pdgesv_mixed.argtypes = [vp, C.POINTER(hplb_algo), C.POINTER(hplb_mixed_opts), i32, vp,
                                     i64, u64, vp, vp, C.POINTER(hplb_mixed_report)]
     L.hplb_pdgesv_mixed.restype = i32
+    ip, i64p, u64p, dp = (C.POINTER(C.c_int), C.POINTER(C.c_int64), C.POINTER(C.c_uint64),
+                          C.POINTER(C.c_double))
+    L.hplb_batch_create.argtypes = [vp, i32, ip, ip, ip, C.POINTER(vp)]
+    L.hplb_batch_destroy.argtypes = [vp]
+    L.hplb_batch_destroy.restype = None
+    L.hplb_batch_layout.argtypes = [vp, i64p, i64p, i64p, i64p, i64p, i64p, ip]
+    L.hplb_batch_matgen.argtypes = [vp, u64p, vp, vp]
+    L.hplb_batch_gesv.argtypes = [vp, vp, vp, vp, vp]
+    L.hplb_batch_getrs.argtypes = [vp, i32, vp, vp, vp]
+    L.hplb_batch_rank_k.argtypes = [vp, C.c_double, vp, vp, vp]
+    L.hplb_batch_residual.argtypes = [vp, u64p, vp, vp]
+    L.hplb_batch_last_ms.argtypes = [vp, dp]
+    L.hplb_batch_tune.argtypes = [vp, i32, ip, dp]
+    for name in ("hplb_batch_create", "hplb_batch_layout", "hplb_batch_matgen", "hplb_batch_gesv",
+                 "hplb_batch_getrs", "hplb_batch_rank_k", "hplb_batch_residual",
+                 "hplb_batch_last_ms", "hplb_batch_tune"):
+        getattr(L, name).restype = i32
     L.hplb_set_stream.argtypes = [vp, vp]
     L.hplb_set_stream.restype = i32
     L.hplb_getrf.argtypes = [vp, C.POINTER(hplb_algo), i32, vp, i64, vp, C.POINTER(C.c_int)]
