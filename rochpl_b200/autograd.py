@@ -8,6 +8,10 @@ pivots are saved for the backward pass, which never refactors:
     Bbar = A^-T Xbar      hplb_getrs(trans = 1) on the stored LU and pivots
     Abar = -Bbar X^T      hplb_rank_k, one fused rank-nrhs kernel
 
+HplSolveBatch / hpl_solve_batch do the same for a whole batch of systems of
+uneven size (hplb_batch_gesv forward; hplb_batch_getrs with trans = 1 and
+hplb_batch_rank_k backward).
+
 Everything runs in FP64 on the device through the C ABI (include/hplb.h); the
 tensors are only the carriers of device memory.  There is no CPU path: a CPU
 tensor is an error.
@@ -19,7 +23,7 @@ import torch
 from .hpl import Algo
 from .lib import HplError, library
 
-__all__ = ["HplSolve", "hpl_solve"]
+__all__ = ["HplSolve", "hpl_solve", "HplSolveBatch", "hpl_solve_batch"]
 
 
 def _colmajor(M: torch.Tensor) -> torch.Tensor:
@@ -87,3 +91,73 @@ def hpl_solve(A: torch.Tensor, B: torch.Tensor, nb: int = 256, nbmin: int = 32) 
     if B.dim() == 1:
         return HplSolve.apply(A, B.unsqueeze(1), nb, nbmin).squeeze(1)
     return HplSolve.apply(A, B, nb, nbmin)
+
+
+class HplSolveBatch(torch.autograd.Function):
+    """X_i = A_i^-1 B_i for every system of a BatchPlan, on packed pools (the
+    plan's A and B layouts, 1-D FP64 CUDA tensors).  Forward: one batched
+    factor-and-solve launch; the factors and pivots are saved.  Backward:
+    Bbar_i = A_i^-T Xbar_i by the batched transposed solve on the stored
+    factors, Abar_i = -Bbar_i X_i^T by the batched rank-k kernel."""
+
+    @staticmethod
+    def forward(ctx, plan, A_pool: torch.Tensor, B_pool: torch.Tensor):
+        if not (A_pool.is_cuda and B_pool.is_cuda):
+            raise ValueError("hpl_solve_batch runs on the GPU only")
+        if A_pool.dtype != torch.float64 or B_pool.dtype != torch.float64:
+            raise ValueError("hpl_solve_batch computes in FP64")
+        if A_pool.numel() != plan.a_elems or B_pool.numel() != plan.b_elems:
+            raise ValueError("pool sizes do not match the plan's layout")
+        lib = plan.lib
+        lib.set_stream(torch.cuda.current_stream(A_pool.device).cuda_stream)
+        LU = A_pool.detach().clone()
+        X = B_pool.detach().clone()
+        ipiv = torch.zeros(max(plan.p_elems, 1), dtype=torch.int32, device=A_pool.device)
+        info = torch.zeros(max(plan.count, 1), dtype=torch.int32, device=A_pool.device)
+        plan.gesv(LU.data_ptr(), X.data_ptr(), ipiv.data_ptr(), info.data_ptr())
+        bad = int(info.max()) if plan.count else 0
+        if bad:
+            raise HplError(3, f"hpl_solve_batch: a system is singular (zero pivot, column {bad})")
+        ctx.plan = plan
+        ctx.save_for_backward(LU, ipiv, X)
+        return X
+
+    @staticmethod
+    def backward(ctx, Xbar: torch.Tensor):
+        LU, ipiv, X = ctx.saved_tensors
+        plan = ctx.plan
+        plan.lib.set_stream(torch.cuda.current_stream(LU.device).cuda_stream)
+        Bbar = Xbar.to(torch.float64).contiguous().clone()
+        plan.getrs(1, LU.data_ptr(), ipiv.data_ptr(), Bbar.data_ptr())
+        gA = None
+        if ctx.needs_input_grad[1]:
+            gA = torch.empty(plan.a_elems, dtype=torch.float64, device=LU.device)
+            plan.rank_k(-1.0, Bbar.data_ptr(), X.data_ptr(), gA.data_ptr())
+        return None, gA, (Bbar if ctx.needs_input_grad[2] else None)
+
+
+def pack_batch(plan, mats, pool_elems: int, offsets) -> torch.Tensor:
+    """Pack square or tall matrices (list of 2-D tensors) into a plan pool,
+    column-major, at the plan's offsets.  Differentiable."""
+    parts = []
+    for M in mats:
+        parts.append(M.t().reshape(-1))
+    out = torch.cat(parts) if parts else torch.zeros(0, dtype=torch.float64)
+    if out.numel() != pool_elems:
+        raise ValueError("matrices do not match the plan's layout")
+    return out
+
+
+def unpack_batch(plan, pool: torch.Tensor, rows, cols, offsets):
+    """Views of the systems' matrices (rows[i] x cols[i]) in a pool."""
+    return [pool[int(o):int(o) + int(r) * int(c)].view(int(c), int(r)).t()
+            for o, r, c in zip(offsets, rows, cols)]
+
+
+def hpl_solve_batch(plan, As, Bs):
+    """X_i = A_i^-1 B_i for lists of FP64 CUDA matrices matching the plan's
+    sizes; differentiable in every A_i and B_i.  Returns the list of X_i."""
+    A_pool = pack_batch(plan, As, plan.a_elems, plan.a_off)
+    B_pool = pack_batch(plan, Bs, plan.b_elems, plan.b_off)
+    X = HplSolveBatch.apply(plan, A_pool, B_pool)
+    return unpack_batch(plan, X, plan.n, plan.nrhs, plan.b_off)

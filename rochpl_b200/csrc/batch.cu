@@ -18,6 +18,8 @@
 // The stored-factor solves (plain and transposed), the batched rank-k product
 // of the adjoint, the per-system LCG generator and the per-system HPL residual
 // use the same CTA-per-system loop.
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.h"
 #include "lcg.cuh"
@@ -456,7 +458,7 @@ HPLB_DEV void permute_rows(const int* ip, int n, double* B, int nrhs, bool inver
     for(int i = 0; i < n; ++i) pos[i] = i;
     for(int j = 0; j < n; ++j) {
       const int r = pv[j];
-      if(r != j) {
+      if(r != j && r >= 0 && r < n) {
         const int t = pos[j];
         pos[j]      = pos[r];
         pos[r]      = t;
@@ -744,19 +746,29 @@ size_t batch_static_smem() { return sizeof(Smem); }
 int    batch_threads() { return kBT; }
 int    batch_nb_max() { return kNbMax; }
 
-cudaError_t batch_set_smem(size_t dyn_bytes) {
-  cudaError_t e = cudaFuncSetAttribute(batch_gesv_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)dyn_bytes);
-  if(e == cudaSuccess)
-    e = cudaFuncSetAttribute(batch_getrs_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dyn_bytes);
-  if(e == cudaSuccess)
-    e = cudaFuncSetAttribute(batch_getrs_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dyn_bytes);
-  if(e == cudaSuccess)
-    e = cudaFuncSetAttribute(batch_residual_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)dyn_bytes);
-  return e;
+// Raise every dynamic-shared-memory kernel's limit to what its own static
+// shared memory leaves of the per-block opt-in maximum; *budget = the
+// smallest of those limits (what a plan may use in every mode).
+cudaError_t batch_set_smem(size_t* budget) {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if(e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  if(e != cudaSuccess) return e;
+  const void* fns[4] = {(const void*)batch_gesv_kernel, (const void*)batch_getrs_kernel<false>,
+                        (const void*)batch_getrs_kernel<true>, (const void*)batch_residual_kernel};
+  size_t lowest = (size_t)optin;
+  for(const void* f : fns) {
+    cudaFuncAttributes fa{};
+    if((e = cudaFuncGetAttributes(&fa, f)) != cudaSuccess) return e;
+    const int lim = optin - (int)fa.sharedSizeBytes;
+    if(lim <= 0) return cudaErrorInvalidValue;
+    if((e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)) !=
+       cudaSuccess)
+      return e;
+    lowest = std::min(lowest, (size_t)lim);
+  }
+  *budget = lowest;
+  return cudaSuccess;
 }
 
 // mode: 0 gesv, 1 getrs, 2 getrs transposed, 3 rank-k, 4 matgen, 5 residual.

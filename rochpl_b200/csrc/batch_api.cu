@@ -61,12 +61,15 @@ size_t dyn_bytes(const hplb_batch* b) {
   return m;
 }
 
-size_t dyn_budget() {
-  int dev = 0, optin = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const long long b = (long long)optin - (long long)batch_static_smem() - 1024;
-  return b > 0 ? (size_t)b : 0;
+// Dynamic shared memory a plan may use (and the kernels' limits set to it).
+hplb_status dyn_budget(hplb_ctx* ctx, size_t* budget) {
+  const cudaError_t e = batch_set_smem(budget);
+  if(e != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(ctx, HPLB_ERR_CUDA, "batch kernels' shared-memory limits: %s",
+                   cudaGetErrorString(e));
+  }
+  return HPLB_OK;
 }
 
 // Capture (once) and launch the graph of `mode` with the arguments already in
@@ -142,6 +145,9 @@ hplb_status hplb_batch_create(hplb_ctx* ctx, int count, const int* n, const int*
       if(nb_by_class[c] != 8 && nb_by_class[c] != 16 && nb_by_class[c] != 32)
         return set_err(ctx, HPLB_ERR_ARG, "hplb_batch_create: panel widths must be 8, 16 or 32");
   ENTER(ctx);
+  size_t      budget = 0;
+  hplb_status sb     = dyn_budget(ctx, &budget);
+  if(sb != HPLB_OK) return sb;
   auto* b  = new hplb_batch();
   b->ctx   = ctx;
   b->count = count;
@@ -151,7 +157,6 @@ hplb_status hplb_batch_create(hplb_ctx* ctx, int count, const int* n, const int*
   b->a_off.resize(count);
   b->b_off.resize(count);
   b->p_off.resize(count);
-  const size_t budget = dyn_budget();
   for(int i = 0; i < count; ++i) {
     int w = (nb_by_class ? nb_by_class : kDefaultNb)[size_class(n[i])];
     while(w > 8 && (size_t)w * n[i] * sizeof(double) > budget) w /= 2;
@@ -171,11 +176,6 @@ hplb_status hplb_batch_create(hplb_ctx* ctx, int count, const int* n, const int*
     return r;
   };
   if(b->dyn > budget) return fail(HPLB_ERR_UNSUPPORTED, "systems too large for shared memory");
-  // The attribute is per kernel, shared by every plan: always the full budget.
-  if(batch_set_smem(budget) != cudaSuccess) {
-    cudaGetLastError();
-    return fail(HPLB_ERR_CUDA, "shared-memory attribute refused");
-  }
   // Largest cost first.
   std::vector<int> order(count);
   std::iota(order.begin(), order.end(), 0);
@@ -322,7 +322,9 @@ hplb_status hplb_batch_tune(hplb_ctx* ctx, int nrhs, int* nb_by_class, double* m
   if(!nb_by_class || nrhs < 0) return set_err(ctx, HPLB_ERR_ARG, "hplb_batch_tune: bad argument");
   ENTER(ctx);
   static const int cand[3] = {8, 16, 32};
-  const size_t     budget  = dyn_budget();
+  size_t           budget  = 0;
+  hplb_status      sb      = dyn_budget(ctx, &budget);
+  if(sb != HPLB_OK) return sb;
   const int        count   = 2 * ctx->num_sms;
   for(int c = 0; c < HPLB_BATCH_CLASSES; ++c) {
     const int n    = kTuneN[c];

@@ -132,7 +132,8 @@ cudaError_t launch_check_ipiv(int n, const int* ipiv, int* status, cudaStream_t 
 size_t      batch_static_smem();
 int         batch_threads();
 int         batch_nb_max();
-cudaError_t batch_set_smem(size_t dyn_bytes);
+// Sets the kernels' dynamic shared-memory limits; *budget = what a plan may use.
+cudaError_t batch_set_smem(size_t* budget);
 // mode: 0 gesv, 1 getrs, 2 getrs transposed, 3 rank-k, 4 matgen, 5 residual.
 cudaError_t launch_batch(int mode, const void* d_args, int grid, size_t dyn_bytes,
                          cudaStream_t st);
