@@ -16,6 +16,12 @@ After the FP64 steps the same system is solved in the mixed-precision form
 same residual threshold); its time to solution, speed-up over the FP64 solve,
 iteration counts and distance to the FP64 x go under "mixed" in the line.
 
+Then the batched form (4096 LCG systems, N log-uniform in [32, 1024], nrhs
+1 / 16 / 64, one persistent graph-captured launch each) and the
+differentiable solve (N = 16384 with 32 RHS, forward and backward; 256
+systems with N in [64, 512] through the batched form) go under "batched" and
+"autograd".
+
 Multi-GPU runs are replicas (each rank solves its own system; P = Q = 1 has
 no inter-GPU data path), reported as weak scaling.
 
@@ -246,6 +252,9 @@ def run_ours(args):
         torch.cuda.empty_cache()
         mixed = mixed_leg(lib, algo, n, seed, x64, solve_ms, args, barrier, max_over_ranks)
 
+    batched = None if args.no_batched else batched_leg(lib, args, max_over_ranks)
+    autograd = None if args.no_autograd else autograd_leg(lib, args, max_over_ranks)
+
     cb = None
     if rank == 0 and not args.no_cpu_baseline:
         cb = cpu_baseline(args.cpu_n, nb)
@@ -287,6 +296,10 @@ def run_ours(args):
             line["e2e"] = e2e
         if mixed is not None:
             line["mixed"] = mixed
+        if batched is not None:
+            line["batched"] = batched
+        if autograd is not None:
+            line["autograd"] = autograd
         if cb is not None:
             line["cpu_baseline"] = cb
         print(json.dumps(line), flush=True)
@@ -351,6 +364,122 @@ def mixed_leg(lib, algo, n, seed, x64, fp64_ms, args, barrier, max_over_ranks):
             "gpu_launches": tm["kernel_launches"], "steps": args.mixed_steps,
         }
     return out
+
+
+def batched_leg(lib, args, max_over_ranks):
+    """The batched form: 4096 independent LCG systems, N log-uniform in
+    [32, 1024], per-system seed 100 + i, nrhs in {1, 16, 64}; one persistent,
+    graph-captured launch per solve, panel widths from the autotuner.  value =
+    sum(2/3 N^3 + 2 N^2 nrhs) / device time of the launch."""
+    import numpy as np
+    import torch
+
+    from rochpl_b200.batch import BatchPlan, autotune, workload_sizes
+
+    torch.cuda.empty_cache()
+    n = workload_sizes(args.batch_count)
+    out = {"workload": f"{args.batch_count} systems, N log-uniform in [32, 1024] "
+                       "(numpy PCG64 seed 20261203), seed_i = 100 + i",
+           "by_nrhs": {}}
+    for nrhs in (1, 16, 64):
+        table = autotune(lib, nrhs=nrhs, use_cache=False)
+        plan = BatchPlan(lib, n, nrhs, table)
+        dA = torch.zeros(plan.a_elems, dtype=torch.float64, device="cuda")
+        dB = torch.zeros(plan.b_elems, dtype=torch.float64, device="cuda")
+        dP = torch.zeros(plan.p_elems, dtype=torch.int32, device="cuda")
+        dI = torch.zeros(plan.count, dtype=torch.int32, device="cuda")
+        seeds = 100 + np.arange(plan.count, dtype=np.uint64)
+        ms = []
+        for it in range(args.warmup + args.steps):
+            plan.matgen(seeds, dA.data_ptr(), dB.data_ptr())  # outside the timed launch
+            plan.gesv(dA.data_ptr(), dB.data_ptr(), dP.data_ptr(), dI.data_ptr())
+            if it >= args.warmup:
+                ms.append(plan.last_ms)
+        res = torch.zeros(plan.count, dtype=torch.float64, device="cuda")
+        plan.residual(seeds, dB.data_ptr(), res.data_ptr())
+        t = max_over_ranks(statistics.mean(ms))
+        out["by_nrhs"][str(nrhs)] = {
+            "ms_per_solve": t, "value": plan.flops() / (t * 1e-3) / 1e12, "unit": UNIT,
+            "resid_max": float(res.max()), "resid_passed": bool(float(res.max()) < 16.0),
+            "singular": int((dI != 0).sum()), "nb_by_class": table, "gpu_launches": 1,
+            "flops": plan.flops()}
+        del dA, dB, dP, dI, res
+        plan.close()
+        torch.cuda.empty_cache()
+    return out
+
+
+def autograd_leg(lib, args, max_over_ranks):
+    """The differentiable solve X = A^-1 B (FP64): N = 16384 with 32 RHS from
+    the LCG (forward: factor + solve; backward: transposed solves on the stored
+    factors + the fused rank-32 kernel), and 256 systems with N uniform in
+    [64, 512] through the batched form."""
+    import numpy as np
+    import torch
+
+    from rochpl_b200.autograd import hpl_solve, hpl_solve_batch
+    from rochpl_b200.batch import BatchPlan
+
+    torch.cuda.empty_cache()
+    n, nrhs = args.ad_n, 32
+    M = torch.empty((n + nrhs) * n, dtype=torch.float64, device="cuda")
+    lib.matgen(n, n + nrhs, 100, M.data_ptr(), n)
+    Mc = M.view(n + nrhs, n)
+    A = Mc[:n].t().contiguous().requires_grad_(True)
+    B = Mc[n:].t().contiguous().requires_grad_(True)
+    del M, Mc
+    Xbar = torch.ones(n, nrhs, dtype=torch.float64, device="cuda")
+    fwd, bwd = [], []
+    for it in range(args.warmup + args.steps):
+        A.grad = None
+        B.grad = None
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record()
+        X = hpl_solve(A, B, nb=512)
+        e1.record()
+        X.backward(Xbar)
+        e2.record()
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            fwd.append(e0.elapsed_time(e1))
+            bwd.append(e1.elapsed_time(e2))
+    with torch.no_grad():
+        r = (A @ X - B).abs().max().item()
+    f_fwd = 2.0 / 3.0 * n ** 3 + 2.0 * n ** 2 * nrhs
+    tf, tb = max_over_ranks(statistics.mean(fwd)), max_over_ranks(statistics.mean(bwd))
+    single = {"n": n, "nrhs": nrhs, "forward_ms": tf, "backward_ms": tb,
+              "forward_tflops": f_fwd / (tf * 1e-3) / 1e12,
+              "backward_flops": 4.0 * n ** 2 * nrhs, "abs_residual_max": r,
+              "note": "torch CUDA events on the current stream around hpl_solve and backward()"}
+    del A, B, X, Xbar
+    torch.cuda.empty_cache()
+    rng = np.random.default_rng(20261203)
+    sizes = rng.integers(64, 513, size=256).astype(np.int32)
+    plan = BatchPlan(lib, sizes, nrhs)
+    As, Bs = [], []
+    for i, m in enumerate(sizes):
+        Mi = torch.empty(int(m) * (int(m) + nrhs), dtype=torch.float64, device="cuda")
+        lib.matgen(int(m), int(m) + nrhs, 100 + i, Mi.data_ptr(), int(m))
+        Mi = Mi.view(int(m) + nrhs, int(m))
+        As.append(Mi[:m].t().contiguous().requires_grad_(True))
+        Bs.append(Mi[m:].t().contiguous().requires_grad_(True))
+    tfb = []
+    for it in range(args.warmup + args.steps):
+        for T in As + Bs:
+            T.grad = None
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        Xs = hpl_solve_batch(plan, As, Bs)
+        sum(X.sum() for X in Xs).backward()
+        torch.cuda.synchronize()
+        if it >= args.warmup:
+            tfb.append((time.perf_counter() - t0) * 1e3)
+    plan.close()
+    batch = {"systems": 256, "n_range": [64, 512], "nrhs": nrhs,
+             "forward_backward_ms_wall": max_over_ranks(statistics.mean(tfb)),
+             "note": "wall clock incl. packing the 512 tensors into pools"}
+    return {"single": single, "batched": batch}
 
 
 def _cudart():
@@ -442,6 +571,10 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision (16-bit LU + GMRES-IR) leg")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched-solver leg")
+    ap.add_argument("--no-autograd", action="store_true", help="skip the autograd leg")
+    ap.add_argument("--batch-count", type=int, default=4096)
+    ap.add_argument("--ad-n", type=int, default=16384)
     ap.add_argument("--mixed-steps", type=int, default=2)
     ap.add_argument("--mixed-warmup", type=int, default=1)
     ap.add_argument("--gemm-traffic", type=float, default=None,
