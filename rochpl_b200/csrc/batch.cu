@@ -33,6 +33,11 @@ constexpr int kBW    = kBT / 32;
 constexpr int kNbMax = 32;   // widest panel
 constexpr int kTile  = 64;   // output tile of the block updates
 constexpr int kLdT   = kTile + 4;
+constexpr int kRegPanelW = 16;  // widest panel held in registers
+
+// Leading dimension of the panel copy in shared memory: >= n rows and = 4
+// (mod 16), so the DMMA A-fragment loads (rows g, columns t) hit distinct banks.
+__host__ __device__ inline int panel_ld(int n) { return (n + 15) / 16 * 16 + 4; }
 
 struct Sys {
   int       n, nrhs, nb, pad;
@@ -67,8 +72,20 @@ struct Smem {
   int    dst[kNbMax];  // old top row x went to row dst[x], or -1 if it stayed on top
   int    next;
   int    info;
-  double As[kNbMax][kLdT];  // A tile: k x rows
-  double Bs[kTile][kNbMax + 2];  // B tile: cols x k
+  // The A tile of the staged GEMMs and the register panel's exchange slots are
+  // never live at once.
+  union {
+    double As[kNbMax][kLdT];  // A tile: k x rows
+    // Register panel: per warp, its pivot candidate and that row's values,
+    // and the diagonal row; double-buffered by column parity.
+    struct {
+      double cv[2][kBW];
+      int    cr[2][kBW];
+      double crow[2][kBW][kRegPanelW];
+      double cur[2][kRegPanelW];
+    } pr;
+  };
+  double Bs[kTile][kNbMax + 4];  // B tile: cols x k (row length = 4 mod 16: conflict free)
   double D[kNbMax][kNbMax + 1];  // a diagonal block
 };
 
@@ -301,18 +318,206 @@ HPLB_DEV int next_system(const Args& a, Smem& S) {
   return S.next;
 }
 
+// The m x kb panel at A (leading dimension lda; rows k0.. of the system) with
+// each thread's rows t + q * kBT (q < RPT) in registers, column loop unrolled.
+// Per column: each warp finds its candidate by shuffles and publishes it with
+// the row's values, the owner of the diagonal row publishes that row, one
+// barrier, then every thread picks the winner and applies the interchange,
+// the division by the pivot and the update to its own rows.  The factored
+// panel goes back to A and to the shared copy P (leading dimension ldp) that
+// the trailing update reads L21 from.
+template <int RPT, int KB>
+HPLB_DEV void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, double* P, int ldp,
+                        Smem& S) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double    x[RPT][KB];
+  int       row[RPT];
+#pragma unroll
+  for(int q = 0; q < RPT; ++q) {
+    row[q]        = threadIdx.x + q * kBT;
+    const bool in = row[q] < m;
+    if(!in) row[q] = -1;
+#pragma unroll
+    for(int c = 0; c < KB; ++c) x[q][c] = (in && c < kb) ? Ag[(size_t)row[q] + (size_t)c * lda] : 0.0;
+  }
+#pragma unroll
+  for(int j = 0; j < KB; ++j) {
+    if(j >= kb) break;
+    const int par = j & 1;
+    double    v   = 0.0;
+    int       r   = -1;
+#pragma unroll
+    for(int q = 0; q < RPT; ++q)
+      if(row[q] >= j && better_b(x[q][j], row[q], v, r)) {
+        v = x[q][j];
+        r = row[q];
+      }
+#pragma unroll
+    for(int off = 16; off > 0; off >>= 1) {
+      const double ov  = __shfl_down_sync(0xffffffffu, v, off);
+      const int    orr = __shfl_down_sync(0xffffffffu, r, off);
+      if(better_b(ov, orr, v, r)) {
+        v = ov;
+        r = orr;
+      }
+    }
+    v = __shfl_sync(0xffffffffu, v, 0);
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if(lane == 0) {
+      S.pr.cv[par][warp] = v;
+      S.pr.cr[par][warp] = r;
+    }
+#pragma unroll
+    for(int q = 0; q < RPT; ++q) {
+      if(r >= 0 && row[q] == r)
+#pragma unroll
+        for(int c = 0; c < KB; ++c) S.pr.crow[par][warp][c] = x[q][c];
+      if(row[q] == j)
+#pragma unroll
+        for(int c = 0; c < KB; ++c) S.pr.cur[par][c] = x[q][c];
+    }
+    __syncthreads();
+    // The winner among the warps' candidates (lanes 0..15 read one each).
+    double bv = lane < kBW ? S.pr.cv[par][lane] : 0.0;
+    int    br = lane < kBW ? S.pr.cr[par][lane] : -1;
+    int    bw = lane < kBW ? lane : -1;
+#pragma unroll
+    for(int off = 16; off > 0; off >>= 1) {
+      const double ov  = __shfl_down_sync(0xffffffffu, bv, off);
+      const int    orr = __shfl_down_sync(0xffffffffu, br, off);
+      const int    ow  = __shfl_down_sync(0xffffffffu, bw, off);
+      if(better_b(ov, orr, bv, br)) {
+        bv = ov;
+        br = orr;
+        bw = ow;
+      }
+    }
+    bv = __shfl_sync(0xffffffffu, bv, 0);
+    br = __shfl_sync(0xffffffffu, br, 0);
+    bw = __shfl_sync(0xffffffffu, bw, 0);
+    if(bw < 0) {  // no candidate: only when the panel has no rows >= j, which cannot happen
+      bw = 0;
+      bv = 0.0;
+      br = j;
+    }
+    const double* u = S.pr.crow[par][bw];
+    if(threadIdx.x == 0) {
+      S.piv[j]   = br;
+      ip[k0 + j] = k0 + br;
+      if(bv == 0.0 && S.info == 0) S.info = k0 + j + 1;
+    }
+#pragma unroll
+    for(int q = 0; q < RPT; ++q) {
+      if(row[q] == j) {
+#pragma unroll
+        for(int c = 0; c < KB; ++c) x[q][c] = u[c];
+      } else if(row[q] == br) {
+#pragma unroll
+        for(int c = 0; c < KB; ++c) x[q][c] = S.pr.cur[par][c];
+      }
+      if(bv != 0.0 && row[q] > j) {
+        const double l = x[q][j] / bv;
+        x[q][j]        = l;
+#pragma unroll
+        for(int c = j + 1; c < KB; ++c) x[q][c] = x[q][c] - l * u[c];
+      }
+    }
+  }
+#pragma unroll
+  for(int q = 0; q < RPT; ++q)
+    if(row[q] >= 0)
+#pragma unroll
+      for(int c = 0; c < KB; ++c)
+        if(c < kb) {
+          Ag[(size_t)row[q] + (size_t)c * lda] = x[q][c];
+          P[(size_t)c * ldp + row[q]]          = x[q][c];
+        }
+  __syncthreads();
+}
+
+// C (m2 x ncols, leading dimension ldc) -= L21 U with L21 = rows kb .. kb+m2 of
+// the panel copy P (leading dimension ldp, kb columns) and U (kb x ncols,
+// leading dimension ldu) in global memory.  U is staged 64 columns at a time;
+// within a column block every warp streams its own 16-row strips of C through
+// DMMA (A fragments straight from P, B fragments from the staged block, C
+// fragments from and back to global memory) with no block barrier between
+// strips.
+HPLB_DEV void update_strips(const double* P, int ldp, int kb, int m2, const double* U, int ldu,
+                            double* C, int ldc, int ncols, Smem& S) {
+  if(m2 <= 0 || ncols <= 0 || kb <= 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int k8 = (kb + 7) & ~7;
+  for(int cb = 0; cb < ncols; cb += kTile) {
+    const int nc = min(kTile, ncols - cb);
+    __syncthreads();
+    for(int idx = threadIdx.x; idx < kTile * k8; idx += kBT) {
+      const int c = idx / k8, k = idx % k8;
+      S.Bs[c][k] = (k < kb && c < nc) ? U[(size_t)k + (size_t)(cb + c) * ldu] : 0.0;
+    }
+    __syncthreads();
+    for(int r0 = warp * 16; r0 < m2; r0 += kBW * 16) {
+      double acc[8][4];
+#pragma unroll
+      for(int j = 0; j < 8; ++j)
+#pragma unroll
+        for(int q = 0; q < 4; ++q) {
+          const int r = r0 + g + (q >> 1) * 8, c = j * 8 + 2 * t + (q & 1);
+          acc[j][q] = (r < m2 && c < nc) ? C[(size_t)r + (size_t)(cb + c) * ldc] : 0.0;
+        }
+      for(int kk = 0; kk < k8; kk += 8) {
+        double af[4];
+        const double* pa = P + (size_t)kb + r0 + g;
+        af[0] = kk + t < kb ? -pa[(size_t)(kk + t) * ldp] : 0.0;
+        af[1] = kk + t < kb ? -pa[(size_t)(kk + t) * ldp + 8] : 0.0;
+        af[2] = kk + t + 4 < kb ? -pa[(size_t)(kk + t + 4) * ldp] : 0.0;
+        af[3] = kk + t + 4 < kb ? -pa[(size_t)(kk + t + 4) * ldp + 8] : 0.0;
+#pragma unroll
+        for(int j = 0; j < 8; ++j) {
+          double bf[2];
+          bf[0] = S.Bs[j * 8 + g][kk + t];
+          bf[1] = S.Bs[j * 8 + g][kk + t + 4];
+          dmma(acc[j], af, bf);
+        }
+      }
+#pragma unroll
+      for(int j = 0; j < 8; ++j)
+#pragma unroll
+        for(int q = 0; q < 4; ++q) {
+          const int r = r0 + g + (q >> 1) * 8, c = j * 8 + 2 * t + (q & 1);
+          if(r < m2 && c < nc) C[(size_t)r + (size_t)(cb + c) * ldc] = acc[j][q];
+        }
+    }
+  }
+  __syncthreads();
+}
+
 // Factor one system (A n x n, lda = n) and solve for its B (n x nrhs, ldb = n).
 HPLB_DEV void solve_system(const Args& a, const Sys& y, double* P, Smem& S) {
   const int n = y.n, nrhs = y.nrhs, nb = y.nb;
-  const int ldp = n;
+  const int ldp = panel_ld(n);
   double*   A  = a.A + y.a_off;
   double*   B  = a.B + y.b_off;
   int*      ip = a.ipiv + y.p_off;
   if(threadIdx.x == 0) S.info = 0;
   for(int k0 = 0; k0 < n; k0 += nb) {
     const int kb = min(nb, n - k0), m = n - k0;
-    // Panel to shared memory.
+    double*   Ap = A + k0 + (size_t)k0 * n;
     __syncthreads();
+    if(kb <= kRegPanelW && m <= 2 * kBT) {
+      if(m <= kBT) {
+        if(kb <= 8)
+          panel_reg<1, 8>(Ap, n, m, kb, k0, ip, P, ldp, S);
+        else
+          panel_reg<1, 16>(Ap, n, m, kb, k0, ip, P, ldp, S);
+      } else {
+        if(kb <= 8)
+          panel_reg<2, 8>(Ap, n, m, kb, k0, ip, P, ldp, S);
+        else
+          panel_reg<2, 16>(Ap, n, m, kb, k0, ip, P, ldp, S);
+      }
+    } else {
+    // Panel to shared memory.
     for(int idx = threadIdx.x; idx < kb * m; idx += kBT) {
       const int c = idx / m, i = idx % m;
       P[(size_t)c * ldp + i] = A[(size_t)(k0 + i) + (size_t)(k0 + c) * n];
@@ -355,6 +560,7 @@ HPLB_DEV void solve_system(const Args& a, const Sys& y, double* P, Smem& S) {
       const int c = idx / m, i = idx % m;
       A[(size_t)(k0 + i) + (size_t)(k0 + c) * n] = P[(size_t)c * ldp + i];
     }
+    }  // shared-memory panel
     // The panel's interchanges as a row map (each thread x < kb traces one
     // position through the kb swaps).
     if(threadIdx.x < kb) {
@@ -409,12 +615,10 @@ HPLB_DEV void solve_system(const Args& a, const Sys& y, double* P, Smem& S) {
     }
     __syncthreads();
     if(rest + nrhs > 0) {
-      // A22 -= L21 U12, B2 -= L21 B1.
-      tile_gemm_sub(rest, rest, kb, A + (k0 + kb) + (size_t)k0 * n, n,
-                    A + k0 + (size_t)(k0 + kb) * n, n, A + (k0 + kb) + (size_t)(k0 + kb) * n, n,
-                    S);
-      tile_gemm_sub(rest, nrhs, kb, A + (k0 + kb) + (size_t)k0 * n, n, B + k0, n, B + (k0 + kb),
-                    n, S);
+      // A22 -= L21 U12, B2 -= L21 B1 (L21 from the panel copy in shared memory).
+      update_strips(P, ldp, kb, rest, A + k0 + (size_t)(k0 + kb) * n, n,
+                    A + (k0 + kb) + (size_t)(k0 + kb) * n, n, rest, S);
+      update_strips(P, ldp, kb, rest, B + k0, n, B + (k0 + kb), n, nrhs, S);
     }
   }
   // U X = B.

@@ -56,7 +56,8 @@ hplb_status batch_err(hplb_batch* b, hplb_status s, const char* msg) {
 // staged solution columns (8n doubles).
 size_t dyn_bytes(const hplb_batch* b) {
   size_t m = 8;
-  for(int i = 0; i < b->count; ++i) m = std::max(m, (size_t)b->nb[i] * b->n[i] * sizeof(double));
+  for(int i = 0; i < b->count; ++i)
+    m = std::max(m, (size_t)b->nb[i] * ((b->n[i] + 15) / 16 * 16 + 4) * sizeof(double));
   m = std::max(m, (size_t)9 * b->n_max * sizeof(double));
   return m;
 }
@@ -159,7 +160,7 @@ hplb_status hplb_batch_create(hplb_ctx* ctx, int count, const int* n, const int*
   b->p_off.resize(count);
   for(int i = 0; i < count; ++i) {
     int w = (nb_by_class ? nb_by_class : kDefaultNb)[size_class(n[i])];
-    while(w > 8 && (size_t)w * n[i] * sizeof(double) > budget) w /= 2;
+    while(w > 8 && (size_t)w * ((n[i] + 15) / 16 * 16 + 4) * sizeof(double) > budget) w /= 2;
     b->nb[i]    = w;
     b->a_off[i] = b->a_total;
     b->b_off[i] = b->b_total;
@@ -332,7 +333,7 @@ hplb_status hplb_batch_tune(hplb_ctx* ctx, int nrhs, int* nb_by_class, double* m
     nb_by_class[c] = kDefaultNb[c];
     for(int q = 0; q < 3; ++q) {
       if(ms_table) ms_table[c * 3 + q] = -1.0;
-      if((size_t)cand[q] * n * sizeof(double) > budget) continue;
+      if((size_t)cand[q] * ((n + 15) / 16 * 16 + 4) * sizeof(double) > budget) continue;
       int table[HPLB_BATCH_CLASSES];
       for(int z = 0; z < HPLB_BATCH_CLASSES; ++z) table[z] = cand[q];
       std::vector<int> nv(count, n), rv(count, nrhs);
