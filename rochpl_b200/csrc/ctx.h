@@ -43,6 +43,7 @@ struct hplb_ctx {
   float*          m_g     = nullptr;  size_t m_g_cap     = 0;  // gathered rows
   unsigned short* m_l16   = nullptr;  size_t m_l16_cap   = 0;  // packed L21
   unsigned short* m_u16   = nullptr;  size_t m_u16_cap   = 0;  // packed U12
+  unsigned short* m_li16  = nullptr;  size_t m_li16_cap  = 0;  // packed -L11^-1
   float*          m_scale = nullptr;  size_t m_scale_cap = 0;  // tile scales
   float*          m_small = nullptr;  size_t m_small_cap = 0;  // inverses' scratch
   double*         m_vec   = nullptr;  size_t m_vec_cap   = 0;  // FP64 vectors

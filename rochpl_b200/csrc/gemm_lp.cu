@@ -371,7 +371,18 @@ cudaError_t launch_gemm_lp(bool bf16, int m, int n, int k, const void* A16, int6
   }
   const int tiles_m = (m + LBM - 1) / LBM, tiles_n = (n + LBN - 1) / LBN;
   const long long ntiles = (long long)tiles_m * tiles_n;
-  const int tpc = 8;
+  // Up to 8 tiles per CTA (CTAs retire regularly, so the panel stream running
+  // beside this kernel gets SMs), balanced so the CTA count fills whole waves
+  // of one CTA per SM.
+  static int sms = 0;
+  if(sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if(sms < 1) sms = 1;
+  }
+  const long long waves = (ntiles + (long long)sms * 8 - 1) / ((long long)sms * 8);
+  const int tpc = (int)((ntiles + (long long)sms * waves - 1) / ((long long)sms * waves));
   const long long grid = (ntiles + tpc - 1) / tpc;
   if(bf16)
     gemm_lp_kernel<true><<<(unsigned)grid, L_THREADS, L_SMEM, stream>>>(

@@ -270,7 +270,7 @@ void hplb_destroy(hplb_ctx* ctx) {
                   ctx->d_w,       ctx->m_w,       ctx->m_linv,        ctx->m_uinv,
                   ctx->m_perm,    ctx->m_g,       ctx->m_l16,         ctx->m_u16,
                   ctx->m_scale,   ctx->m_small,   ctx->m_vec,         ctx->r_t,
-                  ctx->r_ws,      ctx->r_perm};
+                  ctx->r_ws,      ctx->r_perm,    ctx->m_li16};
   for(void* b : bufs)
     if(b) cudaFree(b);
   if(ctx->s_upd) cudaStreamDestroy(ctx->s_upd);

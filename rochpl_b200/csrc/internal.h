@@ -81,11 +81,12 @@ cudaError_t launch_sgemm(int m, int n, int k, const float* A, int64_t lda, const
                          int64_t ldb, float* C, int64_t ldc, bool accumulate, cudaStream_t stream);
 cudaError_t launch_f64_to_f32(int m, int n, const double* A, int64_t lda, float* W, int64_t ldw,
                               cudaStream_t st);
-// split: three jb-wide segments per packed row (hi/lo parts, K = 3 jb).
+// split: three jb-wide segments per packed row (hi/lo parts, K = 3 jb).  The
+// values are multiplied by sign (1 or -1) along with the tile scale.
 cudaError_t launch_pack_l(bool bf16, bool split, int m, int jb, const float* L, int64_t ld,
-                          void* out, int64_t ldo, float* sL, cudaStream_t st);
+                          void* out, int64_t ldo, float* sL, cudaStream_t st, float sign = 1.f);
 cudaError_t launch_pack_u(bool bf16, bool split, int jb, int n, const float* U, int64_t ld,
-                          void* out, int64_t ldo, float* sU, cudaStream_t st);
+                          void* out, int64_t ldo, float* sU, cudaStream_t st, float sign = 1.f);
 // Uinv = U^-1 for the upper-triangular U (jb x jb at U, leading dimension
 // ld); work: 2 jb^2 + jb elements, dinv_work: (jb/32 + 1) * 1024.
 template <typename T>

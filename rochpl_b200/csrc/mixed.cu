@@ -88,12 +88,34 @@ HPLB_DEV void put16(unsigned short* row, int k, int jb, float x) {
   }
 }
 
+// Eight consecutive values (already scaled) of one packed row, stored as one
+// 16-byte vector per segment; VEC needs k and jb multiples of 8.
+template <bool BF16, bool SPLIT, bool IS_L>
+HPLB_DEV void put16x8(unsigned short* row, int k, int jb, const float (&x)[8]) {
+  union {
+    unsigned short h[8];
+    uint4          v;
+  } hi, lo;
+#pragma unroll
+  for(int i = 0; i < 8; ++i) {
+    hi.h[i] = to16<BF16>(x[i]);
+    lo.h[i] = SPLIT ? to16<BF16>(x[i] - from16<BF16>(hi.h[i])) : (unsigned short)0;
+  }
+  *reinterpret_cast<uint4*>(row + k) = hi.v;
+  if(SPLIT) {
+    *reinterpret_cast<uint4*>(row + jb + k)     = IS_L ? hi.v : lo.v;
+    *reinterpret_cast<uint4*>(row + 2 * jb + k) = IS_L ? lo.v : hi.v;
+  }
+}
+
 // L21 (m x jb, column-major, leading dimension ld) -> out (m x ldo row-major
-// 16-bit), one 128-row tile per block.
+// 16-bit), one 128-row tile per block: a max pass for the tile's scale, then
+// 32-column chunks transposed through shared memory and stored 8 values (16
+// bytes) at a time per segment.
 template <bool BF16, bool SPLIT>
 __global__ void __launch_bounds__(256)
 pack_l_kernel(int m, int jb, const float* __restrict__ L, int64_t ld,
-              unsigned short* __restrict__ out, int64_t ldo, float* __restrict__ sL) {
+              unsigned short* __restrict__ out, int64_t ldo, float* __restrict__ sL, float sign) {
   __shared__ float tile[128][33];
   __shared__ float sh[32];
   const int r0 = blockIdx.x * 128;
@@ -105,6 +127,8 @@ pack_l_kernel(int m, int jb, const float* __restrict__ L, int64_t ld,
   float s, inv;
   pow2_scale(mx, s, inv);
   if(threadIdx.x == 0) sL[blockIdx.x] = inv;
+  s *= sign;
+  const bool vec = (jb & 7) == 0;
   for(int cb = 0; cb < jb; cb += 32) {
     for(int c = cq; c < 32; c += 2)
       tile[rr][c] = (r0 + rr < m && cb + c < jb) ? L[(size_t)(r0 + rr) + (size_t)(cb + c) * ld]
@@ -114,9 +138,18 @@ pack_l_kernel(int m, int jb, const float* __restrict__ L, int64_t ld,
     if(r0 + r < m) {
       unsigned short* o = out + (size_t)(r0 + r) * ldo;
 #pragma unroll
-      for(int q = 0; q < 16; ++q) {
-        const int k = cb + half * 16 + q;
-        if(k < jb) put16<BF16, SPLIT, true>(o, k, jb, tile[r][half * 16 + q] * s);
+      for(int g8 = 0; g8 < 2; ++g8) {
+        const int k = cb + half * 16 + g8 * 8;
+        if(vec && k + 8 <= jb) {
+          float x[8];
+#pragma unroll
+          for(int q = 0; q < 8; ++q) x[q] = tile[r][half * 16 + g8 * 8 + q] * s;
+          put16x8<BF16, SPLIT, true>(o, k, jb, x);
+        } else {
+#pragma unroll
+          for(int q = 0; q < 8; ++q)
+            if(k + q < jb) put16<BF16, SPLIT, true>(o, k + q, jb, tile[r][half * 16 + g8 * 8 + q] * s);
+        }
       }
     }
     __syncthreads();
@@ -124,27 +157,58 @@ pack_l_kernel(int m, int jb, const float* __restrict__ L, int64_t ld,
 }
 
 // U12 (jb x n, column-major, leading dimension ld) -> out (n x ldo row-major:
-// column c's jb values contiguous), one 256-column tile per block.
-template <bool BF16, bool SPLIT>
-__global__ void __launch_bounds__(256)
+// column c's jb values contiguous), one 256-column tile per block of 1024
+// threads: a max pass for the tile's scale, then the pack pass, both with
+// float4 loads and 8-byte stores of four 16-bit values when jb, ld and U
+// allow (VEC), else one value at a time.
+template <bool BF16, bool SPLIT, bool VEC>
+__global__ void __launch_bounds__(1024)
 pack_u_kernel(int jb, int n, const float* __restrict__ U, int64_t ld,
-              unsigned short* __restrict__ out, int64_t ldo, float* __restrict__ sU) {
+              unsigned short* __restrict__ out, int64_t ldo, float* __restrict__ sU, float sign) {
   __shared__ float sh[32];
   const int c0 = blockIdx.x * 256;
   const int nc = min(256, n - c0);
-  float mx = 0.f;
-  for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
-    const int c = idx / jb, k = idx - c * jb;
-    mx = fmaxf(mx, fabsf(U[(size_t)k + (size_t)(c0 + c) * ld]));
+  const int W  = VEC ? jb / 4 : jb;  // items per column
+  float     mx = 0.f;
+  for(int idx = threadIdx.x; idx < nc * W; idx += blockDim.x) {
+    const int c = idx / W, k = idx - c * W;
+    const float* col = U + (size_t)(c0 + c) * ld;
+    if(VEC) {
+      const float4 v = *reinterpret_cast<const float4*>(col + 4 * k);
+      mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+    } else {
+      mx = fmaxf(mx, fabsf(col[k]));
+    }
   }
   mx = block_max_f(mx, sh);
   float s, inv;
   pow2_scale(mx, s, inv);
   if(threadIdx.x == 0) sU[blockIdx.x] = inv;
-  for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
-    const int c = idx / jb, k = idx - c * jb;
-    put16<BF16, SPLIT, false>(out + (size_t)(c0 + c) * ldo, k, jb,
-                              U[(size_t)k + (size_t)(c0 + c) * ld] * s);
+  s *= sign;
+  for(int idx = threadIdx.x; idx < nc * W; idx += blockDim.x) {
+    const int c = idx / W, k = idx - c * W;
+    const float*    col = U + (size_t)(c0 + c) * ld;
+    unsigned short* o   = out + (size_t)(c0 + c) * ldo;
+    if(VEC) {
+      const float4 v = *reinterpret_cast<const float4*>(col + 4 * k);
+      const float  x[4] = {v.x * s, v.y * s, v.z * s, v.w * s};
+      union {
+        unsigned short h[4];
+        uint2          v;
+      } hi, lo;
+#pragma unroll
+      for(int i = 0; i < 4; ++i) {
+        hi.h[i] = to16<BF16>(x[i]);
+        lo.h[i] = SPLIT ? to16<BF16>(x[i] - from16<BF16>(hi.h[i])) : (unsigned short)0;
+      }
+      *reinterpret_cast<uint2*>(o + 4 * k) = hi.v;
+      if(SPLIT) {
+        *reinterpret_cast<uint2*>(o + jb + 4 * k)     = lo.v;
+        *reinterpret_cast<uint2*>(o + 2 * jb + 4 * k) = hi.v;
+      }
+    } else {
+      put16<BF16, SPLIT, false>(o, k, jb, col[k] * s);
+    }
   }
 }
 
@@ -352,34 +416,46 @@ cudaError_t launch_f64_to_f32(int m, int n, const double* A, int64_t lda, float*
 }
 
 cudaError_t launch_pack_l(bool bf16, bool split, int m, int jb, const float* L, int64_t ld,
-                          void* out, int64_t ldo, float* sL, cudaStream_t st) {
+                          void* out, int64_t ldo, float* sL, cudaStream_t st, float sign) {
   if(m <= 0 || jb <= 0) return cudaSuccess;
+  if(ldo % 8) return cudaErrorInvalidValue;  // 16-byte rows for the vector stores
   const int       grid = (m + 127) / 128;
   unsigned short* o    = (unsigned short*)out;
   if(bf16 && split)
-    pack_l_kernel<true, true><<<grid, 256, 0, st>>>(m, jb, L, ld, o, ldo, sL);
+    pack_l_kernel<true, true><<<grid, 256, 0, st>>>(m, jb, L, ld, o, ldo, sL, sign);
   else if(bf16)
-    pack_l_kernel<true, false><<<grid, 256, 0, st>>>(m, jb, L, ld, o, ldo, sL);
+    pack_l_kernel<true, false><<<grid, 256, 0, st>>>(m, jb, L, ld, o, ldo, sL, sign);
   else if(split)
-    pack_l_kernel<false, true><<<grid, 256, 0, st>>>(m, jb, L, ld, o, ldo, sL);
+    pack_l_kernel<false, true><<<grid, 256, 0, st>>>(m, jb, L, ld, o, ldo, sL, sign);
   else
-    pack_l_kernel<false, false><<<grid, 256, 0, st>>>(m, jb, L, ld, o, ldo, sL);
+    pack_l_kernel<false, false><<<grid, 256, 0, st>>>(m, jb, L, ld, o, ldo, sL, sign);
   return cudaGetLastError();
 }
 
+template <bool BF16, bool SPLIT>
+static void pack_u_any(bool vec, int grid, int jb, int n, const float* U, int64_t ld,
+                       unsigned short* o, int64_t ldo, float* sU, float sign, cudaStream_t st) {
+  if(vec)
+    pack_u_kernel<BF16, SPLIT, true><<<grid, 1024, 0, st>>>(jb, n, U, ld, o, ldo, sU, sign);
+  else
+    pack_u_kernel<BF16, SPLIT, false><<<grid, 1024, 0, st>>>(jb, n, U, ld, o, ldo, sU, sign);
+}
+
 cudaError_t launch_pack_u(bool bf16, bool split, int jb, int n, const float* U, int64_t ld,
-                          void* out, int64_t ldo, float* sU, cudaStream_t st) {
+                          void* out, int64_t ldo, float* sU, cudaStream_t st, float sign) {
   if(n <= 0 || jb <= 0) return cudaSuccess;
   const int       grid = (n + 255) / 256;
   unsigned short* o    = (unsigned short*)out;
+  const bool vec = (jb % 4 == 0) && (ld % 4 == 0) && ((uintptr_t)U % 16 == 0) && (ldo % 4 == 0) &&
+                   ((uintptr_t)out % 16 == 0);
   if(bf16 && split)
-    pack_u_kernel<true, true><<<grid, 256, 0, st>>>(jb, n, U, ld, o, ldo, sU);
+    pack_u_any<true, true>(vec, grid, jb, n, U, ld, o, ldo, sU, sign, st);
   else if(bf16)
-    pack_u_kernel<true, false><<<grid, 256, 0, st>>>(jb, n, U, ld, o, ldo, sU);
+    pack_u_any<true, false>(vec, grid, jb, n, U, ld, o, ldo, sU, sign, st);
   else if(split)
-    pack_u_kernel<false, true><<<grid, 256, 0, st>>>(jb, n, U, ld, o, ldo, sU);
+    pack_u_any<false, true>(vec, grid, jb, n, U, ld, o, ldo, sU, sign, st);
   else
-    pack_u_kernel<false, false><<<grid, 256, 0, st>>>(jb, n, U, ld, o, ldo, sU);
+    pack_u_any<false, false>(vec, grid, jb, n, U, ld, o, ldo, sU, sign, st);
   return cudaGetLastError();
 }
 

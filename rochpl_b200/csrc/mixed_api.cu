@@ -14,6 +14,8 @@
 // of right-preconditioned flexible GMRES for A d = r, x += d.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
+#include <cstring>
 #include <vector>
 
 #include "ctx.h"
@@ -21,6 +23,16 @@
 using namespace hplb;
 
 namespace {
+
+// U12 = L11^-1 G by the FP32 SIMT GEMM instead of the tensor cores in the x3
+// modes (HPLB_MIXED_U12=simt, kept for comparison).
+bool u12_simt() {
+  static const bool v = [] {
+    const char* e = getenv("HPLB_MIXED_U12");
+    return e && strcmp(e, "simt") == 0;
+  }();
+  return v;
+}
 
 struct Mixed {
   hplb_ctx*        ctx;
@@ -130,8 +142,22 @@ struct Mixed {
     float*       sL = ctx->m_scale;
     float*       sU = ctx->m_scale + ((size_t)n + 127) / 128 + 1;
     CK(launch_laswp_gather<float>(W, ldw, j, jb, perm(p), ctx->m_g, jb, c, wd, su));
-    CK(launch_sgemm(jb, wd, jb, linv(p), jb, ctx->m_g, jb, w(j, c), ldw, false, su));
-    ctx->launches += 2;
+    if(split && !u12_simt()) {
+      // U12 = L11^-1 G on the tensor cores, with the split operands of the
+      // trailing update (FP32-accurate): C = 0, then C -= (-L11^-1) G.
+      float* sLi = sU + ((size_t)n + 255) / 256 + 1;
+      float* sG  = sLi + 32;
+      CK(launch_pack_l(bf16, true, jb, jb, linv(p), jb, ctx->m_li16, ldp, sLi, su, -1.f));
+      CK(launch_pack_u(bf16, true, jb, wd, ctx->m_g, jb, ctx->m_u16, ldp, sG, su));
+      CK(cudaMemset2DAsync(w(j, c), (size_t)ldw * sizeof(float), 0, (size_t)jb * sizeof(float), wd,
+                           su));
+      CK(launch_gemm_lp(bf16, jb, wd, 3 * jb, ctx->m_li16, ldp, ctx->m_u16, ldp, sLi, sG, w(j, c),
+                        ldw, ctx->d_status, su));
+      ctx->launches += 5;
+    } else {
+      CK(launch_sgemm(jb, wd, jb, linv(p), jb, ctx->m_g, jb, w(j, c), ldw, false, su));
+      ctx->launches += 2;
+    }
     if(m <= 0) return HPLB_OK;
     if(pack_l) CK(launch_pack_l(bf16, split, m, jb, w(c1, j), ldw, ctx->m_l16, ldp, sL, su));
     CK(launch_pack_u(bf16, split, jb, wd, w(j, c), ldw, ctx->m_u16, ldp, sU, su));
@@ -375,7 +401,8 @@ extern "C" hplb_status hplb_pdgesv_mixed(hplb_ctx* ctx, const hplb_algo* algo,
      (s = grow(ctx, &ctx->m_g, &ctx->m_g_cap, (size_t)nb * n)) != HPLB_OK ||
      (s = grow(ctx, &ctx->m_l16, &ctx->m_l16_cap, (size_t)M.ldp * n)) != HPLB_OK ||
      (s = grow(ctx, &ctx->m_u16, &ctx->m_u16_cap, (size_t)M.ldp * n)) != HPLB_OK ||
-     (s = grow(ctx, &ctx->m_scale, &ctx->m_scale_cap, (size_t)n / 64 + 8)) != HPLB_OK ||
+     (s = grow(ctx, &ctx->m_scale, &ctx->m_scale_cap, (size_t)n / 64 + 96)) != HPLB_OK ||
+     (s = grow(ctx, &ctx->m_li16, &ctx->m_li16_cap, (size_t)M.ldp * nb)) != HPLB_OK ||
      (s = grow(ctx, &ctx->m_small, &ctx->m_small_cap,
                2 * nblk * 1024 + 2 * (size_t)nb * nb + nb + 64)) != HPLB_OK ||
      (s = grow(ctx, &ctx->m_vec, &ctx->m_vec_cap, Refine::doubles(n, o.restart))) != HPLB_OK ||
