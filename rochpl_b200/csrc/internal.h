@@ -93,8 +93,11 @@ template <typename T>
 cudaError_t launch_upper_inverse(int jb, const T* U, int64_t ld, T* Uinv, T* work, T* dinv_work,
                                  cudaStream_t st);
 cudaError_t launch_perm_vec(double* z, int ia, int jb, const int* permU, cudaStream_t st);
-cudaError_t launch_tri_apply(const float* T, int jb, double* z, int o, cudaStream_t st);
+// y -= M x / y = M x with FP32 M (rows x cols, column-major), FP64 x and y
+// (not overlapping).
 cudaError_t launch_gemv_sub(int rows, int cols, const float* M, int64_t ld, const double* x,
+                            double* y, cudaStream_t st);
+cudaError_t launch_gemv_set(int rows, int cols, const float* M, int64_t ld, const double* x,
                             double* y, cudaStream_t st);
 int         vec_partials();
 cudaError_t launch_dot(int n, const double* a, const double* b, double* part, double* out,

@@ -12,8 +12,8 @@
 //   upper_flip_*        U11^-1 through the unit-lower inverse: with D = diag(U),
 //                       U = D Ut and J the reversal, J Ut J is unit lower, so
 //                       U^-1 = J (J Ut J)^-1 J D^-1
-//   perm_vec, tri_apply, gemv_sub   the preconditioner M^-1 = U^-1 L^-1 P
-//                       applied to an FP64 vector panel by panel
+//   perm_vec, gemv_rows  the preconditioner M^-1 = U^-1 L^-1 P applied to an
+//                       FP64 vector panel by panel (FP32 factors, FP64 sums)
 //   dot / amax / axpy   deterministic FP64 vector kernels for GMRES
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -260,38 +260,40 @@ __global__ void perm_vec_kernel(double* z, int ia, int jb, const int* __restrict
   for(int x = threadIdx.x; x < jb && nx < 8; x += blockDim.x, ++nx) z[ia + x] = v[nx];
 }
 
-// z[o : o+jb] <- T z[o : o+jb] with T (jb x jb, FP32, leading dimension jb).
-// One block; the vector block is staged in shared memory.
-__global__ void tri_apply_kernel(const float* __restrict__ T, int jb, double* z, int o) {
-  extern __shared__ double zs[];
-  for(int i = threadIdx.x; i < jb; i += blockDim.x) zs[i] = z[o + i];
-  __syncthreads();
-  for(int i = threadIdx.x; i < jb; i += blockDim.x) {
-    double acc = 0.0;
-    for(int c = 0; c < jb; ++c) acc += (double)T[(size_t)i + (size_t)c * jb] * zs[c];
-    z[o + i] = acc;
-  }
-}
-
-// y[0:rows] -= M (rows x cols, FP32, column-major) x[0:cols], FP64 accumulate.
+// y = M x (SUB = false) or y -= M x (SUB = true) for an FP32 M (rows x cols,
+// column-major) and FP64 x, y: 32 rows per block, the 8 warps on slices of the
+// columns (lane = row, so each column's 32 rows are one 128-byte read), FP64
+// accumulation, then a fixed-order sum of the 8 slices.  x and y must not
+// overlap.
+template <bool SUB>
 __global__ void __launch_bounds__(256)
-gemv_sub_kernel(int rows, int cols, const float* __restrict__ M, int64_t ld,
-                const double* __restrict__ x, double* __restrict__ y) {
+gemv_rows_kernel(int rows, int cols, const float* __restrict__ M, int64_t ld,
+                 const double* __restrict__ x, double* __restrict__ y) {
   __shared__ double xs[512];
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  double acc = 0.0;
+  __shared__ double part[8][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r    = blockIdx.x * 32 + lane;
+  double    acc  = 0.0;
   for(int c0 = 0; c0 < cols; c0 += 512) {
     const int nc = min(512, cols - c0);
     __syncthreads();
-    for(int i = threadIdx.x; i < nc; i += blockDim.x) xs[i] = x[c0 + i];
+    for(int i = threadIdx.x; i < nc; i += 256) xs[i] = x[c0 + i];
     __syncthreads();
+    const int cs = (nc + 7) / 8, a = warp * cs, b = min(nc, a + cs);
     if(r < rows) {
       const float* m = M + (size_t)r + (size_t)c0 * ld;
 #pragma unroll 8
-      for(int c = 0; c < nc; ++c) acc += (double)m[(size_t)c * ld] * xs[c];
+      for(int c = a; c < b; ++c) acc += (double)m[(size_t)c * ld] * xs[c];
     }
   }
-  if(r < rows) y[r] -= acc;
+  part[warp][lane] = acc;
+  __syncthreads();
+  if(warp == 0 && r < rows) {
+    double t = 0.0;
+#pragma unroll
+    for(int w = 0; w < 8; ++w) t += part[w][lane];
+    y[r] = SUB ? y[r] - t : t;
+  }
 }
 
 // ---- FP64 vector kernels (fixed-order, deterministic reductions) ----
@@ -488,16 +490,17 @@ cudaError_t launch_perm_vec(double* z, int ia, int jb, const int* permU, cudaStr
   return cudaGetLastError();
 }
 
-cudaError_t launch_tri_apply(const float* T, int jb, double* z, int o, cudaStream_t st) {
-  if(jb <= 0) return cudaSuccess;
-  tri_apply_kernel<<<1, 512, jb * sizeof(double), st>>>(T, jb, z, o);
-  return cudaGetLastError();
-}
-
 cudaError_t launch_gemv_sub(int rows, int cols, const float* M, int64_t ld, const double* x,
                             double* y, cudaStream_t st) {
   if(rows <= 0 || cols <= 0) return cudaSuccess;
-  gemv_sub_kernel<<<(rows + 255) / 256, 256, 0, st>>>(rows, cols, M, ld, x, y);
+  gemv_rows_kernel<true><<<(rows + 31) / 32, 256, 0, st>>>(rows, cols, M, ld, x, y);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_gemv_set(int rows, int cols, const float* M, int64_t ld, const double* x,
+                            double* y, cudaStream_t st) {
+  if(rows <= 0) return cudaSuccess;
+  gemv_rows_kernel<false><<<(rows + 31) / 32, 256, 0, st>>>(rows, cols, M, ld, x, y);
   return cudaGetLastError();
 }
 

@@ -199,24 +199,71 @@ struct Mixed {
     return HPLB_OK;
   }
 
-  // z <- M^-1 z (update stream).
-  hplb_status precond(double* z) {
+  // The preconditioner M^-1 = U^-1 L^-1 P applied to the fixed vector pv
+  // (update stream): per panel forward, the row map, pv_top = L11^-1 pv_top
+  // (out of place through ptmp), pv_rest -= L21 pv_top; per panel backward,
+  // pv_top = U11^-1 pv_top, pv_above -= U12' pv_top.
+  double*         pv     = nullptr;  // n doubles
+  double*         ptmp   = nullptr;  // nb doubles
+  cudaGraphExec_t pgraph = nullptr;
+  int             plaunches = 0;
+
+  hplb_status precond_body() {
     hplb_ctx*    ctx = this->ctx;
     cudaStream_t su  = ctx->s_upd;
     for(int p = 0; p < npan; ++p) {
       const int j = p * nb, jb = std::min(nb, n - j);
-      CK(launch_perm_vec(z, j, jb, perm(p), su));
-      CK(launch_tri_apply(linv(p), jb, z, j, su));
-      CK(launch_gemv_sub(n - j - jb, jb, w(j + jb, j), ldw, z + j, z + j + jb, su));
-      ctx->launches += j + jb < n ? 3 : 2;
+      CK(launch_perm_vec(pv, j, jb, perm(p), su));
+      CK(launch_gemv_set(jb, jb, linv(p), jb, pv + j, ptmp, su));
+      CK(cudaMemcpyAsync(pv + j, ptmp, (size_t)jb * sizeof(double), cudaMemcpyDeviceToDevice, su));
+      CK(launch_gemv_sub(n - j - jb, jb, w(j + jb, j), ldw, pv + j, pv + j + jb, su));
+      plaunches += j + jb < n ? 3 : 2;
     }
     for(int p = npan - 1; p >= 0; --p) {
       const int j = p * nb, jb = std::min(nb, n - j);
-      CK(launch_tri_apply(uinv(p), jb, z, j, su));
-      CK(launch_gemv_sub(j, jb, w(0, j), ldw, z + j, z, su));
-      ctx->launches += j > 0 ? 2 : 1;
+      CK(launch_gemv_set(jb, jb, uinv(p), jb, pv + j, ptmp, su));
+      CK(cudaMemcpyAsync(pv + j, ptmp, (size_t)jb * sizeof(double), cudaMemcpyDeviceToDevice, su));
+      CK(launch_gemv_sub(j, jb, w(0, j), ldw, pv + j, pv, su));
+      plaunches += j > 0 ? 2 : 1;
     }
     return HPLB_OK;
+  }
+
+  // The sweep is captured once per factorisation as a CUDA graph (about
+  // 1800 small launches per application otherwise).
+  hplb_status build_precond() {
+    hplb_ctx*   ctx = this->ctx;
+    cudaGraph_t g   = nullptr;
+    plaunches       = 0;
+    CK(cudaStreamBeginCapture(ctx->s_upd, cudaStreamCaptureModeThreadLocal));
+    hplb_status s  = precond_body();
+    cudaError_t e  = cudaStreamEndCapture(ctx->s_upd, &g);
+    if(s == HPLB_OK && e == cudaSuccess) e = cudaGraphInstantiate(&pgraph, g, 0);
+    if(g) cudaGraphDestroy(g);
+    if(s != HPLB_OK) return s;
+    if(e != cudaSuccess) {
+      cudaGetLastError();
+      pgraph = nullptr;
+      return set_err(ctx, HPLB_ERR_CUDA, "preconditioner graph: %s", cudaGetErrorString(e));
+    }
+    return HPLB_OK;
+  }
+
+  // z <- M^-1 z (update stream).
+  hplb_status precond(double* z) {
+    hplb_ctx*    ctx = this->ctx;
+    cudaStream_t su  = ctx->s_upd;
+    hplb_status  s;
+    if(!pgraph && (s = build_precond()) != HPLB_OK) return s;
+    CK(cudaMemcpyAsync(pv, z, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, su));
+    CK(cudaGraphLaunch(pgraph, su));
+    CK(cudaMemcpyAsync(z, pv, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, su));
+    ctx->launches += plaunches;
+    return HPLB_OK;
+  }
+
+  ~Mixed() {
+    if(pgraph) cudaGraphExecDestroy(pgraph);
   }
 };
 
@@ -405,7 +452,8 @@ extern "C" hplb_status hplb_pdgesv_mixed(hplb_ctx* ctx, const hplb_algo* algo,
      (s = grow(ctx, &ctx->m_li16, &ctx->m_li16_cap, (size_t)M.ldp * nb)) != HPLB_OK ||
      (s = grow(ctx, &ctx->m_small, &ctx->m_small_cap,
                2 * nblk * 1024 + 2 * (size_t)nb * nb + nb + 64)) != HPLB_OK ||
-     (s = grow(ctx, &ctx->m_vec, &ctx->m_vec_cap, Refine::doubles(n, o.restart))) != HPLB_OK ||
+     (s = grow(ctx, &ctx->m_vec, &ctx->m_vec_cap,
+               Refine::doubles(n, o.restart) + (size_t)n + nb + 16)) != HPLB_OK ||
      (s = grow(ctx, &ctx->d_res, &ctx->res_cap, residual_ws_doubles(n))) != HPLB_OK)
     return s;
   M.W = ctx->m_w;
@@ -464,6 +512,8 @@ extern "C" hplb_status hplb_pdgesv_mixed(hplb_ctx* ctx, const hplb_algo* algo,
   F.lcg     = dA == nullptr;
   F.seed    = seed;
   F.carve(ctx->m_vec);
+  M.pv   = ctx->m_vec + Refine::doubles(n, o.restart);
+  M.ptmp = M.pv + n;
   // ||A||oo, ||b||oo and eps from the residual kernels at x = 0.
   CK(cudaMemsetAsync(dX, 0, (size_t)n * sizeof(double), su));
   CK(launch_residual(n, dA, ld, F.lcg, seed, dX, ctx->d_res, ctx->d_out8, su));
