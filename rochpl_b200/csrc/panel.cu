@@ -16,6 +16,7 @@
 //  laswp_trsm_kernel-- fused row interchange (HPL_dlaswp00N) + unit-lower TRSM
 //                      (rocblas_dtrsm, src/pgesv/HPL_pdupdateTT.cpp:95-106)
 //                      over a block of columns held in shared memory.
+#include <algorithm>
 #include <cooperative_groups.h>
 #include <cstdlib>
 #include <cstring>
@@ -785,7 +786,14 @@ static cudaError_t try_leaf_reg(const LeafParams<T>& P, int rows, int sms, int g
                                 cudaStream_t stream, bool* done) {
   constexpr int kMaxRpt = sizeof(T) == 8 ? 3 : 4;
   *done                 = false;
-  for(int rpt = 1; rpt <= kMaxRpt; ++rpt) {
+  // HPLB_LEAF_RPT=k starts the search at k rows per thread (fewer, fuller
+  // blocks: a smaller gang to co-schedule beside the trailing update).
+  static const int first = [] {
+    const char* e = getenv("HPLB_LEAF_RPT");
+    const int   v = e ? atoi(e) : 1;
+    return v < 1 ? 1 : v;
+  }();
+  for(int rpt = std::min(first, kMaxRpt); rpt <= kMaxRpt; ++rpt) {
     const int cap = rpt * kRegLeafThreads;
     const int g   = (rows + cap - 1) / cap;
     if(g > sms || g > grid) continue;
