@@ -257,44 +257,17 @@ gemm_lp_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     int it = 0;
     for(int t = t_begin; t < t_end; ++t, ++it) {
       const int buf = it & 1;
-      int       tm, tn;
-      tile_of(t, tiles_m, tiles_n, tm, tn);
-      const int r0    = tm * LBM + sub * 32;
-      const int row   = r0 + lane;
-      const int cbase = tn * LBN + half * (LBN / 2);
-      // While the tile's MMAs run: this warp's 32 rows x 128 columns of C into
-      // L2 (one 128-byte line per column) and its first 32 columns into
-      // registers.  C is only written by this epilogue, so reading it early
-      // is safe.
-      if(r0 < m)
-        for(int j = lane; j < LBN / 2; j += 32)
-          if(cbase + j < n)
-            asm volatile("prefetch.global.L2 [%0];" ::"l"(C + (size_t)r0 + (size_t)(cbase + j) * ldc));
-      float cn[32];
-#pragma unroll
-      for(int j = 0; j < 32; ++j)
-        cn[j] = (row < m && cbase + j < n) ? C[(size_t)row + (size_t)(cbase + j) * ldc] : 0.f;
       if(!bar_wait(&accf[buf], (uint32_t)((it >> 1) & 1), &s_abort)) {
         if(lane == 0) atomicCAS(status + ST_TIMEOUT, 0, 34);
         s_abort = 1;
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      int tm, tn;
+      tile_of(t, tiles_m, tiles_n, tm, tn);
+      const int   row   = tm * LBM + sub * 32 + lane;
       const float scale = sA[tm] * sB[tn];
-#pragma unroll 1
-      for(int q = 0; q < LBN / 2 / 32; ++q) {
-        const int c0 = half * (LBN / 2) + q * 32;
-        const int col0 = cbase + q * 32;
-        float     cv[32];
-#pragma unroll
-        for(int j = 0; j < 32; ++j) cv[j] = cn[j];
-        if(q + 1 < LBN / 2 / 32) {  // next chunk's C in flight during this one
-#pragma unroll
-          for(int j = 0; j < 32; ++j)
-            cn[j] = (row < m && col0 + 32 + j < n)
-                        ? C[(size_t)row + (size_t)(col0 + 32 + j) * ldc]
-                        : 0.f;
-        }
+      for(int c0 = half * (LBN / 2); c0 < (half + 1) * (LBN / 2); c0 += 32) {
         uint32_t r[32];
         const uint32_t taddr = tmem + ((uint32_t)(sub * 32) << 16) + (uint32_t)(buf * LBN + c0);
         asm volatile(
@@ -310,6 +283,11 @@ gemm_lp_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
             : "r"(taddr));
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
         if(row < m) {
+          float cv[32];
+          const int col0 = tn * LBN + c0;
+#pragma unroll
+          for(int j = 0; j < 32; ++j)
+            cv[j] = (col0 + j < n) ? C[(size_t)row + (size_t)(col0 + j) * ldc] : 0.f;
 #pragma unroll
           for(int j = 0; j < 32; ++j)
             if(col0 + j < n)
