@@ -153,13 +153,18 @@ hplb_status hplb_rank_k(hplb_ctx* ctx, int m, int n, int k, double alpha, const 
  * ------------------------------------------------------------------------ */
 #define HPLB_BATCH_CLASSES 6   /* size classes: n < 48, < 96, < 192, < 384, < 768, >= 768 */
 #define HPLB_BATCH_MAX_N 2048
+/* Class entry selecting the recursive factorisation (columns halved down to
+ * 16-wide leaves, GEMM updates with k up to n/2) for systems with n <=
+ * HPLB_BATCH_RECURSIVE_MAX_N; larger systems of the class use 16-wide panels. */
+#define HPLB_BATCH_RECURSIVE 64
+#define HPLB_BATCH_RECURSIVE_MAX_N 1024
 
 typedef struct hplb_batch hplb_batch;
 
-/* Plan a batch (host arrays n, nrhs of length count).  nb_by_class: panel
- * width (8, 16 or 32) per size class, e.g. from hplb_batch_tune; NULL for the
- * built-in table.  Widths are lowered where a panel would not fit in shared
- * memory. */
+/* Plan a batch (host arrays n, nrhs of length count).  nb_by_class: per size
+ * class, a right-looking panel width (8, 16 or 32) or HPLB_BATCH_RECURSIVE,
+ * e.g. from hplb_batch_tune; NULL for the built-in table.  Widths are lowered
+ * where a panel would not fit in shared memory. */
 hplb_status hplb_batch_create(hplb_ctx* ctx, int count, const int* n, const int* nrhs,
                               const int* nb_by_class, hplb_batch** out);
 void        hplb_batch_destroy(hplb_batch* b);
@@ -187,10 +192,10 @@ hplb_status hplb_batch_residual(hplb_batch* b, const uint64_t* seeds, const doub
                                 double* dresid);
 /* Device time of the last batch call (ms). */
 hplb_status hplb_batch_last_ms(const hplb_batch* b, double* ms);
-/* The autotuner: times panel widths 8 / 16 / 32 on a batch of each size class
- * (2 x SM-count systems, nrhs right-hand sides) and writes the fastest to
- * nb_by_class; ms_table (6 x 3, may be NULL) receives every timing, -1 where a
- * width does not fit. */
+/* The autotuner: times panel widths 8 / 16 / 32 and the recursive
+ * factorisation on a batch of each size class (2 x SM-count systems, nrhs
+ * right-hand sides) and writes the fastest to nb_by_class; ms_table (6 x 4,
+ * may be NULL) receives every timing, -1 where a candidate does not fit. */
 hplb_status hplb_batch_tune(hplb_ctx* ctx, int nrhs, int* nb_by_class, double* ms_table);
 
 /* The HPL residual check: dA must hold the regenerated [A|b] (hplb_matgen with

@@ -128,11 +128,11 @@ def autotune(lib: Library, nrhs: int = 16, use_cache: bool = True) -> list[int]:
         if key in cache:
             return [int(v) for v in cache[key]["nb_by_class"]]
     nb = (C.c_int * HPLB_BATCH_CLASSES)()
-    ms = (C.c_double * (HPLB_BATCH_CLASSES * 3))()
+    ms = (C.c_double * (HPLB_BATCH_CLASSES * 4))()
     st = lib.L.hplb_batch_tune(lib.ctx, nrhs, nb, ms)
     lib._check(st)
     table = [int(v) for v in nb]
-    cache[key] = {"nb_by_class": table, "ms_nb8_16_32": [float(v) for v in ms]}
+    cache[key] = {"nb_by_class": table, "ms_nb8_16_32_recursive": [float(v) for v in ms]}
     try:
         os.makedirs(os.path.dirname(_CACHE), exist_ok=True)
         with open(_CACHE, "w") as f:

@@ -34,6 +34,7 @@ constexpr int kNbMax = 32;   // widest panel
 constexpr int kTile  = 64;   // output tile of the block updates
 constexpr int kLdT   = kTile + 4;
 constexpr int kRegPanelW = 16;  // widest panel held in registers
+constexpr int kRecMode   = 64;  // Sys::nb value selecting the recursive factorisation
 
 // Leading dimension of the panel copy in shared memory: >= n rows and = 4
 // (mod 16), so the DMMA A-fragment loads (rows g, columns t) hit distinct banks.
@@ -430,7 +431,7 @@ HPLB_DEV void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, dou
       for(int c = 0; c < KB; ++c)
         if(c < kb) {
           Ag[(size_t)row[q] + (size_t)c * lda] = x[q][c];
-          P[(size_t)c * ldp + row[q]]          = x[q][c];
+          if(P) P[(size_t)c * ldp + row[q]] = x[q][c];
         }
   __syncthreads();
 }
@@ -631,6 +632,224 @@ HPLB_DEV void solve_system(const Args& a, const Sys& y, double* P, Smem& S) {
   if(threadIdx.x == 0) a.info[&y - a.sys] = S.info;
 }
 
+// ---- recursive per-system factorisation ----
+
+constexpr int kRecLeaf = 16;  // leaf width of the recursive factorisation
+constexpr int kGk      = 32;  // k depth of one staged chunk of gemm_nn_sub
+
+// C (m x n) -= A (m x k) B (k x n), all column-major in global memory, any k:
+// 64 x 64 C tiles, each accumulated in DMMA fragments over the whole k (C is
+// read and written once per call), operands staged 32 deep in shared memory
+// (G: two buffers of A 32 x 64 and B 64 x 32), the next chunk loaded into
+// registers while the current one is multiplied.  16 warps in 4 x 4, each 16
+// rows x 16 columns.
+HPLB_DEV void gemm_nn_sub(int m, int n, int k, const double* A, int64_t lda, const double* B,
+                          int64_t ldb, double* C, int64_t ldc, double* G) {
+  if(m <= 0 || n <= 0 || k <= 0) return;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 3) * 16, wn = (warp >> 2) * 16;
+  constexpr int LDA_S = kTile + 4;  // A stage: [k][row], rows padded
+  constexpr int LDB_S = kGk + 4;    // B stage: [col][k], k padded (= 4 mod 16)
+  constexpr int STAGE = kGk * LDA_S + kTile * LDB_S;
+  const int tm = (m + kTile - 1) / kTile, tn = (n + kTile - 1) / kTile;
+  const int nck = (k + kGk - 1) / kGk;
+  // Each thread moves 4 A and 4 B elements per chunk.
+  for(int tile = 0; tile < tm * tn; ++tile) {
+    const int m0 = (tile % tm) * kTile, n0 = (tile / tm) * kTile;
+    double    ra[4], rb[4];
+    auto fetch = [&](int ck) {
+#pragma unroll
+      for(int q = 0; q < 4; ++q) {
+        const int e = threadIdx.x + q * kBT;  // 0 .. 2047
+        const int r = e & (kTile - 1), kk = e >> 6;   // A: 64 rows x 32 k
+        const int gk = ck * kGk + kk;
+        ra[q] = (m0 + r < m && gk < k) ? A[(size_t)(m0 + r) + (size_t)gk * lda] : 0.0;
+        const int k2 = e & (kGk - 1), c = e >> 5;     // B: 32 k x 64 cols
+        const int gk2 = ck * kGk + k2;
+        rb[q] = (n0 + c < n && gk2 < k) ? B[(size_t)gk2 + (size_t)(n0 + c) * ldb] : 0.0;
+      }
+    };
+    auto stash = [&](int buf) {
+      double* As = G + buf * STAGE;
+      double* Bs = As + kGk * LDA_S;
+#pragma unroll
+      for(int q = 0; q < 4; ++q) {
+        const int e = threadIdx.x + q * kBT;
+        As[(e >> 6) * LDA_S + (e & (kTile - 1))] = ra[q];
+        Bs[(e >> 5) * LDB_S + (e & (kGk - 1))]   = rb[q];
+      }
+    };
+    double acc[2][4];
+#pragma unroll
+    for(int j = 0; j < 2; ++j)
+#pragma unroll
+      for(int q = 0; q < 4; ++q) {
+        const int r = m0 + wm + g + (q >> 1) * 8, c = n0 + wn + j * 8 + 2 * t + (q & 1);
+        acc[j][q] = (r < m && c < n) ? C[(size_t)r + (size_t)c * ldc] : 0.0;
+      }
+    fetch(0);
+    __syncthreads();  // the previous tile's readers of G are done
+    stash(0);
+    __syncthreads();
+    for(int ck = 0; ck < nck; ++ck) {
+      const int buf = ck & 1;
+      if(ck + 1 < nck) fetch(ck + 1);
+      const double* As = G + buf * STAGE;
+      const double* Bs = As + kGk * LDA_S;
+#pragma unroll
+      for(int kk = 0; kk < kGk; kk += 8) {
+        double af[4];
+        af[0] = -As[(kk + t) * LDA_S + wm + g];
+        af[1] = -As[(kk + t) * LDA_S + wm + g + 8];
+        af[2] = -As[(kk + t + 4) * LDA_S + wm + g];
+        af[3] = -As[(kk + t + 4) * LDA_S + wm + g + 8];
+#pragma unroll
+        for(int j = 0; j < 2; ++j) {
+          double bf[2];
+          bf[0] = Bs[(wn + j * 8 + g) * LDB_S + kk + t];
+          bf[1] = Bs[(wn + j * 8 + g) * LDB_S + kk + t + 4];
+          dmma(acc[j], af, bf);
+        }
+      }
+      if(ck + 1 < nck) stash(buf ^ 1);
+      __syncthreads();
+    }
+#pragma unroll
+    for(int j = 0; j < 2; ++j)
+#pragma unroll
+      for(int q = 0; q < 4; ++q) {
+        const int r = m0 + wm + g + (q >> 1) * 8, c = n0 + wn + j * 8 + 2 * t + (q & 1);
+        if(r < m && c < n) C[(size_t)r + (size_t)c * ldc] = acc[j][q];
+      }
+  }
+  __syncthreads();
+}
+
+// One leaf of the recursive factorisation: columns [c0, c0 + w) (w <= 16) of
+// rows [c0, n), in registers, then its interchanges on every other column of
+// A and of B (full rows, as LAPACK's getrf).
+HPLB_DEV void rec_leaf(double* A, double* B, int n, int nrhs, int* ip, int c0, int w, double* P,
+                       Smem& S) {
+  const int m = n - c0;
+  double*   Ap = A + c0 + (size_t)c0 * n;
+  const int ldp = panel_ld(n);
+  __syncthreads();
+  if(m <= kBT)
+    panel_reg<1, kRecLeaf>(Ap, n, m, w, c0, ip, P, ldp, S);
+  else
+    panel_reg<2, kRecLeaf>(Ap, n, m, w, c0, ip, P, ldp, S);
+  if(threadIdx.x < w) {
+    const int x = threadIdx.x;
+    int       pos = x;
+    for(int i = w - 1; i >= 0; --i) {
+      const int p = S.piv[i];
+      pos         = (pos == i) ? p : (pos == p ? i : pos);
+    }
+    S.src[x] = pos;
+    pos      = x;
+    for(int i = 0; i < w; ++i) {
+      const int p = S.piv[i];
+      pos         = (pos == i) ? p : (pos == p ? i : pos);
+    }
+    S.dst[x] = pos >= w ? pos : -1;
+  }
+  __syncthreads();
+  const int ncol = n - w + nrhs;
+  for(int q = threadIdx.x; q < ncol; q += kBT) {
+    double* col = q < c0 ? A + (size_t)q * n
+                         : (q < n - w ? A + (size_t)(q + w) * n : B + (size_t)(q - (n - w)) * n);
+    col += c0;
+    double x[kRecLeaf], o[kRecLeaf];
+#pragma unroll
+    for(int r = 0; r < kRecLeaf; ++r)
+      if(r < w) {
+        x[r] = col[S.src[r]];
+        o[r] = S.dst[r] >= 0 ? col[r] : 0.0;
+      }
+#pragma unroll
+    for(int r = 0; r < kRecLeaf; ++r)
+      if(r < w && S.dst[r] >= 0) col[S.dst[r]] = o[r];
+#pragma unroll
+    for(int r = 0; r < kRecLeaf; ++r)
+      if(r < w) col[r] = x[r];
+  }
+  __syncthreads();
+}
+
+// X (w1 x ncols, leading dimension ldx) <- L^-1 X for the unit-lower w1 x w1 L
+// at L (leading dimension ldl): 32-row blocks, substitution on the diagonal
+// block, DMMA update of the rows below.
+HPLB_DEV void trsm_lower_unit(int w1, int ncols, const double* L, int64_t ldl, double* X,
+                              int64_t ldx, double* G, Smem& S) {
+  for(int rb = 0; rb < w1; rb += kNbMax) {
+    const int kb = min(kNbMax, w1 - rb);
+    load_diag(L + rb + (size_t)rb * ldl, ldl, kb, S);
+    diag_solve<LOWER_UNIT>(kb, X + rb, ldx, ncols, S);
+    gemm_nn_sub(w1 - rb - kb, ncols, kb, L + (rb + kb) + (size_t)rb * ldl, ldl, X + rb, ldx,
+                X + rb + kb, ldx, G);
+  }
+}
+
+// Recursive factorisation of one system (the columns split in halves down to
+// 16-wide leaves, an explicit stack in place of recursion), then X = U^-1
+// L^-1 B by blocks (B took every interchange as it happened).
+HPLB_DEV void solve_system_rec(const Args& a, const Sys& y, double* P, double* G, Smem& S) {
+  const int n = y.n, nrhs = y.nrhs;
+  double*   A  = a.A + y.a_off;
+  double*   B  = a.B + y.b_off;
+  int*      ip = a.ipiv + y.p_off;
+  if(threadIdx.x == 0) S.info = 0;
+  int c0s[12], ws[12], w1s[12], stage[12];
+  int top = 0;
+  c0s[0] = 0, ws[0] = n, stage[0] = 0;
+  while(top >= 0) {
+    const int c0 = c0s[top], w = ws[top];
+    if(w <= kRecLeaf) {
+      rec_leaf(A, B, n, nrhs, ip, c0, w, P, S);
+      --top;
+      continue;
+    }
+    if(stage[top] == 0) {
+      const int w1 = ((w / 2 + kRecLeaf - 1) / kRecLeaf) * kRecLeaf;
+      w1s[top]     = w1 < w ? w1 : w - kRecLeaf;
+      stage[top]   = 1;
+      ++top;
+      c0s[top] = c0, ws[top] = w1s[top - 1], stage[top] = 0;
+    } else if(stage[top] == 1) {
+      const int w1 = w1s[top], w2 = w - w1;
+      // U12 = L11^-1 A12, then A22 -= L21 U12 (rows c0 + w1 .. n).
+      trsm_lower_unit(w1, w2, A + c0 + (size_t)c0 * n, n, A + c0 + (size_t)(c0 + w1) * n, n, G, S);
+      gemm_nn_sub(n - c0 - w1, w2, w1, A + (c0 + w1) + (size_t)c0 * n, n,
+                  A + c0 + (size_t)(c0 + w1) * n, n, A + (c0 + w1) + (size_t)(c0 + w1) * n, n, G);
+      stage[top] = 2;
+      ++top;
+      c0s[top] = c0 + w1, ws[top] = w2, stage[top] = 0;
+    } else {
+      --top;
+    }
+  }
+  // L Y = B (forward, 32-row blocks), then U X = Y (backward).
+  for(int k0 = 0; k0 < n; k0 += kNbMax) {
+    const int kb = min(kNbMax, n - k0);
+    load_diag(A + k0 + (size_t)k0 * n, n, kb, S);
+    diag_solve<LOWER_UNIT>(kb, B + k0, n, nrhs, S);
+    gemm_nn_sub(n - k0 - kb, nrhs, kb, A + (k0 + kb) + (size_t)k0 * n, n, B + k0, n, B + k0 + kb,
+                n, G);
+  }
+  for(int k0 = (n - 1) / kNbMax * kNbMax; k0 >= 0; k0 -= kNbMax) {
+    const int kb = min(kNbMax, n - k0);
+    load_diag(A + k0 + (size_t)k0 * n, n, kb, S);
+    diag_solve<UPPER>(kb, B + k0, n, nrhs, S);
+    gemm_nn_sub(k0, nrhs, kb, A + (size_t)k0 * n, n, B + k0, n, B, n, G);
+  }
+  if(threadIdx.x == 0) a.info[&y - a.sys] = S.info;
+}
+
+// Dynamic shared memory of the recursive mode: the GEMM's two stages (the
+// leaves keep no panel copy).
+__host__ __device__ constexpr int rec_stage_doubles() { return 2 * (kGk * (kTile + 4) + kTile * (kGk + 4)); }
+
 __global__ void __launch_bounds__(kBT, 1) batch_gesv_kernel(const Args* pa) {
   extern __shared__ __align__(16) double panel_smem[];
   __shared__ Smem S;
@@ -638,7 +857,11 @@ __global__ void __launch_bounds__(kBT, 1) batch_gesv_kernel(const Args* pa) {
   for(;;) {
     const int s = next_system(a, S);
     if(s < 0) break;
-    solve_system(a, a.sys[s], panel_smem, S);
+    const Sys& y = a.sys[s];
+    if(y.nb == kRecMode)
+      solve_system_rec(a, y, nullptr, panel_smem, S);
+    else
+      solve_system(a, y, panel_smem, S);
   }
 }
 
@@ -947,6 +1170,7 @@ __global__ void __launch_bounds__(kBT, 1) batch_residual_kernel(const Args* pa) 
 // ---------------------------------------------------------------------------
 
 size_t batch_static_smem() { return sizeof(Smem); }
+size_t batch_rec_stage_bytes() { return (size_t)rec_stage_doubles() * sizeof(double); }
 int    batch_threads() { return kBT; }
 int    batch_nb_max() { return kNbMax; }
 

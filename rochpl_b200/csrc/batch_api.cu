@@ -57,7 +57,9 @@ hplb_status batch_err(hplb_batch* b, hplb_status s, const char* msg) {
 size_t dyn_bytes(const hplb_batch* b) {
   size_t m = 8;
   for(int i = 0; i < b->count; ++i)
-    m = std::max(m, (size_t)b->nb[i] * ((b->n[i] + 15) / 16 * 16 + 4) * sizeof(double));
+    m = std::max(m, b->nb[i] == HPLB_BATCH_RECURSIVE
+                        ? batch_rec_stage_bytes()
+                        : (size_t)b->nb[i] * ((b->n[i] + 15) / 16 * 16 + 4) * sizeof(double));
   m = std::max(m, (size_t)9 * b->n_max * sizeof(double));
   return m;
 }
@@ -143,8 +145,10 @@ hplb_status hplb_batch_create(hplb_ctx* ctx, int count, const int* n, const int*
   }
   if(nb_by_class)
     for(int c = 0; c < HPLB_BATCH_CLASSES; ++c)
-      if(nb_by_class[c] != 8 && nb_by_class[c] != 16 && nb_by_class[c] != 32)
-        return set_err(ctx, HPLB_ERR_ARG, "hplb_batch_create: panel widths must be 8, 16 or 32");
+      if(nb_by_class[c] != 8 && nb_by_class[c] != 16 && nb_by_class[c] != 32 &&
+         nb_by_class[c] != HPLB_BATCH_RECURSIVE)
+        return set_err(ctx, HPLB_ERR_ARG,
+                       "hplb_batch_create: class entries must be 8, 16, 32 or HPLB_BATCH_RECURSIVE");
   ENTER(ctx);
   size_t      budget = 0;
   hplb_status sb     = dyn_budget(ctx, &budget);
@@ -160,7 +164,10 @@ hplb_status hplb_batch_create(hplb_ctx* ctx, int count, const int* n, const int*
   b->p_off.resize(count);
   for(int i = 0; i < count; ++i) {
     int w = (nb_by_class ? nb_by_class : kDefaultNb)[size_class(n[i])];
-    while(w > 8 && (size_t)w * ((n[i] + 15) / 16 * 16 + 4) * sizeof(double) > budget) w /= 2;
+    if(w == HPLB_BATCH_RECURSIVE && n[i] > HPLB_BATCH_RECURSIVE_MAX_N) w = 16;
+    while(w != HPLB_BATCH_RECURSIVE && w > 8 &&
+          (size_t)w * ((n[i] + 15) / 16 * 16 + 4) * sizeof(double) > budget)
+      w /= 2;
     b->nb[i]    = w;
     b->a_off[i] = b->a_total;
     b->b_off[i] = b->b_total;
@@ -316,13 +323,14 @@ hplb_status hplb_batch_last_ms(const hplb_batch* b, double* ms) {
 
 // The autotuner: for each size class, a batch of 2 x (SM count) systems of the
 // class's representative size is generated and solved with each candidate
-// panel width; the fastest width (best of three timed graph launches after a
+// (right-looking panels of 8, 16 or 32 columns, or the recursive
+// factorisation); the fastest (best of three timed graph launches after a
 // warm-up) goes into nb_by_class.
 hplb_status hplb_batch_tune(hplb_ctx* ctx, int nrhs, int* nb_by_class, double* ms_table) {
   if(!ctx) return HPLB_ERR_ARG;
   if(!nb_by_class || nrhs < 0) return set_err(ctx, HPLB_ERR_ARG, "hplb_batch_tune: bad argument");
   ENTER(ctx);
-  static const int cand[3] = {8, 16, 32};
+  static const int cand[4] = {8, 16, 32, HPLB_BATCH_RECURSIVE};
   size_t           budget  = 0;
   hplb_status      sb      = dyn_budget(ctx, &budget);
   if(sb != HPLB_OK) return sb;
@@ -331,9 +339,11 @@ hplb_status hplb_batch_tune(hplb_ctx* ctx, int nrhs, int* nb_by_class, double* m
     const int n    = kTuneN[c];
     double    best = 1e30;
     nb_by_class[c] = kDefaultNb[c];
-    for(int q = 0; q < 3; ++q) {
-      if(ms_table) ms_table[c * 3 + q] = -1.0;
-      if((size_t)cand[q] * ((n + 15) / 16 * 16 + 4) * sizeof(double) > budget) continue;
+    for(int q = 0; q < 4; ++q) {
+      if(ms_table) ms_table[c * 4 + q] = -1.0;
+      if(cand[q] != HPLB_BATCH_RECURSIVE &&
+         (size_t)cand[q] * ((n + 15) / 16 * 16 + 4) * sizeof(double) > budget)
+        continue;
       int table[HPLB_BATCH_CLASSES];
       for(int z = 0; z < HPLB_BATCH_CLASSES; ++z) table[z] = cand[q];
       std::vector<int> nv(count, n), rv(count, nrhs);
@@ -366,7 +376,7 @@ hplb_status hplb_batch_tune(hplb_ctx* ctx, int nrhs, int* nb_by_class, double* m
       cudaFree(dI);
       hplb_batch_destroy(b);
       if(s != HPLB_OK) return s;
-      if(ms_table) ms_table[c * 3 + q] = t;
+      if(ms_table) ms_table[c * 4 + q] = t;
       if(t < best) {
         best           = t;
         nb_by_class[c] = cand[q];

@@ -134,6 +134,7 @@ cudaError_t launch_check_ipiv(int n, const int* ipiv, int* status, cudaStream_t 
 
 // Batched solver kernels (batch.cu); the plan and C ABI are in batch_api.cu.
 size_t      batch_static_smem();
+size_t      batch_rec_stage_bytes();  // dynamic shared memory of the recursive mode
 int         batch_threads();
 int         batch_nb_max();
 // Sets the kernels' dynamic shared-memory limits; *budget = what a plan may use.

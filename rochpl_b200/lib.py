@@ -34,6 +34,8 @@ EXPORTS = [
 
 HPLB_BATCH_CLASSES = 6
 HPLB_BATCH_MAX_N = 2048
+HPLB_BATCH_RECURSIVE = 64
+HPLB_BATCH_RECURSIVE_MAX_N = 1024
 
 
 class hplb_algo(C.Structure):

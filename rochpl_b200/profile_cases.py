@@ -7,6 +7,7 @@
     python -m rochpl_b200.profile_cases mixed 131072 3    # hplb_pdgesv_mixed (N, precision), with
                                                           # a per-kernel breakdown from CUPTI tracing
     python -m rochpl_b200.profile_cases batch 1024 16     # 592 systems of one size (N, NB), nrhs 16
+                                                          # (NB 64: the recursive factorisation)
 
 Each case prints its event-timed rate, so the same command can be run plainly
 before it is run under a profiler.

@@ -39,11 +39,14 @@ SIZES = [1, 2, 7, 31, 32, 33, 47, 64, 100, 129, 257, 400, 513, 700, 1024]
 
 
 @pytest.mark.parametrize("nrhs", [1, 16, 64])
-def test_batch_gesv_matches_lapack(hlib, oracle, nrhs):
+@pytest.mark.parametrize("mode", ["default", "recursive"])
+def test_batch_gesv_matches_lapack(hlib, oracle, nrhs, mode):
     import scipy.linalg as sl
 
+    from rochpl_b200.lib import HPLB_BATCH_RECURSIVE
+
     n = np.array(SIZES, dtype=np.int32)
-    plan = _plan(hlib, n, nrhs)
+    plan = _plan(hlib, n, nrhs, None if mode == "default" else [HPLB_BATCH_RECURSIVE] * 6)
     seeds = 100 + np.arange(plan.count, dtype=np.uint64)
     dA, dB, dP, dI = _pools(plan)
     plan.matgen(seeds, dA.data_ptr(), dB.data_ptr())
