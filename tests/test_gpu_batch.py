@@ -189,7 +189,7 @@ def test_batch_autotuner_and_workload(hlib):
     from rochpl_b200.batch import autotune, workload_sizes
 
     table = autotune(hlib, nrhs=1, use_cache=False)
-    assert len(table) == 6 and all(v in (8, 16, 32) for v in table)
+    assert len(table) == 6 and all(v in (8, 16, 32, 64) for v in table)
     n = workload_sizes(512)
     assert n.min() >= 32 and n.max() <= 1024
     plan = _plan(hlib, n, 1, table)
