@@ -54,6 +54,10 @@ cudaError_t launch_laswp_trsm(T* A, int64_t ld, int ia, int jb, int lc, const in
 template <typename T>
 cudaError_t launch_unit_lower_inverse(const T* L, int64_t ldl, int jb, const T* dinv, T* Linv,
                                       int64_t ldinv, cudaStream_t stream);
+// X (jb x n) <- L^-1 X for the unit-lower L at L (leading dimension ldl) with
+// its 32 x 32 diagonal inverses dinv (launch_diag_inv), FP64.
+cudaError_t launch_trsm_unit_lower(double* X, int64_t ldx, int jb, const double* L, int64_t ldl,
+                                   const double* dinv, int n, cudaStream_t stream);
 // Panel interchanges on columns [c0, c0+n): new top rows gathered into W
 // (jb x n, leading dimension ldw), displaced rows written in place.
 template <typename T>
@@ -121,6 +125,19 @@ cudaError_t launch_matgen_f32(int m, int n, uint64_t seed, float* W, int64_t ld,
 template <typename T>
 cudaError_t launch_transpose(int m, int n, const T* src, int64_t lds, T* dst, int64_t ldd,
                              cudaStream_t st);
+// The unit-lower jb x jb matrix (leading dimension jb) equivalent to the
+// diagonal block T (leading dimension ldt) of the LU factors for a solve:
+//   kind 0 (U):   J D^-1 U J,   with D = diag(U) written to d
+//   kind 1 (L^T): J L^T J
+//   kind 2 (U^T): (D^-1 U)^T,   with D to d
+// (J reverses the order of rows and columns.)
+cudaError_t launch_unit_lower_view(int kind, int jb, const double* T, int64_t ldt, double* out,
+                                   double* d, cudaStream_t st);
+// out (jb x n, leading dimension ldo) = in with rows reversed (flip) and / or
+// divided by d (scale; d indexed by the source row).
+cudaError_t launch_rows_xform(int jb, int n, const double* in, int64_t ldi, double* out,
+                              int64_t ldo, const double* d, bool flip, bool scale,
+                              cudaStream_t st);
 // Inverse of a panel's row map on columns [0, n) of B: rows moved back to where
 // the forward interchanges took them from.
 cudaError_t launch_laswp_inverse(double* B, int64_t ldb, int ia, int jb, const int* permU, int n,

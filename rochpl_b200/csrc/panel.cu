@@ -951,6 +951,13 @@ cudaError_t launch_laswp_trsm(T* A, int64_t ld, int ia, int jb, int lc, const in
                             n, stream);
 }
 
+// X (jb x n, leading dimension ldx) <- L^-1 X for the unit-lower jb x jb L at
+// L (leading dimension ldl), dinv its 32 x 32 diagonal inverses (diag_inv).
+cudaError_t launch_trsm_unit_lower(double* X, int64_t ldx, int jb, const double* L, int64_t ldl,
+                                   const double* dinv, int n, cudaStream_t stream) {
+  return launch_trsm_any<double>(X, ldx, 0, jb, L, ldl, nullptr, dinv, 0, n, stream);
+}
+
 template <typename T>
 cudaError_t launch_unit_lower_inverse(const T* L, int64_t ldl, int jb, const T* dinv, T* Linv,
                                       int64_t ldinv, cudaStream_t stream) {

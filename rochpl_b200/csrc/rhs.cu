@@ -101,6 +101,40 @@ rank_k_kernel(int m, int n, int k, double alpha, const double* __restrict__ A, i
   }
 }
 
+__global__ void unit_lower_view_kernel(int kind, int jb, const double* __restrict__ T,
+                                       int64_t ldt, double* __restrict__ out,
+                                       double* __restrict__ d) {
+  const int c = blockIdx.x;
+  for(int r = threadIdx.x; r < jb; r += blockDim.x) {
+    double v = r == c ? 1.0 : 0.0;
+    if(r > c) {
+      if(kind == 0) {  // (J D^-1 U J)[r][c] = U[jb-1-r][jb-1-c] / U[jb-1-r][jb-1-r]
+        const int ur = jb - 1 - r, uc = jb - 1 - c;
+        v = T[(size_t)ur + (size_t)uc * ldt] / T[(size_t)ur + (size_t)ur * ldt];
+      } else if(kind == 1) {  // (J L^T J)[r][c] = L[jb-1-c][jb-1-r]
+        v = T[(size_t)(jb - 1 - c) + (size_t)(jb - 1 - r) * ldt];
+      } else {  // ((D^-1 U)^T)[r][c] = U[c][r] / U[c][c]
+        v = T[(size_t)c + (size_t)r * ldt] / T[(size_t)c + (size_t)c * ldt];
+      }
+    }
+    out[(size_t)r + (size_t)c * jb] = v;
+  }
+  if(c == 0 && kind != 1)
+    for(int i = threadIdx.x; i < jb; i += blockDim.x) d[i] = T[(size_t)i + (size_t)i * ldt];
+}
+
+__global__ void rows_xform_kernel(int jb, const double* __restrict__ in, int64_t ldi,
+                                  double* __restrict__ out, int64_t ldo,
+                                  const double* __restrict__ d, int flip, int scale) {
+  const int c = blockIdx.x;
+  for(int i = threadIdx.x; i < jb; i += blockDim.x) {
+    const int src = flip ? jb - 1 - i : i;
+    double    v   = in[(size_t)src + (size_t)c * ldi];
+    if(scale) v = v / d[src];
+    out[(size_t)i + (size_t)c * ldo] = v;
+  }
+}
+
 __global__ void check_ipiv_kernel(int n, const int* __restrict__ ipiv, int* status) {
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     if(ipiv[i] < i || ipiv[i] >= n) record_info(status, i + 1);
@@ -141,6 +175,22 @@ cudaError_t launch_rank_k(int m, int n, int k, double alpha, const double* A, in
     rank_k_kernel<true><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, C, ldc);
   else
     rank_k_kernel<false><<<grid, 256, 0, st>>>(m, n, k, alpha, A, lda, B, ldb, C, ldc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_unit_lower_view(int kind, int jb, const double* T, int64_t ldt, double* out,
+                                   double* d, cudaStream_t st) {
+  if(jb <= 0) return cudaSuccess;
+  unit_lower_view_kernel<<<jb, 256, 0, st>>>(kind, jb, T, ldt, out, d);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows_xform(int jb, int n, const double* in, int64_t ldi, double* out,
+                              int64_t ldo, const double* d, bool flip, bool scale,
+                              cudaStream_t st) {
+  if(jb <= 0 || n <= 0) return cudaSuccess;
+  if(n > 65535) return cudaErrorInvalidValue;
+  rows_xform_kernel<<<n, 256, 0, st>>>(jb, in, ldi, out, ldo, d, flip ? 1 : 0, scale ? 1 : 0);
   return cudaGetLastError();
 }
 

@@ -10,9 +10,11 @@
 //   A^-1 = U^-1 E_{np-1} P_{np-1} ... E_0 P_0,  E_p = [L11^-1 0; -L21 L11^-1 I]
 // and
 //   A^-T = P_0^T E_0^T ... P_{np-1}^T E_{np-1}^T U^-T.
-// Every block product is a DMMA GEMM of this library (the diagonal blocks
-// through their explicit inverses, as in the trailing update); the transposed
-// solve reads a transposed copy of the factors so that its GEMMs are plain NN.
+// The off-diagonal block products are DMMA GEMMs of this library; the
+// diagonal blocks are solved by the blocked substitution kernel (explicit
+// inverses of 512 x 512 blocks would cost far more than a few right-hand
+// sides); the transposed solve reads a transposed copy of the factors so that
+// its GEMMs are plain NN.
 #include <algorithm>
 
 #include "ctx.h"
@@ -29,48 +31,47 @@ struct Rhs {
   const int*    ipiv;
   double*       B;
   int64_t       ldb;
-  double *      W, *M1, *M2, *work, *dinv, *dinv_piece, *T;
+  double *      W, *M1, *dvec, *dinv, *T;
   int64_t       ldt;  // rows of T: n rounded up to 16, + 16, so a 16-row slab never leaves it
   int*          perm;
   cudaStream_t  st;
 
   static size_t ws_doubles(int nb, int nrhs) {
     const size_t nblk = (size_t)nb / 32 + 1;
-    return (size_t)nb * nrhs + 4 * (size_t)nb * nb + nb + 2 * nblk * 1024 + 64;
+    return (size_t)nb * nrhs + (size_t)nb * nb + nb + nblk * 1024 + 64;
   }
   void carve(double* base) {
-    const size_t nblk = (size_t)nb / 32 + 1;
-    W          = base;
-    M1         = W + (size_t)nb * nrhs;
-    M2         = M1 + (size_t)nb * nb;
-    work       = M2 + (size_t)nb * nb;  // 2 nb^2 + nb
-    dinv       = work + 2 * (size_t)nb * nb + nb;
-    dinv_piece = dinv + nblk * 1024;
+    W    = base;
+    M1   = W + (size_t)nb * nrhs;
+    dvec = M1 + (size_t)nb * nb;
+    dinv = dvec + nb;
   }
 
   const double* lu(int i, int j) const { return LU + (size_t)i + (size_t)j * (size_t)ld; }
   double*       b(int i) const { return B + i; }
   const double* t(int i, int j) const { return T + (size_t)i + (size_t)j * (size_t)ldt; }
 
-  // B[j : j + jb] <- Mx B[j : j + jb] (Mx jb x jb, leading dimension jb).
-  hplb_status apply_block(const double* Mx, int j, int jb) {
-    hplb_ctx* ctx = this->ctx;
-    CK(cudaMemcpy2DAsync(W, (size_t)jb * sizeof(double), b(j), (size_t)ldb * sizeof(double),
-                         (size_t)jb * sizeof(double), nrhs, cudaMemcpyDeviceToDevice, st));
-    CK(launch_dgemm_set(jb, nrhs, jb, Mx, jb, W, jb, b(j), ldb, ctx->d_status, st));
-    ctx->launches += 1;
-    return HPLB_OK;
-  }
-  hplb_status lower_inv(int j, int jb, double* out) {
+  // B[j : j + jb] <- L11^-1 B[j : j + jb], the unit-lower diagonal block of
+  // panel j, by the blocked substitution (32 x 32 diagonal inverses, then
+  // updates of the rows below), in place.
+  hplb_status solve_lower(int j, int jb) {
     hplb_ctx* ctx = this->ctx;
     CK(launch_diag_inv<double>(LU, ld, j, j, jb, dinv, st));
-    CK(launch_unit_lower_inverse<double>(lu(j, j), ld, jb, dinv, out, jb, st));
-    ctx->launches += 3;
+    CK(launch_trsm_unit_lower(b(j), ldb, jb, lu(j, j), ld, dinv, nrhs, st));
+    ctx->launches += 2;
     return HPLB_OK;
   }
-  hplb_status upper_inv(int j, int jb, double* out) {
+  // B[j : j + jb] <- S^-1 B[j : j + jb] for S = U11 (kind 0), L11^T (kind 1)
+  // or U11^T (kind 2), each solved as the unit-lower system it is equivalent
+  // to (launch_unit_lower_view): U x = b is (J D^-1 U J)(J x) = J D^-1 b,
+  // L^T x = b is (J L^T J)(J x) = J b, U^T x = b is (D^-1 U)^T (D x) = b.
+  hplb_status solve_view(int kind, int j, int jb) {
     hplb_ctx* ctx = this->ctx;
-    CK(launch_upper_inverse<double>(jb, lu(j, j), ld, out, work, dinv_piece, st));
+    CK(launch_unit_lower_view(kind, jb, lu(j, j), ld, M1, dvec, st));
+    CK(launch_diag_inv<double>(M1, jb, 0, 0, jb, dinv, st));
+    CK(launch_rows_xform(jb, nrhs, b(j), ldb, W, jb, dvec, kind != 2, kind == 0, st));
+    CK(launch_trsm_unit_lower(W, jb, jb, M1, jb, dinv, nrhs, st));
+    CK(launch_rows_xform(jb, nrhs, W, jb, b(j), ldb, dvec, kind != 2, kind == 2, st));
     ctx->launches += 5;
     return HPLB_OK;
   }
@@ -83,16 +84,16 @@ struct Rhs {
       const int jb = std::min(nb, n - j);
       CK(launch_perm(ipiv + j, j, jb, perm, st));
       CK(launch_laswp_gather<double>(B, ldb, j, jb, perm, W, jb, 0, nrhs, st));
-      if((s = lower_inv(j, jb, M1)) != HPLB_OK) return s;
-      CK(launch_dgemm_set(jb, nrhs, jb, M1, jb, W, jb, b(j), ldb, ctx->d_status, st));
+      CK(cudaMemcpy2DAsync(b(j), (size_t)ldb * sizeof(double), W, (size_t)jb * sizeof(double),
+                           (size_t)jb * sizeof(double), nrhs, cudaMemcpyDeviceToDevice, st));
+      if((s = solve_lower(j, jb)) != HPLB_OK) return s;
       CK(launch_dgemm_sub(n - j - jb, nrhs, jb, lu(j + jb, j), ld, b(j), ldb, b(j + jb), ldb,
                           ctx->d_status, st));
-      ctx->launches += 4;
+      ctx->launches += 3;
     }
     for(int j = (n - 1) / nb * nb; j >= 0; j -= nb) {
       const int jb = std::min(nb, n - j);
-      if((s = upper_inv(j, jb, M1)) != HPLB_OK) return s;
-      if((s = apply_block(M1, j, jb)) != HPLB_OK) return s;
+      if((s = solve_view(0, j, jb)) != HPLB_OK) return s;
       CK(launch_dgemm_sub(j, nrhs, jb, lu(0, j), ld, b(j), ldb, b(0), ldb, ctx->d_status, st));
       ctx->launches += 1;
     }
@@ -107,10 +108,7 @@ struct Rhs {
     ctx->launches += 1;
     for(int j = 0; j < n; j += nb) {  // U^T y = b, forward
       const int jb = std::min(nb, n - j);
-      if((s = upper_inv(j, jb, M1)) != HPLB_OK) return s;
-      CK(launch_transpose<double>(jb, jb, M1, jb, M2, jb, st));
-      ctx->launches += 1;
-      if((s = apply_block(M2, j, jb)) != HPLB_OK) return s;
+      if((s = solve_view(2, j, jb)) != HPLB_OK) return s;
       CK(launch_dgemm_sub(n - j - jb, nrhs, jb, t(j + jb, j), ldt, b(j), ldb, b(j + jb), ldb,
                           ctx->d_status, st));
       ctx->launches += 1;
@@ -120,10 +118,8 @@ struct Rhs {
       // y_top <- L11^-T (y_top - L21^T y_rest)
       CK(launch_dgemm_sub(jb, nrhs, n - j - jb, t(j, j + jb), ldt, b(j + jb), ldb, b(j), ldb,
                           ctx->d_status, st));
-      if((s = lower_inv(j, jb, M1)) != HPLB_OK) return s;
-      CK(launch_transpose<double>(jb, jb, M1, jb, M2, jb, st));
-      ctx->launches += 2;
-      if((s = apply_block(M2, j, jb)) != HPLB_OK) return s;
+      ctx->launches += 1;
+      if((s = solve_view(1, j, jb)) != HPLB_OK) return s;
       CK(launch_perm(ipiv + j, j, jb, perm, st));
       CK(launch_laswp_inverse(B, ldb, j, jb, perm, nrhs, st));
       ctx->launches += 2;
