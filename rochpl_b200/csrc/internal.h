@@ -138,6 +138,16 @@ cudaError_t launch_unit_lower_view(int kind, int jb, const double* T, int64_t ld
 cudaError_t launch_rows_xform(int jb, int n, const double* in, int64_t ldi, double* out,
                               int64_t ldo, const double* d, bool flip, bool scale,
                               cudaStream_t st);
+// X (jb x ncols) <- L^-1 X, unit-lower L, for few right-hand sides: one CTA per
+// column (dinv: the 32 x 32 diagonal inverses of L).
+cudaError_t launch_trsm_small(int jb, int ncols, double* X, int64_t ldx, const double* L,
+                              int64_t ldl, const double* dinv, cudaStream_t st);
+// C (jb x nrhs) -= M (jb x K) Y (K x nrhs) for K >> jb, nrhs: split-k partial
+// products into ws (splitk_ws_doubles) and a fixed-order reduction.
+size_t      splitk_ws_doubles(int jb, int nrhs, int K);
+cudaError_t launch_splitk_sub(int jb, int nrhs, int K, const double* M, int64_t ldm,
+                              const double* Y, int64_t ldy, double* C, int64_t ldc, double* ws,
+                              cudaStream_t st);
 // Inverse of a panel's row map on columns [0, n) of B: rows moved back to where
 // the forward interchanges took them from.
 cudaError_t launch_laswp_inverse(double* B, int64_t ldb, int ia, int jb, const int* permU, int n,

@@ -10,6 +10,8 @@
 //   rank_k         C = alpha A B^T (+ C), k <= 64: 64 x 64 output tiles, A and B
 //                  slices in shared memory, streaming stores (C is written once)
 //   check_ipiv     pivots in range before any kernel indexes with them
+#include <algorithm>
+
 #include "common.cuh"
 #include "internal.h"
 
@@ -135,6 +137,98 @@ __global__ void rows_xform_kernel(int jb, const double* __restrict__ in, int64_t
   }
 }
 
+// X (jb x ncols) <- L^-1 X for a unit-lower L and few right-hand sides: one
+// CTA per column, the column in shared memory.  Per 32-row block the 16 warps
+// split the dot products of the block's rows with the solved rows above (lane
+// = row, so each step reads 32 consecutive entries of a column of L), a fixed
+// order sum of the 16 slices, then the block's 32 x 32 inverse (dinv, from
+// diag_inv) applied.
+constexpr int kSmallThreads = 512;
+__global__ void __launch_bounds__(kSmallThreads)
+trsm_small_kernel(int jb, double* X, int64_t ldx, const double* __restrict__ L, int64_t ldl,
+                  const double* __restrict__ dinv) {
+  extern __shared__ double xs[];
+  __shared__ double part[kSmallThreads / 32][33];
+  __shared__ double tmp[32];
+  double*   col  = X + (size_t)blockIdx.x * ldx;
+  const int lane = threadIdx.x & 31, sl = threadIdx.x >> 5, nsl = kSmallThreads / 32;
+  for(int i = threadIdx.x; i < jb; i += kSmallThreads) xs[i] = col[i];
+  __syncthreads();
+  for(int b0 = 0; b0 < jb; b0 += 32) {
+    const int r   = b0 + lane;
+    double    acc = 0.0;
+    if(r < jb) {
+      const double* lr = L + r;
+#pragma unroll 4
+      for(int k = sl; k < b0; k += nsl) acc += lr[(size_t)k * ldl] * xs[k];
+    }
+    part[sl][lane] = acc;
+    __syncthreads();
+    if(threadIdx.x < 32) {
+      double t = 0.0;
+      for(int q = 0; q < nsl; ++q) t += part[q][lane];
+      tmp[lane] = r < jb ? xs[r] - t : 0.0;
+    }
+    __syncthreads();
+    if(threadIdx.x < 32 && r < jb) {
+      const double* D = dinv + (size_t)(b0 / 32) * 1024;
+      double        x = 0.0;
+#pragma unroll 8
+      for(int c = 0; c < 32; ++c) x += D[c * 32 + lane] * tmp[c];
+      xs[r] = x;
+    }
+    __syncthreads();
+  }
+  for(int i = threadIdx.x; i < jb; i += kSmallThreads) col[i] = xs[i];
+}
+
+// Split-k partial products for C (jb x nrhs) -= M (jb x K) Y (K x nrhs) with
+// K much larger than jb and nrhs: CTA (chunk, column block) writes
+// part[chunk] = M[:, chunk] Y[chunk, 32 columns]; Y's slice in shared memory,
+// each thread 32 accumulators per row it owns.
+constexpr int kSkK = 128;
+__global__ void __launch_bounds__(256)
+splitk_partial_kernel(int jb, int nrhs, int K, const double* __restrict__ M, int64_t ldm,
+                      const double* __restrict__ Y, int64_t ldy, double* __restrict__ part) {
+  __shared__ double ys[kSkK][33];
+  const int k0 = blockIdx.x * kSkK, c0 = blockIdx.y * 32;
+  const int kc = min(kSkK, K - k0), ncb = min(32, nrhs - c0);
+  for(int e = threadIdx.x; e < kSkK * 32; e += 256) {
+    const int k = e % kSkK, c = e / kSkK;
+    ys[k][c] = (k < kc && c < ncb) ? Y[(size_t)(k0 + k) + (size_t)(c0 + c) * ldy] : 0.0;
+  }
+  __syncthreads();
+  double* out = part + ((size_t)blockIdx.x * gridDim.y + blockIdx.y) * 32 * (size_t)jb;
+  for(int r = threadIdx.x; r < jb; r += 256) {
+    double acc[32];
+#pragma unroll
+    for(int c = 0; c < 32; ++c) acc[c] = 0.0;
+    const double* m = M + r + (size_t)k0 * ldm;
+    for(int k = 0; k < kc; ++k) {
+      const double a = m[(size_t)k * ldm];
+#pragma unroll
+      for(int c = 0; c < 32; ++c) acc[c] = fma(a, ys[k][c], acc[c]);
+    }
+#pragma unroll
+    for(int c = 0; c < 32; ++c) out[(size_t)c * jb + r] = acc[c];
+  }
+}
+
+// C -= the sum of the partial products, chunk by chunk in order.
+__global__ void splitk_reduce_kernel(int jb, int nrhs, int nchunks, int ncb,
+                                     const double* __restrict__ part, double* C, int64_t ldc) {
+  const int64_t total = (int64_t)jb * nrhs;
+  for(int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < total;
+      e += (int64_t)gridDim.x * blockDim.x) {
+    const int r = (int)(e % jb), c = (int)(e / jb);
+    const int cb = c / 32, cc = c % 32;
+    double    t  = 0.0;
+    for(int q = 0; q < nchunks; ++q)
+      t += part[(((size_t)q * ncb + cb) * 32 + cc) * jb + r];
+    C[(size_t)r + (size_t)c * ldc] -= t;
+  }
+}
+
 __global__ void check_ipiv_kernel(int n, const int* __restrict__ ipiv, int* status) {
   for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
     if(ipiv[i] < i || ipiv[i] >= n) record_info(status, i + 1);
@@ -191,6 +285,33 @@ cudaError_t launch_rows_xform(int jb, int n, const double* in, int64_t ldi, doub
   if(jb <= 0 || n <= 0) return cudaSuccess;
   if(n > 65535) return cudaErrorInvalidValue;
   rows_xform_kernel<<<n, 256, 0, st>>>(jb, in, ldi, out, ldo, d, flip ? 1 : 0, scale ? 1 : 0);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_trsm_small(int jb, int ncols, double* X, int64_t ldx, const double* L,
+                              int64_t ldl, const double* dinv, cudaStream_t st) {
+  if(jb <= 0 || ncols <= 0) return cudaSuccess;
+  if(jb > 4096 || ncols > 65535) return cudaErrorInvalidValue;
+  trsm_small_kernel<<<ncols, kSmallThreads, (size_t)jb * sizeof(double), st>>>(jb, X, ldx, L, ldl,
+                                                                              dinv);
+  return cudaGetLastError();
+}
+
+size_t splitk_ws_doubles(int jb, int nrhs, int K) {
+  const size_t nch = (size_t)(K + kSkK - 1) / kSkK, ncb = (size_t)(nrhs + 31) / 32;
+  return nch * ncb * 32 * (size_t)jb;
+}
+
+cudaError_t launch_splitk_sub(int jb, int nrhs, int K, const double* M, int64_t ldm,
+                              const double* Y, int64_t ldy, double* C, int64_t ldc, double* ws,
+                              cudaStream_t st) {
+  if(jb <= 0 || nrhs <= 0 || K <= 0) return cudaSuccess;
+  const int nch = (K + kSkK - 1) / kSkK, ncb = (nrhs + 31) / 32;
+  if(ncb > 65535) return cudaErrorInvalidValue;
+  splitk_partial_kernel<<<dim3(nch, ncb), 256, 0, st>>>(jb, nrhs, K, M, ldm, Y, ldy, ws);
+  const int64_t total = (int64_t)jb * nrhs;
+  const int     grid  = (int)std::min<int64_t>((total + 255) / 256, 4096);
+  splitk_reduce_kernel<<<grid, 256, 0, st>>>(jb, nrhs, nch, ncb, ws, C, ldc);
   return cudaGetLastError();
 }
 

@@ -31,20 +31,27 @@ struct Rhs {
   const int*    ipiv;
   double*       B;
   int64_t       ldb;
-  double *      W, *M1, *dvec, *dinv, *T;
+  double *      W, *M1, *dvec, *dinv, *T, *SK;  // SK: split-k partial products
   int64_t       ldt;  // rows of T: n rounded up to 16, + 16, so a 16-row slab never leaves it
   int*          perm;
   cudaStream_t  st;
 
-  static size_t ws_doubles(int nb, int nrhs) {
+  static size_t ws_doubles(int n, int nb, int nrhs) {
     const size_t nblk = (size_t)nb / 32 + 1;
-    return (size_t)nb * nrhs + (size_t)nb * nb + nb + nblk * 1024 + 64;
+    return (size_t)nb * nrhs + (size_t)nb * nb + nb + nblk * 1024 + 64 +
+           splitk_ws_doubles(nb, nrhs, std::max(n, 1));
   }
   void carve(double* base) {
     W    = base;
     M1   = W + (size_t)nb * nrhs;
     dvec = M1 + (size_t)nb * nb;
     dinv = dvec + nb;
+    SK   = dinv + ((size_t)nb / 32 + 1) * 1024 + 64;
+  }
+  // Few right-hand sides: one CTA per column; many: the blocked kernel.
+  cudaError_t trsm(double* X, int64_t ldx, int jb, const double* L, int64_t ldl) {
+    if(nrhs <= 128) return launch_trsm_small(jb, nrhs, X, ldx, L, ldl, dinv, st);
+    return launch_trsm_unit_lower(X, ldx, jb, L, ldl, dinv, nrhs, st);
   }
 
   const double* lu(int i, int j) const { return LU + (size_t)i + (size_t)j * (size_t)ld; }
@@ -57,7 +64,7 @@ struct Rhs {
   hplb_status solve_lower(int j, int jb) {
     hplb_ctx* ctx = this->ctx;
     CK(launch_diag_inv<double>(LU, ld, j, j, jb, dinv, st));
-    CK(launch_trsm_unit_lower(b(j), ldb, jb, lu(j, j), ld, dinv, nrhs, st));
+    CK(trsm(b(j), ldb, jb, lu(j, j), ld));
     ctx->launches += 2;
     return HPLB_OK;
   }
@@ -70,7 +77,7 @@ struct Rhs {
     CK(launch_unit_lower_view(kind, jb, lu(j, j), ld, M1, dvec, st));
     CK(launch_diag_inv<double>(M1, jb, 0, 0, jb, dinv, st));
     CK(launch_rows_xform(jb, nrhs, b(j), ldb, W, jb, dvec, kind != 2, kind == 0, st));
-    CK(launch_trsm_unit_lower(W, jb, jb, M1, jb, dinv, nrhs, st));
+    CK(trsm(W, jb, jb, M1, jb));
     CK(launch_rows_xform(jb, nrhs, W, jb, b(j), ldb, dvec, kind != 2, kind == 2, st));
     ctx->launches += 5;
     return HPLB_OK;
@@ -115,10 +122,17 @@ struct Rhs {
     }
     for(int j = (n - 1) / nb * nb; j >= 0; j -= nb) {
       const int jb = std::min(nb, n - j);
-      // y_top <- L11^-T (y_top - L21^T y_rest)
-      CK(launch_dgemm_sub(jb, nrhs, n - j - jb, t(j, j + jb), ldt, b(j + jb), ldb, b(j), ldb,
-                          ctx->d_status, st));
-      ctx->launches += 1;
+      // y_top <- L11^-T (y_top - L21^T y_rest); the product has a long k and
+      // few outputs, so it is split over k.
+      const int K = n - j - jb;
+      if(K > 4 * jb && nrhs <= 128) {
+        CK(launch_splitk_sub(jb, nrhs, K, t(j, j + jb), ldt, b(j + jb), ldb, b(j), ldb, SK, st));
+        ctx->launches += 2;
+      } else {
+        CK(launch_dgemm_sub(jb, nrhs, K, t(j, j + jb), ldt, b(j + jb), ldb, b(j), ldb,
+                            ctx->d_status, st));
+        ctx->launches += 1;
+      }
       if((s = solve_view(1, j, jb)) != HPLB_OK) return s;
       CK(launch_perm(ipiv + j, j, jb, perm, st));
       CK(launch_laswp_inverse(B, ldb, j, jb, perm, nrhs, st));
@@ -158,7 +172,7 @@ hplb_status hplb_getrs(hplb_ctx* ctx, int trans, int n, int nb, int nrhs, const 
   R.st   = ctx->s_upd;
   R.ldt  = ((int64_t)n + 15) / 16 * 16 + 16;
   hplb_status s;
-  if((s = grow(ctx, &ctx->r_ws, &ctx->r_ws_cap, Rhs::ws_doubles(R.nb, nrhs))) != HPLB_OK ||
+  if((s = grow(ctx, &ctx->r_ws, &ctx->r_ws_cap, Rhs::ws_doubles(n, R.nb, nrhs))) != HPLB_OK ||
      (s = grow(ctx, &ctx->r_perm, &ctx->r_perm_cap, 2 * (size_t)R.nb)) != HPLB_OK)
     return s;
   if(trans && (s = grow(ctx, &ctx->r_t, &ctx->r_t_cap, (size_t)R.ldt * n)) != HPLB_OK) return s;
