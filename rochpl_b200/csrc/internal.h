@@ -148,6 +148,11 @@ size_t      splitk_ws_doubles(int jb, int nrhs, int K);
 cudaError_t launch_splitk_sub(int jb, int nrhs, int K, const double* M, int64_t ldm,
                               const double* Y, int64_t ldy, double* C, int64_t ldc, double* ws,
                               cudaStream_t st);
+// C (m x nrhs) -= M (m x K) Y (K x nrhs) for tall M and few right-hand sides
+// (one row per thread, the whole K per CTA).
+cudaError_t launch_rows_sub(int m, int nrhs, int K, const double* M, int64_t ldm,
+                            const double* Y, int64_t ldy, double* C, int64_t ldc,
+                            cudaStream_t st);
 // Inverse of a panel's row map on columns [0, n) of B: rows moved back to where
 // the forward interchanges took them from.
 cudaError_t launch_laswp_inverse(double* B, int64_t ldb, int ia, int jb, const int* permU, int n,

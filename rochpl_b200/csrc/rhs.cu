@@ -214,6 +214,41 @@ splitk_partial_kernel(int jb, int nrhs, int K, const double* __restrict__ M, int
   }
 }
 
+// C (m x nrhs) -= M (m x K) Y (K x nrhs) for tall M and few right-hand sides:
+// one row per thread (128 per CTA), 32 accumulators, Y staged kSkK deep in
+// shared memory, the whole K in one CTA (C read and written once).
+__global__ void __launch_bounds__(128)
+rows_sub_kernel(int m, int nrhs, int K, const double* __restrict__ M, int64_t ldm,
+                const double* __restrict__ Y, int64_t ldy, double* __restrict__ C, int64_t ldc) {
+  __shared__ double ys[kSkK][33];
+  const int r = blockIdx.x * 128 + threadIdx.x, c0 = blockIdx.y * 32;
+  const int ncb = min(32, nrhs - c0);
+  double    acc[32];
+#pragma unroll
+  for(int c = 0; c < 32; ++c) acc[c] = 0.0;
+  for(int k0 = 0; k0 < K; k0 += kSkK) {
+    const int kc = min(kSkK, K - k0);
+    __syncthreads();
+    for(int e = threadIdx.x; e < kSkK * 32; e += 128) {
+      const int k = e % kSkK, c = e / kSkK;
+      ys[k][c] = (k < kc && c < ncb) ? Y[(size_t)(k0 + k) + (size_t)(c0 + c) * ldy] : 0.0;
+    }
+    __syncthreads();
+    if(r < m) {
+      const double* mr = M + r + (size_t)k0 * ldm;
+      for(int k = 0; k < kc; ++k) {
+        const double a = mr[(size_t)k * ldm];
+#pragma unroll
+        for(int c = 0; c < 32; ++c) acc[c] = fma(a, ys[k][c], acc[c]);
+      }
+    }
+  }
+  if(r < m)
+#pragma unroll
+    for(int c = 0; c < 32; ++c)
+      if(c < ncb) C[(size_t)r + (size_t)(c0 + c) * ldc] -= acc[c];
+}
+
 // C -= the sum of the partial products, chunk by chunk in order.
 __global__ void splitk_reduce_kernel(int jb, int nrhs, int nchunks, int ncb,
                                      const double* __restrict__ part, double* C, int64_t ldc) {
@@ -312,6 +347,17 @@ cudaError_t launch_splitk_sub(int jb, int nrhs, int K, const double* M, int64_t 
   const int64_t total = (int64_t)jb * nrhs;
   const int     grid  = (int)std::min<int64_t>((total + 255) / 256, 4096);
   splitk_reduce_kernel<<<grid, 256, 0, st>>>(jb, nrhs, nch, ncb, ws, C, ldc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows_sub(int m, int nrhs, int K, const double* M, int64_t ldm,
+                            const double* Y, int64_t ldy, double* C, int64_t ldc,
+                            cudaStream_t st) {
+  if(m <= 0 || nrhs <= 0 || K <= 0) return cudaSuccess;
+  const int ncb = (nrhs + 31) / 32;
+  if(ncb > 65535) return cudaErrorInvalidValue;
+  rows_sub_kernel<<<dim3((m + 127) / 128, ncb), 128, 0, st>>>(m, nrhs, K, M, ldm, Y, ldy, C,
+                                                              ldc);
   return cudaGetLastError();
 }
 

@@ -48,6 +48,13 @@ struct Rhs {
     dinv = dvec + nb;
     SK   = dinv + ((size_t)nb / 32 + 1) * 1024 + 64;
   }
+  // C (m x nrhs) -= M (m x k) Y: the row-parallel kernel for few right-hand
+  // sides, the DMMA GEMM otherwise.
+  cudaError_t update(int m, int k, const double* M, int64_t ldm, const double* Y, int64_t ldy,
+                     double* C, int64_t ldc) {
+    if(nrhs <= 128) return launch_rows_sub(m, nrhs, k, M, ldm, Y, ldy, C, ldc, st);
+    return launch_dgemm_sub(m, nrhs, k, M, ldm, Y, ldy, C, ldc, ctx->d_status, st);
+  }
   // Few right-hand sides: one CTA per column; many: the blocked kernel.
   cudaError_t trsm(double* X, int64_t ldx, int jb, const double* L, int64_t ldl) {
     if(nrhs <= 128) return launch_trsm_small(jb, nrhs, X, ldx, L, ldl, dinv, st);
@@ -94,14 +101,13 @@ struct Rhs {
       CK(cudaMemcpy2DAsync(b(j), (size_t)ldb * sizeof(double), W, (size_t)jb * sizeof(double),
                            (size_t)jb * sizeof(double), nrhs, cudaMemcpyDeviceToDevice, st));
       if((s = solve_lower(j, jb)) != HPLB_OK) return s;
-      CK(launch_dgemm_sub(n - j - jb, nrhs, jb, lu(j + jb, j), ld, b(j), ldb, b(j + jb), ldb,
-                          ctx->d_status, st));
+      CK(update(n - j - jb, jb, lu(j + jb, j), ld, b(j), ldb, b(j + jb), ldb));
       ctx->launches += 3;
     }
     for(int j = (n - 1) / nb * nb; j >= 0; j -= nb) {
       const int jb = std::min(nb, n - j);
       if((s = solve_view(0, j, jb)) != HPLB_OK) return s;
-      CK(launch_dgemm_sub(j, nrhs, jb, lu(0, j), ld, b(j), ldb, b(0), ldb, ctx->d_status, st));
+      CK(update(j, jb, lu(0, j), ld, b(j), ldb, b(0), ldb));
       ctx->launches += 1;
     }
     return HPLB_OK;
@@ -116,8 +122,7 @@ struct Rhs {
     for(int j = 0; j < n; j += nb) {  // U^T y = b, forward
       const int jb = std::min(nb, n - j);
       if((s = solve_view(2, j, jb)) != HPLB_OK) return s;
-      CK(launch_dgemm_sub(n - j - jb, nrhs, jb, t(j + jb, j), ldt, b(j), ldb, b(j + jb), ldb,
-                          ctx->d_status, st));
+      CK(update(n - j - jb, jb, t(j + jb, j), ldt, b(j), ldb, b(j + jb), ldb));
       ctx->launches += 1;
     }
     for(int j = (n - 1) / nb * nb; j >= 0; j -= nb) {
