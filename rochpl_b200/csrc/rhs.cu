@@ -156,11 +156,22 @@ trsm_small_kernel(int jb, double* X, int64_t ldx, const double* __restrict__ L, 
   __syncthreads();
   for(int b0 = 0; b0 < jb; b0 += 32) {
     const int r   = b0 + lane;
-    double    acc = 0.0;
+    double    acc = 0.0, acc2 = 0.0;
     if(r < jb) {
       const double* lr = L + r;
-#pragma unroll 4
-      for(int k = sl; k < b0; k += nsl) acc += lr[(size_t)k * ldl] * xs[k];
+      int           k  = sl;
+      for(; k + 7 * nsl < b0; k += 8 * nsl) {  // eight loads in flight, two chains
+        double a[8];
+#pragma unroll
+        for(int q = 0; q < 8; ++q) a[q] = lr[(size_t)(k + q * nsl) * ldl];
+#pragma unroll
+        for(int q = 0; q < 8; q += 2) {
+          acc  = fma(a[q], xs[k + q * nsl], acc);
+          acc2 = fma(a[q + 1], xs[k + (q + 1) * nsl], acc2);
+        }
+      }
+      for(; k < b0; k += nsl) acc = fma(lr[(size_t)k * ldl], xs[k], acc);
+      acc += acc2;
     }
     part[sl][lane] = acc;
     __syncthreads();
@@ -204,7 +215,17 @@ splitk_partial_kernel(int jb, int nrhs, int K, const double* __restrict__ M, int
 #pragma unroll
     for(int c = 0; c < 32; ++c) acc[c] = 0.0;
     const double* m = M + r + (size_t)k0 * ldm;
-    for(int k = 0; k < kc; ++k) {
+    int           k = 0;
+    for(; k + 8 <= kc; k += 8) {  // eight loads in flight before their FMAs
+      double a[8];
+#pragma unroll
+      for(int q = 0; q < 8; ++q) a[q] = m[(size_t)(k + q) * ldm];
+#pragma unroll
+      for(int q = 0; q < 8; ++q)
+#pragma unroll
+        for(int c = 0; c < 32; ++c) acc[c] = fma(a[q], ys[k + q][c], acc[c]);
+    }
+    for(; k < kc; ++k) {
       const double a = m[(size_t)k * ldm];
 #pragma unroll
       for(int c = 0; c < 32; ++c) acc[c] = fma(a, ys[k][c], acc[c]);
@@ -236,7 +257,17 @@ rows_sub_kernel(int m, int nrhs, int K, const double* __restrict__ M, int64_t ld
     __syncthreads();
     if(r < m) {
       const double* mr = M + r + (size_t)k0 * ldm;
-      for(int k = 0; k < kc; ++k) {
+      int           k  = 0;
+      for(; k + 8 <= kc; k += 8) {  // eight loads in flight before their FMAs
+        double a[8];
+#pragma unroll
+        for(int q = 0; q < 8; ++q) a[q] = mr[(size_t)(k + q) * ldm];
+#pragma unroll
+        for(int q = 0; q < 8; ++q)
+#pragma unroll
+          for(int c = 0; c < 32; ++c) acc[c] = fma(a[q], ys[k + q][c], acc[c]);
+      }
+      for(; k < kc; ++k) {
         const double a = mr[(size_t)k * ldm];
 #pragma unroll
         for(int c = 0; c < 32; ++c) acc[c] = fma(a, ys[k][c], acc[c]);
