@@ -236,13 +236,16 @@ splitk_partial_kernel(int jb, int nrhs, int K, const double* __restrict__ M, int
 }
 
 // C (m x nrhs) -= M (m x K) Y (K x nrhs) for tall M and few right-hand sides:
-// one row per thread (128 per CTA), 32 accumulators, Y staged kSkK deep in
-// shared memory, the whole K in one CTA (C read and written once).
-__global__ void __launch_bounds__(128)
+// 32 rows per CTA (lane = row), the CTA's 8 warps on interleaved slices of
+// each 128-deep chunk of k (Y's chunk in shared memory), 32 accumulators per
+// thread, 16 loads in flight per warp; the 8 slices are summed in a fixed
+// order at the end (C read and written once).
+__global__ void __launch_bounds__(256)
 rows_sub_kernel(int m, int nrhs, int K, const double* __restrict__ M, int64_t ldm,
                 const double* __restrict__ Y, int64_t ldy, double* __restrict__ C, int64_t ldc) {
-  __shared__ double ys[kSkK][33];
-  const int r = blockIdx.x * 128 + threadIdx.x, c0 = blockIdx.y * 32;
+  __shared__ double ys[kSkK][33];  // also the reduction buffer, 16 columns at a time
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int r = blockIdx.x * 32 + lane, c0 = blockIdx.y * 32;
   const int ncb = min(32, nrhs - c0);
   double    acc[32];
 #pragma unroll
@@ -250,34 +253,43 @@ rows_sub_kernel(int m, int nrhs, int K, const double* __restrict__ M, int64_t ld
   for(int k0 = 0; k0 < K; k0 += kSkK) {
     const int kc = min(kSkK, K - k0);
     __syncthreads();
-    for(int e = threadIdx.x; e < kSkK * 32; e += 128) {
+    for(int e = threadIdx.x; e < kSkK * 32; e += 256) {
       const int k = e % kSkK, c = e / kSkK;
       ys[k][c] = (k < kc && c < ncb) ? Y[(size_t)(k0 + k) + (size_t)(c0 + c) * ldy] : 0.0;
     }
     __syncthreads();
     if(r < m) {
+      // This warp's k: warp, warp + 8, ... within the chunk (16 of them).
       const double* mr = M + r + (size_t)k0 * ldm;
-      int           k  = 0;
-      for(; k + 8 <= kc; k += 8) {  // eight loads in flight before their FMAs
-        double a[8];
+      double        a[kSkK / 8];
 #pragma unroll
-        for(int q = 0; q < 8; ++q) a[q] = mr[(size_t)(k + q) * ldm];
-#pragma unroll
-        for(int q = 0; q < 8; ++q)
-#pragma unroll
-          for(int c = 0; c < 32; ++c) acc[c] = fma(a[q], ys[k + q][c], acc[c]);
+      for(int q = 0; q < kSkK / 8; ++q) {
+        const int k = warp + 8 * q;
+        a[q]        = k < kc ? mr[(size_t)k * ldm] : 0.0;
       }
-      for(; k < kc; ++k) {
-        const double a = mr[(size_t)k * ldm];
 #pragma unroll
-        for(int c = 0; c < 32; ++c) acc[c] = fma(a, ys[k][c], acc[c]);
+      for(int q = 0; q < kSkK / 8; ++q) {
+        const int k = warp + 8 * q;
+#pragma unroll
+        for(int c = 0; c < 32; ++c) acc[c] = fma(a[q], ys[k][c], acc[c]);
       }
     }
   }
-  if(r < m)
+  double(*red)[16][33] = reinterpret_cast<double(*)[16][33]>(&ys[0][0]);  // [8][16][33]
 #pragma unroll
-    for(int c = 0; c < 32; ++c)
-      if(c < ncb) C[(size_t)r + (size_t)(c0 + c) * ldc] -= acc[c];
+  for(int h = 0; h < 2; ++h) {
+    __syncthreads();
+#pragma unroll
+    for(int c = 0; c < 16; ++c) red[warp][c][lane] = acc[h * 16 + c];
+    __syncthreads();
+    // Thread (column h*16 + c, row lane): sum the 8 slices in order.
+    for(int c = warp; c < 16; c += 8) {
+      double t = 0.0;
+#pragma unroll
+      for(int w = 0; w < 8; ++w) t += red[w][c][lane];
+      if(r < m && h * 16 + c < ncb) C[(size_t)r + (size_t)(c0 + h * 16 + c) * ldc] -= t;
+    }
+  }
 }
 
 // C -= the sum of the partial products, chunk by chunk in order.
@@ -387,8 +399,7 @@ cudaError_t launch_rows_sub(int m, int nrhs, int K, const double* M, int64_t ldm
   if(m <= 0 || nrhs <= 0 || K <= 0) return cudaSuccess;
   const int ncb = (nrhs + 31) / 32;
   if(ncb > 65535) return cudaErrorInvalidValue;
-  rows_sub_kernel<<<dim3((m + 127) / 128, ncb), 128, 0, st>>>(m, nrhs, K, M, ldm, Y, ldy, C,
-                                                              ldc);
+  rows_sub_kernel<<<dim3((m + 31) / 32, ncb), 256, 0, st>>>(m, nrhs, K, M, ldm, Y, ldy, C, ldc);
   return cudaGetLastError();
 }
 
