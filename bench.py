@@ -179,27 +179,12 @@ def run_ours(args):
     from rochpl_b200 import library
     from rochpl_b200.hpl import Algo, default_ld
 
+    from rochpl_b200.ranks import Ranks
+
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=1800))
-        pg = dist
-
-    def barrier():
-        if pg is not None:
-            pg.barrier()
-
-    def max_over_ranks(v: float) -> float:
-        if pg is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+    ranks = Ranks("nccl", timeout_s=1800)
+    barrier, max_over_ranks = ranks.barrier, ranks.max
 
     lib = library(local)
     n, nb = args.n, args.nb
@@ -252,7 +237,7 @@ def run_ours(args):
         torch.cuda.empty_cache()
         mixed = mixed_leg(lib, algo, n, seed, x64, solve_ms, args, barrier, max_over_ranks)
 
-    batched = None if args.no_batched else batched_leg(lib, args, max_over_ranks)
+    batched = None if args.no_batched else batched_leg(lib, args, ranks)
     autograd = None if args.no_autograd else autograd_leg(lib, args, max_over_ranks)
 
     cb = None
@@ -303,8 +288,7 @@ def run_ours(args):
         if cb is not None:
             line["cpu_baseline"] = cb
         print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.destroy_process_group()
+    ranks.close()
     return 0
 
 
@@ -366,45 +350,53 @@ def mixed_leg(lib, algo, n, seed, x64, fp64_ms, args, barrier, max_over_ranks):
     return out
 
 
-def batched_leg(lib, args, max_over_ranks):
+def batched_leg(lib, args, ranks):
     """The batched form: 4096 independent LCG systems, N log-uniform in
     [32, 1024], per-system seed 100 + i, nrhs in {1, 16, 64}; one persistent,
-    graph-captured launch per solve, panel widths from the autotuner.  value =
-    sum(2/3 N^3 + 2 N^2 nrhs) / device time of the launch."""
+    graph-captured launch per solve, panel widths from the autotuner.  Over
+    several ranks the systems are split by flops (batch.partition_systems):
+    each rank generates and solves only its own, and the per-system residuals
+    are assembled once at the end.  value = sum over ALL systems of
+    (2/3 N^3 + 2 N^2 nrhs) / the max over ranks of the launch's device time."""
     import numpy as np
     import torch
 
-    from rochpl_b200.batch import BatchPlan, autotune, workload_sizes
+    from rochpl_b200.batch import BatchShard, autotune, workload_sizes
 
     torch.cuda.empty_cache()
     n = workload_sizes(args.batch_count)
     out = {"workload": f"{args.batch_count} systems, N log-uniform in [32, 1024] "
                        "(numpy PCG64 seed 20261203), seed_i = 100 + i",
+           "scaling": "strong (the systems are split across ranks by flops)"
+                      if ranks.world > 1 else "one GPU",
            "by_nrhs": {}}
     for nrhs in (1, 16, 64):
         table = autotune(lib, nrhs=nrhs, use_cache=False)
-        plan = BatchPlan(lib, n, nrhs, table)
-        dA = torch.zeros(plan.a_elems, dtype=torch.float64, device="cuda")
-        dB = torch.zeros(plan.b_elems, dtype=torch.float64, device="cuda")
-        dP = torch.zeros(plan.p_elems, dtype=torch.int32, device="cuda")
-        dI = torch.zeros(plan.count, dtype=torch.int32, device="cuda")
-        seeds = 100 + np.arange(plan.count, dtype=np.uint64)
+        shard = BatchShard(lib, n, nrhs, ranks.rank, ranks.world, table)
+        plan, seeds = shard.plan, shard.seeds
+        dA = torch.zeros(max(plan.a_elems, 1), dtype=torch.float64, device="cuda")
+        dB = torch.zeros(max(plan.b_elems, 1), dtype=torch.float64, device="cuda")
+        dP = torch.zeros(max(plan.p_elems, 1), dtype=torch.int32, device="cuda")
+        dI = torch.zeros(max(plan.count, 1), dtype=torch.int32, device="cuda")
         ms = []
         for it in range(args.warmup + args.steps):
             plan.matgen(seeds, dA.data_ptr(), dB.data_ptr())  # outside the timed launch
+            ranks.barrier()
             plan.gesv(dA.data_ptr(), dB.data_ptr(), dP.data_ptr(), dI.data_ptr())
             if it >= args.warmup:
-                ms.append(plan.last_ms)
-        res = torch.zeros(plan.count, dtype=torch.float64, device="cuda")
+                ms.append(plan.last_ms if plan.count else 0.0)
+        res = torch.zeros(max(plan.count, 1), dtype=torch.float64, device="cuda")
         plan.residual(seeds, dB.data_ptr(), res.data_ptr())
-        t = max_over_ranks(statistics.mean(ms))
+        res_all = ranks.assemble(res.cpu().numpy()[:plan.count], shard.index, shard.total)
+        sing = ranks.sum(float((dI[:plan.count] != 0).sum()))
+        t = ranks.max(statistics.mean(ms))
         out["by_nrhs"][str(nrhs)] = {
-            "ms_per_solve": t, "value": plan.flops() / (t * 1e-3) / 1e12, "unit": UNIT,
-            "resid_max": float(res.max()), "resid_passed": bool(float(res.max()) < 16.0),
-            "singular": int((dI != 0).sum()), "nb_by_class": table, "gpu_launches": 1,
-            "flops": plan.flops()}
+            "ms_per_solve": t, "value": shard.total_flops / (t * 1e-3) / 1e12, "unit": UNIT,
+            "resid_max": float(res_all.max()), "resid_passed": bool(float(res_all.max()) < 16.0),
+            "singular": int(sing), "nb_by_class": table, "gpu_launches": 1,
+            "flops": shard.total_flops, "systems_on_rank0": int(plan.count)}
         del dA, dB, dP, dI, res
-        plan.close()
+        shard.close()
         torch.cuda.empty_cache()
     return out
 

@@ -17,7 +17,8 @@ import numpy as np
 
 from .lib import HPLB_BATCH_CLASSES, HPLB_OK, HplError, Library
 
-__all__ = ["BatchPlan", "autotune", "workload_sizes", "batch_flops"]
+__all__ = ["BatchPlan", "BatchShard", "autotune", "workload_sizes", "batch_flops",
+           "system_cost", "partition_systems"]
 
 _CACHE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning", "batch_nb.json")
 
@@ -29,11 +30,39 @@ def workload_sizes(count: int = 4096, lo: int = 32, hi: int = 1024,
     return np.rint(np.exp(math.log(lo) + u * (math.log(hi) - math.log(lo)))).astype(np.int32)
 
 
-def batch_flops(n, nrhs) -> float:
-    """Sum of 2/3 n^3 + 2 n^2 nrhs over the systems (LU + both triangular solves)."""
+def system_cost(n, nrhs) -> np.ndarray:
+    """Per-system flops 2/3 n^3 + 2 n^2 nrhs (LU + both triangular solves)."""
     n = np.asarray(n, dtype=np.float64)
-    r = np.asarray(nrhs, dtype=np.float64)
-    return float(np.sum(2.0 / 3.0 * n ** 3 + 2.0 * n ** 2 * r))
+    r = np.broadcast_to(np.asarray(nrhs, dtype=np.float64), n.shape)
+    return 2.0 / 3.0 * n ** 3 + 2.0 * n ** 2 * r
+
+
+def batch_flops(n, nrhs) -> float:
+    """Sum of system_cost over the systems."""
+    return float(np.sum(system_cost(n, nrhs)))
+
+
+def partition_systems(n, nrhs, world: int) -> list[np.ndarray]:
+    """Split a batched workload across `world` ranks with balanced flops.
+
+    Longest-processing-time greedy: systems in decreasing cost (ties by
+    index) go one by one to the rank with the least cost so far (ties to the
+    lowest rank).  The result depends only on the sizes, so every rank
+    computes the same split and nothing is exchanged to agree on it.  The
+    heaviest rank carries at most 4/3 of the optimal makespan, and exceeds the
+    lightest by at most one system's cost.  Returns, per rank, the global
+    indices of its systems in increasing order."""
+    if world < 1:
+        raise ValueError("world size must be at least 1")
+    cost = system_cost(n, nrhs)
+    order = np.lexsort((np.arange(cost.size), -cost))
+    load = [0.0] * world
+    owner = np.empty(cost.size, dtype=np.int64)
+    for i in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        owner[i] = r
+        load[r] += float(cost[i])
+    return [np.flatnonzero(owner == r) for r in range(world)]
 
 
 class BatchPlan:
@@ -110,6 +139,29 @@ class BatchPlan:
 
     def flops(self) -> float:
         return batch_flops(self.n, self.nrhs)
+
+
+class BatchShard:
+    """One rank's part of a batched workload split by partition_systems: the
+    global indices of its systems, their seeds (seed_base + global index, so
+    every system is generated and solved exactly as in a one-rank run) and a
+    BatchPlan over them.  Ranks.assemble puts per-system results back in
+    global order."""
+
+    def __init__(self, lib: Library, n, nrhs, rank: int, world: int, nb_by_class=None,
+                 seed_base: int = 100):
+        n = np.asarray(n, dtype=np.int32)
+        nrhs = np.broadcast_to(np.asarray(nrhs, dtype=np.int32), n.shape)
+        if not 0 <= rank < world:
+            raise ValueError(f"rank {rank} outside world size {world}")
+        self.total = int(n.size)
+        self.total_flops = batch_flops(n, nrhs)
+        self.index = partition_systems(n, nrhs, world)[rank]
+        self.seeds = (np.uint64(seed_base) + self.index.astype(np.uint64)).astype(np.uint64)
+        self.plan = BatchPlan(lib, n[self.index], nrhs[self.index], nb_by_class)
+
+    def close(self):
+        self.plan.close()
 
 
 def autotune(lib: Library, nrhs: int = 16, use_cache: bool = True) -> list[int]:

@@ -99,44 +99,45 @@ HPLB_DEV bool better_b(double av, int ar, double bv, int br) {
   return ar < br;
 }
 
+// Argmax over the warp's candidates (v, r), r < 0 meaning none: the largest
+// |v|, the lowest row among equal magnitudes (the order of better_b for
+// finite values).  Branch free: |v| as an unsigned 64-bit key reduced by two
+// 32-bit max reductions (high word, then low word among the lanes that hold
+// the high maximum), the lowest matching row by a min reduction, the signed
+// value fetched from the lane that holds it.  Every lane gets the result;
+// returns the winning lane, or -1 if no lane has a candidate.
+HPLB_DEV int warp_argmax(double& v, int& r) {
+  const unsigned long long key =
+      r >= 0 ? (unsigned long long)__double_as_longlong(fabs(v)) : 0ull;
+  const unsigned hi  = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool     hit = r >= 0 && hi == mhi && lo == mlo;
+  const unsigned best = __reduce_min_sync(0xffffffffu, hit ? (unsigned)r : 0xffffffffu);
+  const unsigned who  = __ballot_sync(0xffffffffu, hit && (unsigned)r == best);
+  const int      wl   = who ? __ffs(who) - 1 : 0;
+  v = __shfl_sync(0xffffffffu, v, wl);
+  if(!who) {
+    v = 0.0;
+    r = -1;
+    return -1;
+  }
+  r = (int)best;
+  return wl;
+}
+
 HPLB_DEV void argmax_block(double& v, int& r, Smem& S) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for(int off = 16; off > 0; off >>= 1) {
-    const double ov = __shfl_down_sync(0xffffffffu, v, off);
-    const int    orr = __shfl_down_sync(0xffffffffu, r, off);
-    if(better_b(ov, orr, v, r)) {
-      v = ov;
-      r = orr;
-    }
-  }
+  warp_argmax(v, r);
   __syncthreads();
   if(lane == 0) {
     S.red_v[warp] = v;
     S.red_r[warp] = r;
   }
   __syncthreads();
-  if(warp == 0) {
-    v = lane < kBW ? S.red_v[lane] : 0.0;
-    r = lane < kBW ? S.red_r[lane] : -1;
-#pragma unroll
-    for(int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_down_sync(0xffffffffu, v, off);
-      const int    orr = __shfl_down_sync(0xffffffffu, r, off);
-      if(better_b(ov, orr, v, r)) {
-        v = ov;
-        r = orr;
-      }
-    }
-    if(lane == 0) {
-      S.red_v[0] = v;
-      S.red_r[0] = r;
-    }
-  }
-  __syncthreads();
-  v = S.red_v[0];
-  r = S.red_r[0];
-  __syncthreads();
+  v = lane < kBW ? S.red_v[lane] : 0.0;
+  r = lane < kBW ? S.red_r[lane] : -1;
+  warp_argmax(v, r);
 }
 
 HPLB_DEV void dmma(double (&d)[4], const double (&a)[4], const double (&b)[2]) {
@@ -266,44 +267,35 @@ HPLB_DEV void load_diag(const double* A, int64_t lda, int kb, Smem& S) {
 }
 
 // Substitution with S.D on n columns of X (kb rows, leading dimension ldx),
-// one column per thread:
+// one warp per column, lane = row, a run-time loop over the kb steps (each
+// solved entry broadcast by a shuffle and eliminated from the other lanes):
 //   LOWER_UNIT:      X <- L^-1 X     (unit lower, forward)
 //   UPPER:           X <- U^-1 X     (backward)
 //   UPPER_T:         X <- U^-T X     (U^T lower, forward)
 //   LOWER_UNIT_T:    X <- L^-T X     (L^T unit upper, backward)
 enum { LOWER_UNIT = 0, UPPER = 1, UPPER_T = 2, LOWER_UNIT_T = 3 };
 template <int KIND>
-HPLB_DEV void diag_solve(int kb, double* X, int64_t ldx, int n, const Smem& S) {
-  for(int c = threadIdx.x; c < n; c += kBT) {
-    double  x[kNbMax];
+__device__ __noinline__ void diag_solve(int kb, double* X, int64_t ldx, int n, const Smem& S) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for(int c = warp; c < n; c += kBW) {
     double* col = X + (size_t)c * ldx;
-#pragma unroll
-    for(int r = 0; r < kNbMax; ++r) x[r] = r < kb ? col[r] : 0.0;
+    double  x   = lane < kb ? col[lane] : 0.0;
     if(KIND == LOWER_UNIT || KIND == UPPER_T) {
-#pragma unroll
-      for(int r = 0; r < kNbMax; ++r) {
-        if(r < kb) {
-          double s = x[r];
-#pragma unroll
-          for(int q = 0; q < r; ++q) s -= (KIND == LOWER_UNIT ? S.D[r][q] : S.D[q][r]) * x[q];
-          x[r] = KIND == UPPER_T ? s / S.D[r][r] : s;
-        }
+#pragma unroll 4
+      for(int r = 0; r < kb; ++r) {
+        if(KIND == UPPER_T && lane == r) x = x / S.D[r][r];
+        const double xr = __shfl_sync(0xffffffffu, x, r);
+        if(lane > r && lane < kb) x -= (KIND == LOWER_UNIT ? S.D[lane][r] : S.D[r][lane]) * xr;
       }
     } else {
-#pragma unroll
-      for(int r = kNbMax - 1; r >= 0; --r) {
-        if(r < kb) {
-          double s = x[r];
-#pragma unroll
-          for(int q = r + 1; q < kNbMax; ++q)
-            if(q < kb) s -= (KIND == UPPER ? S.D[r][q] : S.D[q][r]) * x[q];
-          x[r] = KIND == UPPER ? s / S.D[r][r] : s;
-        }
+#pragma unroll 4
+      for(int r = kb - 1; r >= 0; --r) {
+        if(KIND == UPPER && lane == r) x = x / S.D[r][r];
+        const double xr = __shfl_sync(0xffffffffu, x, r);
+        if(lane < r) x -= (KIND == UPPER ? S.D[lane][r] : S.D[r][lane]) * xr;
       }
     }
-#pragma unroll
-    for(int r = 0; r < kNbMax; ++r)
-      if(r < kb) col[r] = x[r];
+    if(lane < kb) col[lane] = x;
   }
   __syncthreads();
 }
@@ -319,17 +311,30 @@ HPLB_DEV int next_system(const Args& a, Smem& S) {
   return S.next;
 }
 
-// The m x kb panel at A (leading dimension lda; rows k0.. of the system) with
-// each thread's rows t + q * kBT (q < RPT) in registers, column loop unrolled.
-// Per column: each warp finds its candidate by shuffles and publishes it with
-// the row's values, the owner of the diagonal row publishes that row, one
-// barrier, then every thread picks the winner and applies the interchange,
-// the division by the pivot and the update to its own rows.  The factored
-// panel goes back to A and to the shared copy P (leading dimension ldp) that
-// the trailing update reads L21 from.
+// x[c] for a column index c known only at run time, by selects over the
+// row's registers (so the row stays in registers).
+template <int KB>
+HPLB_DEV double pick(const double (&x)[KB], int c) {
+  double s = x[0];
+#pragma unroll
+  for(int q = 1; q < KB; ++q) s = (q == c) ? x[q] : s;
+  return s;
+}
+
+// The m x kb panel at A (leading dimension lda; rows k0.. of the system),
+// kb <= KB, with each thread's rows t + q * kBT (q < RPT) in registers.  The
+// column loop is a run-time loop whose body touches every register of the row
+// (selects and predicated updates), so the code stays a few KB and is fetched
+// once, not once per column.  Per column: each warp finds its candidate by
+// shuffles and publishes it with the row's values, the owner of the diagonal
+// row publishes that row, one barrier, then every thread picks the winner and
+// applies the interchange, the division by the pivot and the update to its own
+// rows.  The factored panel goes back to A and, if P is given, to the shared
+// copy P (leading dimension ldp) that the trailing update reads L21 from.
 template <int RPT, int KB>
-HPLB_DEV void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, double* P, int ldp,
+__device__ __noinline__ void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, double* P, int ldp,
                         Smem& S) {
+  static_assert(KB <= kRegPanelW, "panel wider than the exchange slots");
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   double    x[RPT][KB];
   int       row[RPT];
@@ -341,29 +346,20 @@ HPLB_DEV void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, dou
 #pragma unroll
     for(int c = 0; c < KB; ++c) x[q][c] = (in && c < kb) ? Ag[(size_t)row[q] + (size_t)c * lda] : 0.0;
   }
-#pragma unroll
-  for(int j = 0; j < KB; ++j) {
-    if(j >= kb) break;
+#pragma unroll 1
+  for(int j = 0; j < kb; ++j) {
     const int par = j & 1;
     double    v   = 0.0;
     int       r   = -1;
 #pragma unroll
-    for(int q = 0; q < RPT; ++q)
-      if(row[q] >= j && better_b(x[q][j], row[q], v, r)) {
-        v = x[q][j];
+    for(int q = 0; q < RPT; ++q) {
+      const double xj = pick(x[q], j);
+      if(row[q] >= j && better_b(xj, row[q], v, r)) {
+        v = xj;
         r = row[q];
       }
-#pragma unroll
-    for(int off = 16; off > 0; off >>= 1) {
-      const double ov  = __shfl_down_sync(0xffffffffu, v, off);
-      const int    orr = __shfl_down_sync(0xffffffffu, r, off);
-      if(better_b(ov, orr, v, r)) {
-        v = ov;
-        r = orr;
-      }
     }
-    v = __shfl_sync(0xffffffffu, v, 0);
-    r = __shfl_sync(0xffffffffu, r, 0);
+    warp_argmax(v, r);
     if(lane == 0) {
       S.pr.cv[par][warp] = v;
       S.pr.cr[par][warp] = r;
@@ -381,21 +377,7 @@ HPLB_DEV void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, dou
     // The winner among the warps' candidates (lanes 0..15 read one each).
     double bv = lane < kBW ? S.pr.cv[par][lane] : 0.0;
     int    br = lane < kBW ? S.pr.cr[par][lane] : -1;
-    int    bw = lane < kBW ? lane : -1;
-#pragma unroll
-    for(int off = 16; off > 0; off >>= 1) {
-      const double ov  = __shfl_down_sync(0xffffffffu, bv, off);
-      const int    orr = __shfl_down_sync(0xffffffffu, br, off);
-      const int    ow  = __shfl_down_sync(0xffffffffu, bw, off);
-      if(better_b(ov, orr, bv, br)) {
-        bv = ov;
-        br = orr;
-        bw = ow;
-      }
-    }
-    bv = __shfl_sync(0xffffffffu, bv, 0);
-    br = __shfl_sync(0xffffffffu, br, 0);
-    bw = __shfl_sync(0xffffffffu, bw, 0);
+    int    bw = warp_argmax(bv, br);
     if(bw < 0) {  // no candidate: only when the panel has no rows >= j, which cannot happen
       bw = 0;
       bv = 0.0;
@@ -417,10 +399,12 @@ HPLB_DEV void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, dou
         for(int c = 0; c < KB; ++c) x[q][c] = S.pr.cur[par][c];
       }
       if(bv != 0.0 && row[q] > j) {
-        const double l = x[q][j] / bv;
-        x[q][j]        = l;
+        const double l = pick(x[q], j) / bv;
 #pragma unroll
-        for(int c = j + 1; c < KB; ++c) x[q][c] = x[q][c] - l * u[c];
+        for(int c = 0; c < KB; ++c) {
+          if(c == j) x[q][c] = l;
+          else if(c > j) x[q][c] = x[q][c] - l * u[c];
+        }
       }
     }
   }
@@ -443,7 +427,7 @@ HPLB_DEV void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, dou
 // DMMA (A fragments straight from P, B fragments from the staged block, C
 // fragments from and back to global memory) with no block barrier between
 // strips.
-HPLB_DEV void update_strips(const double* P, int ldp, int kb, int m2, const double* U, int ldu,
+__device__ __noinline__ void update_strips(const double* P, int ldp, int kb, int m2, const double* U, int ldu,
                             double* C, int ldc, int ncols, Smem& S) {
   if(m2 <= 0 || ncols <= 0 || kb <= 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -507,15 +491,9 @@ HPLB_DEV void solve_system(const Args& a, const Sys& y, double* P, Smem& S) {
     __syncthreads();
     if(kb <= kRegPanelW && m <= 2 * kBT) {
       if(m <= kBT) {
-        if(kb <= 8)
-          panel_reg<1, 8>(Ap, n, m, kb, k0, ip, P, ldp, S);
-        else
-          panel_reg<1, 16>(Ap, n, m, kb, k0, ip, P, ldp, S);
+        panel_reg<1, kRegPanelW>(Ap, n, m, kb, k0, ip, P, ldp, S);
       } else {
-        if(kb <= 8)
-          panel_reg<2, 8>(Ap, n, m, kb, k0, ip, P, ldp, S);
-        else
-          panel_reg<2, 16>(Ap, n, m, kb, k0, ip, P, ldp, S);
+        panel_reg<2, kRegPanelW>(Ap, n, m, kb, k0, ip, P, ldp, S);
       }
     } else {
     // Panel to shared memory.
@@ -580,41 +558,38 @@ HPLB_DEV void solve_system(const Args& a, const Sys& y, double* P, Smem& S) {
       S.dst[x] = pos >= kb ? pos : -1;
     }
     load_diag(A + k0 + (size_t)k0 * n, n, kb, S);
-    // Interchanges on every other column of A and on B, and on the columns
-    // right of the panel (and B) the unit-lower solve with L11, fused: each
-    // thread gathers its column's new top rows and displaced rows into
-    // registers before it stores anything.
+    // Interchanges on every other column of A and on B: each thread gathers
+    // its column's new top rows into registers before it stores anything.
     const int rest = n - k0 - kb;
     const int ncol = k0 + rest + nrhs;
     for(int q = threadIdx.x; q < ncol; q += kBT) {
       double* col = q < k0 ? A + (size_t)q * n
                            : (q < k0 + rest ? A + (size_t)(q + kb) * n : B + (size_t)(q - k0 - rest) * n);
       col += k0;
-      double x[kNbMax], o[kNbMax];
+      double x[kNbMax];
 #pragma unroll
       for(int r = 0; r < kNbMax; ++r)
-        if(r < kb) {
-          x[r] = col[S.src[r]];
-          o[r] = S.dst[r] >= 0 ? col[r] : 0.0;
-        }
+        if(r < kb) x[r] = col[S.src[r]];
+      // The displaced old top rows go below the block (dst >= kb), which no
+      // later access of this column reads; 8 loads in flight at a time.
 #pragma unroll
-      for(int r = 0; r < kNbMax; ++r)
-        if(r < kb && S.dst[r] >= 0) col[S.dst[r]] = o[r];
-      if(q >= k0) {
+      for(int h = 0; h < kNbMax; h += 8) {
+        double o[8];
 #pragma unroll
-        for(int r = 0; r < kNbMax; ++r)
-          if(r < kb) {
-            double t = x[r];
+        for(int r = 0; r < 8; ++r)
+          o[r] = (h + r < kb && S.dst[h + r] >= 0) ? col[h + r] : 0.0;
 #pragma unroll
-            for(int c = 0; c < r; ++c) t -= S.D[r][c] * x[c];
-            x[r] = t;
-          }
+        for(int r = 0; r < 8; ++r)
+          if(h + r < kb && S.dst[h + r] >= 0) col[S.dst[h + r]] = o[r];
       }
 #pragma unroll
       for(int r = 0; r < kNbMax; ++r)
         if(r < kb) col[r] = x[r];
     }
     __syncthreads();
+    // U12 = L11^-1 A12 and the same for B's rows.
+    diag_solve<LOWER_UNIT>(kb, A + k0 + (size_t)(k0 + kb) * n, n, rest, S);
+    diag_solve<LOWER_UNIT>(kb, B + k0, n, nrhs, S);
     if(rest + nrhs > 0) {
       // A22 -= L21 U12, B2 -= L21 B1 (L21 from the panel copy in shared memory).
       update_strips(P, ldp, kb, rest, A + k0 + (size_t)(k0 + kb) * n, n,
@@ -643,7 +618,7 @@ constexpr int kGk      = 32;  // k depth of one staged chunk of gemm_nn_sub
 // (G: two buffers of A 32 x 64 and B 64 x 32), the next chunk loaded into
 // registers while the current one is multiplied.  16 warps in 4 x 4, each 16
 // rows x 16 columns.
-HPLB_DEV void gemm_nn_sub(int m, int n, int k, const double* A, int64_t lda, const double* B,
+__device__ __noinline__ void gemm_nn_sub(int m, int n, int k, const double* A, int64_t lda, const double* B,
                           int64_t ldb, double* C, int64_t ldc, double* G) {
   if(m <= 0 || n <= 0 || k <= 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -767,6 +742,7 @@ HPLB_DEV void rec_leaf(double* A, double* B, int n, int nrhs, int* ip, int c0, i
         x[r] = col[S.src[r]];
         o[r] = S.dst[r] >= 0 ? col[r] : 0.0;
       }
+    // The displaced old top rows go below the block (dst >= w).
 #pragma unroll
     for(int r = 0; r < kRecLeaf; ++r)
       if(r < w && S.dst[r] >= 0) col[S.dst[r]] = o[r];
@@ -791,42 +767,58 @@ HPLB_DEV void trsm_lower_unit(int w1, int ncols, const double* L, int64_t ldl, d
   }
 }
 
+// Width of the left half of a node of the recursive factorisation (w > 16):
+// about half, rounded up to a whole number of leaves.
+HPLB_DEV int rec_split(int w) {
+  const int w1 = ((w / 2 + kRecLeaf - 1) / kRecLeaf) * kRecLeaf;
+  return w1 < w ? w1 : w - kRecLeaf;
+}
+
 // Recursive factorisation of one system (the columns split in halves down to
-// 16-wide leaves, an explicit stack in place of recursion), then X = U^-1
-// L^-1 B by blocks (B took every interchange as it happened).
+// 16-wide leaves), then X = U^-1 L^-1 B by blocks (B took every interchange
+// as it happened).  The recursion is walked without a stack: the leaves are
+// factored left to right, and after the leaf that ends at column pos the one
+// node whose left half ends at pos does its update (U12 = L11^-1 A12, then
+// A22 -= L21 U12) -- the order of the recursive algorithm.  Both are found
+// by a descent from the root, so the walk lives in a few registers.
 HPLB_DEV void solve_system_rec(const Args& a, const Sys& y, double* P, double* G, Smem& S) {
   const int n = y.n, nrhs = y.nrhs;
   double*   A  = a.A + y.a_off;
   double*   B  = a.B + y.b_off;
   int*      ip = a.ipiv + y.p_off;
   if(threadIdx.x == 0) S.info = 0;
-  int c0s[12], ws[12], w1s[12], stage[12];
-  int top = 0;
-  c0s[0] = 0, ws[0] = n, stage[0] = 0;
-  while(top >= 0) {
-    const int c0 = c0s[top], w = ws[top];
-    if(w <= kRecLeaf) {
-      rec_leaf(A, B, n, nrhs, ip, c0, w, P, S);
-      --top;
-      continue;
+  int pos = 0;
+  while(pos < n) {
+    int c0 = 0, w = n;
+    while(w > kRecLeaf) {  // the leaf that starts at pos
+      const int w1 = rec_split(w);
+      if(pos < c0 + w1) {
+        w = w1;
+      } else {
+        c0 += w1;
+        w -= w1;
+      }
     }
-    if(stage[top] == 0) {
-      const int w1 = ((w / 2 + kRecLeaf - 1) / kRecLeaf) * kRecLeaf;
-      w1s[top]     = w1 < w ? w1 : w - kRecLeaf;
-      stage[top]   = 1;
-      ++top;
-      c0s[top] = c0, ws[top] = w1s[top - 1], stage[top] = 0;
-    } else if(stage[top] == 1) {
-      const int w1 = w1s[top], w2 = w - w1;
-      // U12 = L11^-1 A12, then A22 -= L21 U12 (rows c0 + w1 .. n).
-      trsm_lower_unit(w1, w2, A + c0 + (size_t)c0 * n, n, A + c0 + (size_t)(c0 + w1) * n, n, G, S);
-      gemm_nn_sub(n - c0 - w1, w2, w1, A + (c0 + w1) + (size_t)c0 * n, n,
-                  A + c0 + (size_t)(c0 + w1) * n, n, A + (c0 + w1) + (size_t)(c0 + w1) * n, n, G);
-      stage[top] = 2;
-      ++top;
-      c0s[top] = c0 + w1, ws[top] = w2, stage[top] = 0;
-    } else {
-      --top;
+    rec_leaf(A, B, n, nrhs, ip, c0, w, P, S);
+    pos = c0 + w;
+    c0 = 0, w = n;
+    while(pos < n && w > kRecLeaf) {  // the node whose left half ends at pos
+      const int w1 = rec_split(w);
+      if(pos == c0 + w1) {
+        const int w2 = w - w1;
+        trsm_lower_unit(w1, w2, A + c0 + (size_t)c0 * n, n, A + c0 + (size_t)(c0 + w1) * n, n,
+                        G, S);
+        gemm_nn_sub(n - c0 - w1, w2, w1, A + (c0 + w1) + (size_t)c0 * n, n,
+                    A + c0 + (size_t)(c0 + w1) * n, n, A + (c0 + w1) + (size_t)(c0 + w1) * n, n,
+                    G);
+        break;
+      }
+      if(pos < c0 + w1) {
+        w = w1;
+      } else {
+        c0 += w1;
+        w -= w1;
+      }
     }
   }
   // L Y = B (forward, 32-row blocks), then U X = Y (backward).
