@@ -99,33 +99,6 @@ HPLB_DEV bool better_b(double av, int ar, double bv, int br) {
   return ar < br;
 }
 
-// Argmax over the warp's candidates (v, r), r < 0 meaning none: the largest
-// |v|, the lowest row among equal magnitudes (the order of better_b for
-// finite values).  Branch free: |v| as an unsigned 64-bit key reduced by two
-// 32-bit max reductions (high word, then low word among the lanes that hold
-// the high maximum), the lowest matching row by a min reduction, the signed
-// value fetched from the lane that holds it.  Every lane gets the result;
-// returns the winning lane, or -1 if no lane has a candidate.
-HPLB_DEV int warp_argmax(double& v, int& r) {
-  const unsigned long long key =
-      r >= 0 ? (unsigned long long)__double_as_longlong(fabs(v)) : 0ull;
-  const unsigned hi  = (unsigned)(key >> 32), lo = (unsigned)key;
-  const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
-  const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
-  const bool     hit = r >= 0 && hi == mhi && lo == mlo;
-  const unsigned best = __reduce_min_sync(0xffffffffu, hit ? (unsigned)r : 0xffffffffu);
-  const unsigned who  = __ballot_sync(0xffffffffu, hit && (unsigned)r == best);
-  const int      wl   = who ? __ffs(who) - 1 : 0;
-  v = __shfl_sync(0xffffffffu, v, wl);
-  if(!who) {
-    v = 0.0;
-    r = -1;
-    return -1;
-  }
-  r = (int)best;
-  return wl;
-}
-
 HPLB_DEV void argmax_block(double& v, int& r, Smem& S) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   warp_argmax(v, r);

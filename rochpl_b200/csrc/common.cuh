@@ -38,6 +38,36 @@ HPLB_DEV void st_release_gpu(int* p, int v) {
   asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
 
+// Pivot search order: the larger |v| wins, ties go to the lower row; r < 0
+// marks "no candidate".  warp_argmax reduces the warp's (v, r) pairs in that
+// order without branches: |v| as an unsigned 64-bit key reduced by two 32-bit
+// max reductions (high word, then low word among the lanes holding the high
+// maximum), the lowest matching row by a min reduction, the signed value
+// taken from the lane that holds it.  Every lane gets the result; returns the
+// winning lane, or -1 (v = 0, r = -1) if no lane has a candidate.  For finite
+// values the order is that of a sequential scan with "strictly larger |v|
+// replaces" over increasing rows (LAPACK's idamax); a NaN magnitude ranks
+// above every finite one.
+HPLB_DEV int warp_argmax(double& v, int& r) {
+  const unsigned long long key =
+      r >= 0 ? (unsigned long long)__double_as_longlong(fabs(v)) : 0ull;
+  const unsigned hi   = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mhi  = __reduce_max_sync(0xffffffffu, hi);
+  const unsigned mlo  = __reduce_max_sync(0xffffffffu, hi == mhi ? lo : 0u);
+  const bool     hit  = r >= 0 && hi == mhi && lo == mlo;
+  const unsigned best = __reduce_min_sync(0xffffffffu, hit ? (unsigned)r : 0xffffffffu);
+  const unsigned who  = __ballot_sync(0xffffffffu, hit && (unsigned)r == best);
+  const int      wl   = who ? __ffs(who) - 1 : 0;
+  v = __shfl_sync(0xffffffffu, v, wl);
+  if(!who) {
+    v = 0.0;
+    r = -1;
+    return -1;
+  }
+  r = (int)best;
+  return wl;
+}
+
 // Grid-wide barrier for co-resident (cooperatively launched) grids, on a
 // monotonic arrival counter: the gen-th barrier of a launch (1-based) returns
 // once bar[0] >= gen * nblocks.  One atomic per block and no reset between

@@ -124,7 +124,9 @@ inline hplb_status ensure_leaf_ws(hplb_ctx* ctx, int n, int nbmin) {
   hplb_status s;
   if((s = grow(ctx, &ctx->d_ipiv, &ctx->ipiv_cap, (size_t)(n > 1 ? n : 1))) != HPLB_OK) return s;
   const int    gmax = leaf_grid_size(ctx->num_sms, n > 1 ? n : 1);
-  const size_t cand = 2 * (size_t)gmax * (2 + (nbmin < kMaxLeaf ? nbmin : kMaxLeaf));
+  // Slots of 2 + w doubles, rounded up to an even count so that the register
+  // leaf's 16-byte (value, row) accesses stay aligned.
+  const size_t cand = 2 * (size_t)gmax * (size_t)((3 + (nbmin < kMaxLeaf ? nbmin : kMaxLeaf)) & ~1);
   if((s = grow(ctx, &ctx->d_cand, &ctx->cand_cap, cand + 2 * kMaxLeaf)) != HPLB_OK) return s;
   ctx->d_cur = ctx->d_cand + cand;
   return HPLB_OK;

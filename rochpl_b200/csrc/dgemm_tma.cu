@@ -31,6 +31,8 @@
 //
 // Every mbarrier wait is bounded: a wait only expires when a copy never lands;
 // the CTA then records the site in the status word and exits.
+#include <cstdlib>
+
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
@@ -312,7 +314,59 @@ bool get_encoder() {
   return true;
 }
 
-constexpr int kTpc = 4;
+// Tiles per CTA.  Four (a whole group: the A tile fetched once and re-read
+// from L2 by the group's other column tiles, one pipeline across them) for a
+// large product, at least 256 tiles per SM -- the trailing update while it is
+// the critical path.  Below that, one: the panel's own updates spread over
+// the SMs, and the trailing update's CTAs retire every tile, so the
+// high-priority panel kernels (the critical path once the trailing matrix is
+// small) wait less for SMs.  Measured at N = 16384 (getrf, NB = 512, B200):
+// 251 ms with four, 208 ms with one, identical bits.  HPLB_DGEMM_TPC = 1, 2
+// or 4 fixes the choice.
+int tiles_per_cta(long long ntiles) {
+  static const int forced = [] {
+    const char* e = getenv("HPLB_DGEMM_TPC");
+    const int   v = e ? atoi(e) : 0;
+    return (v == 1 || v == 2 || v == 4) ? v : 0;
+  }();
+  static const int sms = [] {
+    int dev = 0, n = 148;
+    if(cudaGetDevice(&dev) != cudaSuccess ||
+       cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+      cudaGetLastError();
+      n = 148;
+    }
+    return n;
+  }();
+  if(forced) return forced;
+  return ntiles >= 256LL * sms ? 4 : 1;
+}
+
+template <int TPC>
+cudaError_t launch_tpc(const CUtensorMap& mA, const CUtensorMap& mB, int m, int n, int k,
+                       double* C, int64_t ldc, int tiles_m, int tiles_n, bool accumulate,
+                       int* status, cudaStream_t stream) {
+  static bool attr = false;
+  if(!attr) {
+    cudaError_t e = cudaFuncSetAttribute(dgemm_tma_kernel<TPC, true>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if(e == cudaSuccess)
+      e = cudaFuncSetAttribute(dgemm_tma_kernel<TPC, false>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
+    if(e != cudaSuccess) return e;
+    attr = true;
+  }
+  const long long ntiles = (long long)tiles_m * tiles_n;
+  const long long grid   = (ntiles + TPC - 1) / TPC;
+  if(grid > 0x7fffffff) return cudaErrorInvalidValue;
+  if(accumulate)
+    dgemm_tma_kernel<TPC, true><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
+        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
+  else
+    dgemm_tma_kernel<TPC, false><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
+        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
+  return cudaGetLastError();
+}
 
 }  // namespace
 
@@ -350,27 +404,15 @@ cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda, 
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if(r != CUDA_SUCCESS) return cudaErrorInvalidValue;
   }
-  static bool attr = false;
-  if(!attr) {
-    cudaError_t e = cudaFuncSetAttribute(dgemm_tma_kernel<kTpc, true>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    if(e == cudaSuccess)
-      e = cudaFuncSetAttribute(dgemm_tma_kernel<kTpc, false>,
-                               cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
-    if(e != cudaSuccess) return e;
-    attr = true;
-  }
   const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  const long long ntiles = (long long)tiles_m * tiles_n;
-  const long long grid   = (ntiles + kTpc - 1) / kTpc;
-  if(grid > 0x7fffffff) return cudaErrorInvalidValue;
-  if(accumulate)
-    dgemm_tma_kernel<kTpc, true><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
-        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
-  else
-    dgemm_tma_kernel<kTpc, false><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
-        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
-  return cudaGetLastError();
+  switch(tiles_per_cta((long long)tiles_m * tiles_n)) {
+    case 1:
+      return launch_tpc<1>(mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, accumulate, status, stream);
+    case 2:
+      return launch_tpc<2>(mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, accumulate, status, stream);
+    default:
+      return launch_tpc<4>(mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, accumulate, status, stream);
+  }
 }
 
 }  // namespace hplb

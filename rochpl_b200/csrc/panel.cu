@@ -42,46 +42,22 @@ HPLB_DEV bool better(double av, int ar, double bv, int br) {
   return ar < br;
 }
 
-// Block-wide arg-max; result valid in every thread.
+// Block-wide arg-max in the order of `better`; result valid in every thread.
+// Two barriers: the first also orders this call's writes of s_v / s_r after
+// the previous call's reads.
 HPLB_DEV void block_argmax(double& v, int& r, double* s_v, int* s_r) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for(int off = 16; off > 0; off >>= 1) {
-    const double ov = __shfl_down_sync(0xffffffffu, v, off);
-    const int    orow = __shfl_down_sync(0xffffffffu, r, off);
-    if(better(ov, orow, v, r)) {
-      v = ov;
-      r = orow;
-    }
-  }
+  warp_argmax(v, r);
   __syncthreads();
   if(lane == 0) {
     s_v[warp] = v;
     s_r[warp] = r;
   }
   __syncthreads();
-  if(warp == 0) {
-    const int nw = blockDim.x >> 5;
-    v = lane < nw ? s_v[lane] : 0.0;
-    r = lane < nw ? s_r[lane] : -1;
-#pragma unroll
-    for(int off = 16; off > 0; off >>= 1) {
-      const double ov = __shfl_down_sync(0xffffffffu, v, off);
-      const int    orow = __shfl_down_sync(0xffffffffu, r, off);
-      if(better(ov, orow, v, r)) {
-        v = ov;
-        r = orow;
-      }
-    }
-    if(lane == 0) {
-      s_v[0] = v;
-      s_r[0] = r;
-    }
-  }
-  __syncthreads();
-  v = s_v[0];
-  r = s_r[0];
-  __syncthreads();
+  const int nw = blockDim.x >> 5;
+  v = lane < nw ? s_v[lane] : 0.0;
+  r = lane < nw ? s_r[lane] : -1;
+  warp_argmax(v, r);
 }
 
 template <typename T>
@@ -374,13 +350,23 @@ __global__ void __launch_bounds__(kSmemLeafThreads) leaf_smem_kernel(LeafParams<
 
 // Leaf with every row in registers: thread t of block b owns rows
 // r0 + b * rpb + t + q * blockDim.x (q < RPT) across all w <= 32 leaf
-// columns.  The column loop is unrolled, so step k updates exactly columns
-// k+1 .. w-1 of the thread's rows without shared-memory traffic; a column
-// step costs the pivot search, one bounded grid barrier and two 32-word
-// reads (pivot row, old diagonal row).  Arithmetic identical to leaf_kernel
-// (division by the pivot, a_cc - l * u_cc), hence identical bits.
+// columns.  The column loop is a run-time loop (not unrolled: an unrolled
+// 32-step body is about a megabyte of code, fetched from L2 once per column);
+// its body reaches column k of the row registers by selects and updates
+// columns k+1 .. w-1 by predicated FMAs, so the rows stay in registers.  A
+// column step costs the pivot search, one bounded grid barrier and two
+// 32-word reads (pivot row, old diagonal row).  Arithmetic identical to
+// leaf_kernel (division by the pivot, a_cc - l * u_cc), hence identical bits.
 constexpr int kRegLeafW       = 32;
 constexpr int kRegLeafThreads = 256;
+
+template <typename T, int N>
+HPLB_DEV T pick_col(const T (&x)[N], int c) {
+  T s = x[0];
+#pragma unroll
+  for(int q = 1; q < N; ++q) s = (q == c) ? x[q] : s;
+  return s;
+}
 
 template <typename T, int RPT>
 __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams<T> P) {
@@ -391,10 +377,12 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
   __shared__ double s_piv;
   __shared__ int    s_p;
 
-  const int    G  = gridDim.x;
-  const int    lo = P.r0 + blockIdx.x * P.rpb;
-  const size_t ld = (size_t)P.ld;
-  const int    w  = P.w;
+  const int    G    = gridDim.x;
+  const int    lane = threadIdx.x & 31;
+  const int    lo   = P.r0 + blockIdx.x * P.rpb;
+  const size_t ld   = (size_t)P.ld;
+  const int    w    = P.w;
+  const int    sw   = (3 + w) & ~1;  // slot stride: 2 + w rounded up to even (16-byte pairs)
 
   T   x[RPT][kRegLeafW];
   int row[RPT];
@@ -408,26 +396,24 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
       x[q][c] = (in && c < w) ? P.A[(size_t)row[q] + (size_t)(P.c0 + c) * ld] : (T)0;
   }
 
-#pragma unroll
-  for(int k = 0; k < kRegLeafW; ++k) {
-    if(k >= w) break;
+#pragma unroll 1
+  for(int k = 0; k < w; ++k) {
     const int par = k & 1;
     const int d   = P.r0 + k;
     // This block's candidate among its rows >= d, and the rows it must publish.
     double v = 0.0;
     int    r = -1;
 #pragma unroll
-    for(int q = 0; q < RPT; ++q)
-      if(row[q] >= d && better((double)x[q][k], row[q], v, r)) {
-        v = x[q][k];
+    for(int q = 0; q < RPT; ++q) {
+      const double xk = (double)pick_col(x[q], k);
+      if(row[q] >= d && better(xk, row[q], v, r)) {
+        v = xk;
         r = row[q];
       }
-    block_argmax(v, r, s_v, s_r);
-    double* slot = P.cand + ((size_t)par * G + blockIdx.x) * (2 + w);
-    if(threadIdx.x == 0) {
-      slot[0] = v;
-      slot[1] = (double)r;
     }
+    block_argmax(v, r, s_v, s_r);
+    double* slot = P.cand + ((size_t)par * G + blockIdx.x) * sw;
+    if(threadIdx.x == 0) *reinterpret_cast<double2*>(slot) = make_double2(v, (double)r);
 #pragma unroll
     for(int q = 0; q < RPT; ++q) {
       if(r >= 0 && row[q] == r)
@@ -442,31 +428,36 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
     if(!grid_sync(P.bar, G, k + 1, P.status, 15)) return;
 
     if(threadIdx.x < 32) {
+      // Every block's (value, row) pair, all loads in flight before any
+      // comparison; then the lane's best, then the warp's.
+      constexpr int kHoist = 8;  // grids up to 256 blocks
+      double2       cv[kHoist];
+#pragma unroll
+      for(int t = 0; t < kHoist; ++t) {
+        const int b = lane + 32 * t;
+        cv[t] = b < G ? __ldcg(reinterpret_cast<const double2*>(P.cand + ((size_t)par * G + b) * sw))
+                      : make_double2(0.0, -1.0);
+      }
       double bv = 0.0;
       int    br = -1, bs = -1;
-      for(int b = threadIdx.x; b < G; b += 32) {
-        const double* sl = P.cand + ((size_t)par * G + b) * (2 + w);
-        const double  sv = __ldcg(sl);
-        const int     sr = (int)__ldcg(sl + 1);
-        if(better(sv, sr, bv, br)) {
-          bv = sv;
-          br = sr;
+#pragma unroll
+      for(int t = 0; t < kHoist; ++t)
+        if(better(cv[t].x, (int)cv[t].y, bv, br)) {
+          bv = cv[t].x;
+          br = (int)cv[t].y;
+          bs = lane + 32 * t;
+        }
+      for(int b = lane + 32 * kHoist; b < G; b += 32) {
+        const double2 c2 = __ldcg(reinterpret_cast<const double2*>(P.cand + ((size_t)par * G + b) * sw));
+        if(better(c2.x, (int)c2.y, bv, br)) {
+          bv = c2.x;
+          br = (int)c2.y;
           bs = b;
         }
       }
-#pragma unroll
-      for(int off = 16; off > 0; off >>= 1) {
-        const double ov   = __shfl_down_sync(0xffffffffu, bv, off);
-        const int    orow = __shfl_down_sync(0xffffffffu, br, off);
-        const int    os   = __shfl_down_sync(0xffffffffu, bs, off);
-        if(better(ov, orow, bv, br)) {
-          bv = ov;
-          br = orow;
-          bs = os;
-        }
-      }
-      bs = __shfl_sync(0xffffffffu, bs, 0);
-      if(bs < 0) {  // unreachable while the leaf has rows >= d; keeps reads in bounds
+      const int wl = warp_argmax(bv, br);
+      bs           = __shfl_sync(0xffffffffu, bs, wl < 0 ? 0 : wl);
+      if(wl < 0 || bs < 0) {  // unreachable while the leaf has rows >= d; keeps reads in bounds
         bs = 0;
         bv = 0.0;
         br = d;
@@ -475,7 +466,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
         s_piv = bv;
         s_p   = br;
       }
-      const double* sl = P.cand + ((size_t)par * G + bs) * (2 + w);
+      const double* sl = P.cand + ((size_t)par * G + bs) * sw;
       if(threadIdx.x < w) {
         s_u[threadIdx.x]   = __ldcg(sl + 2 + threadIdx.x);
         s_cur[threadIdx.x] = __ldcg(P.cur + par * w + threadIdx.x);
@@ -498,10 +489,14 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
         for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_cur[c];
       }
       if(row[q] > d) {
-        const T l = x[q][k] / piv;
-        x[q][k]   = l;
+        const T l = pick_col(x[q], k) / piv;
 #pragma unroll
-        for(int cc = k + 1; cc < kRegLeafW; ++cc) x[q][cc] = x[q][cc] - l * (T)s_u[cc];
+        for(int c = 0; c < kRegLeafW; ++c) {
+          if(c == k)
+            x[q][c] = l;
+          else if(c > k)
+            x[q][c] = x[q][c] - l * (T)s_u[c];
+        }
       }
     }
   }
