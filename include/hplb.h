@@ -211,6 +211,14 @@ hplb_status hplb_residual_lcg(hplb_ctx* ctx, int n, uint64_t seed,
 /* Timings of the last hplb_pdgesv on this context. */
 hplb_status hplb_last_timing(const hplb_ctx* ctx, hplb_timing* out);
 
+/* Per-step times of the last hplb_pdgesv / hplb_getrf on this context, for
+ * the progress report of src/pgesv/HPL_pdgesv.cpp:136-341 (HPL_PROGRESS_REPORT):
+ * step i factors columns [col[i], col[i] + NB); ms[i] runs from the end of
+ * step i-1 (the start of the call for i = 0) to the end of step i's trailing
+ * update, CUDA events on the update stream.  *count = the number of steps;
+ * min(cap, *count) entries are written. */
+hplb_status hplb_last_steps(const hplb_ctx* ctx, int cap, int* count, int* col, double* ms);
+
 /* Building blocks, exposed for tests and tools (device pointers, synchronous).
  *   hplb_dgemm_sub : C(m x n) -= A(m x k) B(k x n), column-major; the trailing
  *                    update kernel of hplb_pdgesv (rocblas_dgemm call in

@@ -15,6 +15,8 @@ struct hplb_ctx {
   cudaStream_t s_pan   = nullptr;
   std::string  err;
   hplb_timing  timing{};
+  std::vector<int>    step_col;  // first column of each step of the last factorisation
+  std::vector<double> step_ms;   // its time, previous step's end to this step's end (ms)
 
   int*    d_status = nullptr;  // ST_COUNT ints
   int*    d_bar    = nullptr;  // 2 ints

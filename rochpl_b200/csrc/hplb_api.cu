@@ -319,6 +319,10 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
   CK(cudaStreamWaitEvent(ctx->s_pan, ev_start, 0));
 
   const int nb = algo->nb;
+  std::vector<cudaEvent_t> step_end;
+  step_end.reserve((size_t)(n + nb - 1) / nb);
+  ctx->step_col.clear();
+  ctx->step_ms.clear();
   if((s = S.panel(0, 0, ev_panel[0])) != HPLB_OK) return s;
   for(int j = 0; j < n; j += nb) {
     const int set = (j / nb) & 1;
@@ -334,6 +338,11 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
       if((s = S.panel(c1, set ^ 1, ev_panel[set ^ 1])) != HPLB_OK) return s;
     }
     if((s = S.update(j, set, c1 + la, n + (rhs ? 1 : 0) - (c1 + la))) != HPLB_OK) return s;
+    // Step j ends when its trailing update is done (the update stream has
+    // already waited for panel j); the progress report reads these.
+    step_end.push_back(next_event(ctx));
+    CK(cudaEventRecord(step_end.back(), ctx->s_upd));
+    ctx->step_col.push_back(j);
   }
   CK(cudaEventRecord(ev_lu, ctx->s_upd));
   if(rhs) CK(launch_trsv(dA, ld, n, dX, ctx->d_status, ctx->s_upd, &ctx->launches));
@@ -367,6 +376,10 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
   for(auto& p : S.panel_ev) {
     cudaEventElapsedTime(&ms, p.first, p.second);
     T.panel_ms += ms;
+  }
+  for(size_t i = 0; i < step_end.size(); ++i) {
+    cudaEventElapsedTime(&ms, i ? step_end[i - 1] : ev_start, step_end[i]);
+    ctx->step_ms.push_back(ms);
   }
   T.gemm_launches   = (int)S.gemm_ev.size();
   T.kernel_launches = ctx->launches;
@@ -424,6 +437,17 @@ hplb_status hplb_residual_lcg(hplb_ctx* ctx, int n, uint64_t seed, const double*
 hplb_status hplb_last_timing(const hplb_ctx* ctx, hplb_timing* out) {
   if(!ctx || !out) return HPLB_ERR_ARG;
   *out = ctx->timing;
+  return HPLB_OK;
+}
+
+hplb_status hplb_last_steps(const hplb_ctx* ctx, int cap, int* count, int* col, double* ms) {
+  if(!ctx || !count || cap < 0 || (cap > 0 && (!col || !ms))) return HPLB_ERR_ARG;
+  const int n = (int)ctx->step_ms.size();
+  *count      = n;
+  for(int i = 0; i < n && i < cap; ++i) {
+    col[i] = ctx->step_col[i];
+    ms[i]  = ctx->step_ms[i];
+  }
   return HPLB_OK;
 }
 

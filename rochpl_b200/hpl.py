@@ -142,6 +142,8 @@ class HplConfig:
     outfile: str | None = None
     iters: int = 1
     frac: float = 0.3
+    pmap: int = 1  # process mapping: 0 row-major, 1 column-major (the command line's)
+    bcasts: list = dataclasses.field(default_factory=lambda: [0])  # 0..5: 1rg .. blongM
 
     def algos(self):
         for nb in self.nbs:
@@ -197,7 +199,7 @@ def parse_hpl_dat(text: str) -> HplConfig:
     nbs = ints(nxt(), k)
     if any(v < 1 for v in nbs):
         raise HplInputError("Value of NB less than 1")
-    nxt()  # PMAP process mapping
+    pmap = 1 if first_int(nxt()) == 1 else 0  # PMAP: 1 column-major, else row-major
     k = count(nxt(), "grids")
     ps = ints(nxt(), k)
     qs = ints(nxt(), k)
@@ -220,7 +222,8 @@ def parse_hpl_dat(text: str) -> HplConfig:
     k = count(nxt(), "RFACT")
     rfacts = [_fact(v) for v in ints(nxt(), k)]
     k = count(nxt(), "BCAST")
-    nxt()  # broadcast topologies: a no-op at Q = 1
+    # Broadcast topologies: no data moves at Q = 1, but each is a test of its own.
+    bcasts = [v if 0 <= v <= 4 else 5 for v in ints(nxt(), k)]
     k = count(nxt(), "DEPTH")
     depths = ints(nxt(), k)
     if any(v < 0 for v in depths):
@@ -243,7 +246,7 @@ def parse_hpl_dat(text: str) -> HplConfig:
         raise HplInputError("Equilibration currently unsupported")
     return HplConfig(ns=ns, nbs=nbs, ps=ps, qs=qs, thrsh=thrsh, pfacts=pfacts, nbmins=nbmins,
                      ndivs=ndivs, rfacts=rfacts, depths=depths, l1notran=l1,
-                     outfile=outname if dev not in (6, 7) else None)
+                     outfile=outname if dev not in (6, 7) else None, pmap=pmap, bcasts=bcasts)
 
 
 def _isint(s: str) -> bool:

@@ -24,7 +24,7 @@ HPLB_ERR_UNSUPPORTED = 6
 EXPORTS = [
     "hplb_create", "hplb_destroy", "hplb_status_string", "hplb_last_error",
     "hplb_default_ld", "hplb_matgen", "hplb_pdgesv", "hplb_residual",
-    "hplb_residual_lcg", "hplb_last_timing", "hplb_dgemm_sub", "hplb_laswp_trsm",
+    "hplb_residual_lcg", "hplb_last_timing", "hplb_last_steps", "hplb_dgemm_sub", "hplb_laswp_trsm",
     "hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_residual_lcg_noalloc",
     "hplb_gemm_lp_sub", "hplb_pdgesv_mixed", "hplb_getrf", "hplb_getrs", "hplb_rank_k",
     "hplb_set_stream", "hplb_batch_create", "hplb_batch_destroy", "hplb_batch_layout",
@@ -104,6 +104,8 @@ def load() -> C.CDLL:
     L.hplb_residual.argtypes = [vp, i32, vp, i64, vp, C.POINTER(hplb_resid)]
     L.hplb_residual_lcg.argtypes = [vp, i32, u64, vp, C.POINTER(hplb_resid)]
     L.hplb_last_timing.argtypes = [vp, C.POINTER(hplb_timing)]
+    L.hplb_last_steps.argtypes = [vp, i32, C.POINTER(C.c_int), vp, vp]
+    L.hplb_last_steps.restype = i32
     L.hplb_dgemm_sub.argtypes = [vp, i32, i32, i32, vp, i64, vp, i64, vp, i64]
     L.hplb_laswp_trsm.argtypes = [vp, vp, i64, i32, i32, i32, vp, i32, i32]
     L.hplb_fp64_peak.argtypes = [vp, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -237,6 +239,16 @@ class Library:
         t = hplb_timing()
         self._check(self.L.hplb_last_timing(self.ctx, C.byref(t)))
         return {k: getattr(t, k) for k, _ in hplb_timing._fields_}
+
+    def last_steps(self) -> list:
+        """[(first column, ms), ...] per step of the last pdgesv / getrf."""
+        cnt = C.c_int(0)
+        self._check(self.L.hplb_last_steps(self.ctx, 0, C.byref(cnt), None, None))
+        n = cnt.value
+        cols = (C.c_int * max(n, 1))()
+        ms = (C.c_double * max(n, 1))()
+        self._check(self.L.hplb_last_steps(self.ctx, n, C.byref(cnt), cols, ms))
+        return [(int(cols[i]), float(ms[i])) for i in range(min(n, cnt.value))]
 
     def dgemm_sub(self, m, n, k, A, lda, B, ldb, Cp, ldc):
         self._check(self.L.hplb_dgemm_sub(self.ctx, m, n, k, A, lda, B, ldb, Cp, ldc))

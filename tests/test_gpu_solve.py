@@ -144,3 +144,42 @@ def test_repeat_solves_are_bitwise_reproducible(hlib, oracle):
     a = solve_both(hlib, oracle, 1500, 256, 32)
     b = solve_both(hlib, oracle, 1500, 256, 32)
     assert np.array_equal(a["x"].view(np.uint64), b["x"].view(np.uint64))
+
+
+@pytest.mark.parametrize("n,nb", [(1000, 128), (777, 100), (64, 128)])
+def test_step_times(hlib, n, nb):
+    """hplb_last_steps: one entry per NB-wide step, at columns 0, NB, 2 NB...,
+    positive times that add up to the factorisation's (the last step ends
+    where the LU ends)."""
+    import torch
+
+    from rochpl_b200.hpl import Algo, default_ld
+
+    ld = default_ld(n)
+    A = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+    X = torch.zeros(n, dtype=torch.float64, device="cuda")
+    hlib.matgen(n, n + 1, 100, A.data_ptr(), ld, nb)
+    hlib.pdgesv(Algo(nb, 16, 2, 2, 2, 1, 0).c(), n, A.data_ptr(), ld, X.data_ptr())
+    steps = hlib.last_steps()
+    assert [c for c, _ in steps] == list(range(0, n, nb))
+    assert all(ms > 0 for _, ms in steps)
+    lu = hlib.last_timing()["lu_ms"]
+    assert abs(sum(ms for _, ms in steps) - lu) <= 0.02 * lu + 0.05
+
+
+def test_driver_on_the_gpu(hlib):
+    """The run driver end to end on the device: two sizes, two repetitions
+    each, with the progress report; every residual passes."""
+    import io
+
+    from rochpl_b200.driver import GpuSolver, run
+    from rochpl_b200.hpl import HplConfig
+
+    out = io.StringIO()
+    cfg = HplConfig(ns=[300, 1000], nbs=[64], ps=[1], qs=[1], iters=2, nbmins=[16])
+    tally = run(cfg, out, GpuSolver(0), progress=True)
+    assert tally == {"passed": 4, "failed": 0, "skipped": 0}
+    text = out.getvalue()
+    assert text.count(" ...... PASSED") == 4 and text.count("Overall GFLOPS") == 4
+    assert ("WC10R2R16" + "1000".rjust(12) + " " + "64".rjust(5) + " " + "1".rjust(5) + " "
+            + "1".rjust(5)) in text
