@@ -29,6 +29,13 @@ def _nvcc() -> str:
     return "nvcc"
 
 
+def _cuda_home() -> str:
+    nv = _nvcc()
+    if os.path.isabs(nv):
+        return os.path.dirname(os.path.dirname(nv))
+    return os.environ.get("CUDA_HOME", "/usr/local/cuda")
+
+
 def _sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
 
@@ -63,9 +70,10 @@ def build(force: bool = False, verbose: bool = False) -> str:
         subprocess.check_call(cmd)
     cli_src = os.path.join(PKG, "cli", "hplb_main.cpp")
     if os.path.exists(cli_src) and (force or _stale(CLI, [cli_src, LIB])):
-        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, cli_src, "-o", CLI,
-               "-L", PKG, "-lhplb200", "-Wl,-rpath,$ORIGIN",
-               "-L/usr/local/cuda/lib64", "-lcudart"]
+        cuda = _cuda_home()
+        cmd = ["g++", "-O2", "-std=c++17", "-I", INCLUDE, "-I", os.path.join(cuda, "include"),
+               cli_src, "-o", CLI, "-L", PKG, "-lhplb200", "-Wl,-rpath,$ORIGIN",
+               "-L", os.path.join(cuda, "lib64"), "-lcudart"]
         subprocess.check_call(cmd)
     return LIB
 

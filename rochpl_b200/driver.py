@@ -132,6 +132,12 @@ def sweep(cfg: HplConfig):
                                                                 cfg.l1notran)
 
 
+def skipped(p: int, q: int, algo: Algo) -> bool:
+    """Tests this driver counts as skipped: grids beyond one process, and
+    values the library does not take (NBMIN > 128, NB > 2048, DEPTH != 1)."""
+    return p * q != 1 or algo.nbmin > 128 or algo.nb > 2048 or algo.depth != 1
+
+
 class GpuSolver:
     """One device, one [A|b] buffer reused while N stays the same.  A call
     generates [A|b] (seed 100), times hplb_pdgesv by the wall clock around the
@@ -200,8 +206,7 @@ def run(cfg: HplConfig, out=None, solver=None, progress: bool = False) -> dict:
     kpass = kfail = kskip = 0
     first = True
     for n, p, q, bc, algo in sweep(cfg):
-        if p * q != 1 or algo.nbmin > 128 or algo.nb > 2048 or algo.depth != 1:
-            # Grids beyond one process and values this library does not take.
+        if skipped(p, q, algo):
             kskip += 1
             continue
         warm = getattr(solver, "warmup", None)

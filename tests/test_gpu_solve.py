@@ -183,3 +183,46 @@ def test_driver_on_the_gpu(hlib):
     assert text.count(" ...... PASSED") == 4 and text.count("Overall GFLOPS") == 4
     assert ("WC10R2R16" + "1000".rjust(12) + " " + "64".rjust(5) + " " + "1".rjust(5) + " "
             + "1".rjust(5)) in text
+
+
+def test_native_driver_on_the_gpu(hlib, tmp_path):
+    """rochpl_b200/hplb (the C++ driver over the C ABI): a command-line run
+    with two repetitions and the progress report, and an HPL.dat run with a
+    skipped 2 x 1 grid, written to the file HPL.dat names."""
+    import os
+    import subprocess
+
+    from rochpl_b200.build import build
+
+    build()
+    cli = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "rochpl_b200",
+                       "hplb")
+    r = subprocess.run([cli, "-N", "1000", "-NB", "128", "-it", "2", "--progress"],
+                       capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert r.stdout.count(" ...... PASSED") == 2 and r.stdout.count("Overall GFLOPS") == 2
+    assert "Finished      2 tests with the following results:" in r.stdout
+    dat = "\n".join([
+        "HPLinpack benchmark input file", "test", "out.txt      output file name (if any)",
+        "8            device out (6=stdout,7=stderr,file)", "1            # of problems sizes (N)",
+        "777          Ns", "1            # of NBs", "64           NBs",
+        "0            PMAP process mapping (0=Row-,1=Column-major)",
+        "2            # of process grids (P x Q)", "1 2          Ps", "1 1          Qs",
+        "16.0         threshold", "2            # of panel fact", "0 1          PFACTs",
+        "1            # of recursive stopping criterium", "8            NBMINs",
+        "1            # of panels in recursion", "2            NDIVs",
+        "1            # of recursive panel fact.", "2            RFACTs",
+        "1            # of broadcast", "1            BCASTs",
+        "1            # of lookahead depth", "1            DEPTHs",
+        "1            SWAP (0=bin-exch,1=long,2=mix)", "64           swapping threshold",
+        "0            L1 in (0=transposed,1=no-transposed) form",
+        "0            U  in (0=transposed,1=no-transposed) form",
+        "0            Equilibration (0=no,1=yes)", "8            memory alignment in double (> 0)"])
+    (tmp_path / "HPL.dat").write_text(dat + "\n")
+    r = subprocess.run([cli, "-i", "HPL.dat"], capture_output=True, text=True, timeout=300,
+                       cwd=tmp_path)
+    assert r.returncode == 0, r.stderr
+    text = (tmp_path / "out.txt").read_text()
+    assert text.count(" ...... PASSED") == 2
+    assert "WR11R2L8" in text and "WR11R2C8" in text
+    assert "              2 tests skipped because of illegal input values." in text
