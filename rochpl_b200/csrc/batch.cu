@@ -585,14 +585,31 @@ HPLB_DEV void solve_system(const Args& a, const Sys& y, double* P, Smem& S) {
 constexpr int kRecLeaf = 16;  // leaf width of the recursive factorisation
 constexpr int kGk      = 32;  // k depth of one staged chunk of gemm_nn_sub
 
+constexpr int kGkStages = 4;  // chunks of gemm_nn_sub in flight
+
+// 8-byte asynchronous global -> shared copy; src_bytes = 0 writes zeros and
+// reads nothing (src must still be a valid address).
+HPLB_DEV void cp_async8(double* dst, const double* src, int src_bytes) {
+  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes)
+               : "memory");
+}
+HPLB_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+HPLB_DEV void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
 // C (m x n) -= A (m x k) B (k x n), all column-major in global memory, any k:
 // 64 x 64 C tiles, each accumulated in DMMA fragments over the whole k (C is
 // read and written once per call), operands staged 32 deep in shared memory
-// (G: two buffers of A 32 x 64 and B 64 x 32), the next chunk loaded into
-// registers while the current one is multiplied.  16 warps in 4 x 4, each 16
-// rows x 16 columns.
-__device__ __noinline__ void gemm_nn_sub(int m, int n, int k, const double* A, int64_t lda, const double* B,
-                          int64_t ldb, double* C, int64_t ldc, double* G) {
+// (G: kGkStages buffers of A 32 x 64 and B 64 x 32) by asynchronous copies
+// issued kGkStages - 1 chunks ahead of the one being multiplied, so that
+// several chunks' global loads are in flight behind the DMMAs.  16 warps in
+// 4 x 4, each 16 rows x 16 columns.
+__device__ __noinline__ void gemm_nn_sub(int m, int n, int k, const double* A, int64_t lda,
+                                         const double* B, int64_t ldb, double* C, int64_t ldc,
+                                         double* G) {
   if(m <= 0 || n <= 0 || k <= 0) return;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int g = lane >> 2, t = lane & 3;
@@ -602,30 +619,25 @@ __device__ __noinline__ void gemm_nn_sub(int m, int n, int k, const double* A, i
   constexpr int STAGE = kGk * LDA_S + kTile * LDB_S;
   const int tm = (m + kTile - 1) / kTile, tn = (n + kTile - 1) / kTile;
   const int nck = (k + kGk - 1) / kGk;
-  // Each thread moves 4 A and 4 B elements per chunk.
   for(int tile = 0; tile < tm * tn; ++tile) {
     const int m0 = (tile % tm) * kTile, n0 = (tile / tm) * kTile;
-    double    ra[4], rb[4];
-    auto fetch = [&](int ck) {
-#pragma unroll
-      for(int q = 0; q < 4; ++q) {
-        const int e = threadIdx.x + q * kBT;  // 0 .. 2047
-        const int r = e & (kTile - 1), kk = e >> 6;   // A: 64 rows x 32 k
-        const int gk = ck * kGk + kk;
-        ra[q] = (m0 + r < m && gk < k) ? A[(size_t)(m0 + r) + (size_t)gk * lda] : 0.0;
-        const int k2 = e & (kGk - 1), c = e >> 5;     // B: 32 k x 64 cols
-        const int gk2 = ck * kGk + k2;
-        rb[q] = (n0 + c < n && gk2 < k) ? B[(size_t)gk2 + (size_t)(n0 + c) * ldb] : 0.0;
-      }
-    };
-    auto stash = [&](int buf) {
-      double* As = G + buf * STAGE;
+    // Chunk ck into buffer ck % kGkStages: each thread copies 4 A and 4 B
+    // elements (zeros outside the matrices).
+    auto issue = [&](int ck) {
+      double* As = G + (ck % kGkStages) * STAGE;
       double* Bs = As + kGk * LDA_S;
 #pragma unroll
       for(int q = 0; q < 4; ++q) {
-        const int e = threadIdx.x + q * kBT;
-        As[(e >> 6) * LDA_S + (e & (kTile - 1))] = ra[q];
-        Bs[(e >> 5) * LDB_S + (e & (kGk - 1))]   = rb[q];
+        const int  e  = threadIdx.x + q * kBT;  // 0 .. 2047
+        const int  r  = e & (kTile - 1), kk = e >> 6;  // A: 64 rows x 32 k
+        const int  gk = ck * kGk + kk;
+        const bool ia = m0 + r < m && gk < k;
+        cp_async8(As + kk * LDA_S + r, ia ? A + (size_t)(m0 + r) + (size_t)gk * lda : A, ia ? 8 : 0);
+        const int  k2  = e & (kGk - 1), c = e >> 5;  // B: 32 k x 64 cols
+        const int  gk2 = ck * kGk + k2;
+        const bool ib  = n0 + c < n && gk2 < k;
+        cp_async8(Bs + c * LDB_S + k2, ib ? B + (size_t)gk2 + (size_t)(n0 + c) * ldb : B,
+                  ib ? 8 : 0);
       }
     };
     double acc[2][4];
@@ -636,14 +648,18 @@ __device__ __noinline__ void gemm_nn_sub(int m, int n, int k, const double* A, i
         const int r = m0 + wm + g + (q >> 1) * 8, c = n0 + wn + j * 8 + 2 * t + (q & 1);
         acc[j][q] = (r < m && c < n) ? C[(size_t)r + (size_t)c * ldc] : 0.0;
       }
-    fetch(0);
     __syncthreads();  // the previous tile's readers of G are done
-    stash(0);
-    __syncthreads();
+#pragma unroll
+    for(int s = 0; s < kGkStages - 1; ++s) {
+      if(s < nck) issue(s);
+      cp_async_commit();
+    }
     for(int ck = 0; ck < nck; ++ck) {
-      const int buf = ck & 1;
-      if(ck + 1 < nck) fetch(ck + 1);
-      const double* As = G + buf * STAGE;
+      cp_async_wait<kGkStages - 2>();  // this thread's copies of chunk ck have landed
+      __syncthreads();  // everyone's have; and chunk ck - 1's buffer is no longer read
+      if(ck + kGkStages - 1 < nck) issue(ck + kGkStages - 1);
+      cp_async_commit();
+      const double* As = G + (ck % kGkStages) * STAGE;
       const double* Bs = As + kGk * LDA_S;
 #pragma unroll
       for(int kk = 0; kk < kGk; kk += 8) {
@@ -660,8 +676,6 @@ __device__ __noinline__ void gemm_nn_sub(int m, int n, int k, const double* A, i
           dmma(acc[j], af, bf);
         }
       }
-      if(ck + 1 < nck) stash(buf ^ 1);
-      __syncthreads();
     }
 #pragma unroll
     for(int j = 0; j < 2; ++j)
@@ -671,6 +685,7 @@ __device__ __noinline__ void gemm_nn_sub(int m, int n, int k, const double* A, i
         if(r < m && c < n) C[(size_t)r + (size_t)c * ldc] = acc[j][q];
       }
   }
+  cp_async_wait<0>();
   __syncthreads();
 }
 
@@ -813,7 +828,9 @@ HPLB_DEV void solve_system_rec(const Args& a, const Sys& y, double* P, double* G
 
 // Dynamic shared memory of the recursive mode: the GEMM's two stages (the
 // leaves keep no panel copy).
-__host__ __device__ constexpr int rec_stage_doubles() { return 2 * (kGk * (kTile + 4) + kTile * (kGk + 4)); }
+__host__ __device__ constexpr int rec_stage_doubles() {
+  return kGkStages * (kGk * (kTile + 4) + kTile * (kGk + 4));
+}
 
 __global__ void __launch_bounds__(kBT, 1) batch_gesv_kernel(const Args* pa) {
   extern __shared__ __align__(16) double panel_smem[];
