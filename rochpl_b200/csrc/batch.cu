@@ -741,17 +741,55 @@ HPLB_DEV void rec_leaf(double* A, double* B, int n, int nrhs, int* ip, int c0, i
   __syncthreads();
 }
 
+// Width of the upper half of a node of the recursive triangular solve (w > 32):
+// about half, rounded up to whole 32-row diagonal blocks.
+HPLB_DEV int trsm_split(int w) {
+  const int h = ((w / 2 + kNbMax - 1) / kNbMax) * kNbMax;
+  return h < w ? h : w - kNbMax;
+}
+
 // X (w1 x ncols, leading dimension ldx) <- L^-1 X for the unit-lower w1 x w1 L
-// at L (leading dimension ldl): 32-row blocks, substitution on the diagonal
-// block, DMMA update of the rows below.
+// at L (leading dimension ldl), recursively: the rows split in halves down to
+// diagonal blocks of at most 32 rows, each solved by substitution; after a
+// node's upper half is solved, its lower half takes X2 -= L21 X1 in one DMMA
+// GEMM with k = the upper half's height.  The recursion is walked without a
+// stack, as in solve_system_rec: blocks top to bottom, and after the block
+// that ends at row pos the one node whose upper half ends at pos updates.
+// Each row of X is rewritten once per level (log2(w1 / 32) times) instead of
+// once per 32-row block.
 HPLB_DEV void trsm_lower_unit(int w1, int ncols, const double* L, int64_t ldl, double* X,
                               int64_t ldx, double* G, Smem& S) {
-  for(int rb = 0; rb < w1; rb += kNbMax) {
-    const int kb = min(kNbMax, w1 - rb);
-    load_diag(L + rb + (size_t)rb * ldl, ldl, kb, S);
-    diag_solve<LOWER_UNIT>(kb, X + rb, ldx, ncols, S);
-    gemm_nn_sub(w1 - rb - kb, ncols, kb, L + (rb + kb) + (size_t)rb * ldl, ldl, X + rb, ldx,
-                X + rb + kb, ldx, G);
+  if(w1 <= 0 || ncols <= 0) return;
+  int pos = 0;
+  while(pos < w1) {
+    int r0 = 0, h = w1;
+    while(h > kNbMax) {  // the diagonal block that starts at pos
+      const int h1 = trsm_split(h);
+      if(pos < r0 + h1) {
+        h = h1;
+      } else {
+        r0 += h1;
+        h -= h1;
+      }
+    }
+    load_diag(L + r0 + (size_t)r0 * ldl, ldl, h, S);
+    diag_solve<LOWER_UNIT>(h, X + r0, ldx, ncols, S);
+    pos = r0 + h;
+    r0 = 0, h = w1;
+    while(pos < w1 && h > kNbMax) {  // the node whose upper half ends at pos
+      const int h1 = trsm_split(h);
+      if(pos == r0 + h1) {
+        gemm_nn_sub(h - h1, ncols, h1, L + (r0 + h1) + (size_t)r0 * ldl, ldl, X + r0, ldx,
+                    X + r0 + h1, ldx, G);
+        break;
+      }
+      if(pos < r0 + h1) {
+        h = h1;
+      } else {
+        r0 += h1;
+        h -= h1;
+      }
+    }
   }
 }
 
@@ -809,14 +847,8 @@ HPLB_DEV void solve_system_rec(const Args& a, const Sys& y, double* P, double* G
       }
     }
   }
-  // L Y = B (forward, 32-row blocks), then U X = Y (backward).
-  for(int k0 = 0; k0 < n; k0 += kNbMax) {
-    const int kb = min(kNbMax, n - k0);
-    load_diag(A + k0 + (size_t)k0 * n, n, kb, S);
-    diag_solve<LOWER_UNIT>(kb, B + k0, n, nrhs, S);
-    gemm_nn_sub(n - k0 - kb, nrhs, kb, A + (k0 + kb) + (size_t)k0 * n, n, B + k0, n, B + k0 + kb,
-                n, G);
-  }
+  // L Y = B (forward, recursive), then U X = Y (backward, 32-row blocks).
+  trsm_lower_unit(n, nrhs, A, n, B, n, G, S);
   for(int k0 = (n - 1) / kNbMax * kNbMax; k0 >= 0; k0 -= kNbMax) {
     const int kb = min(kNbMax, n - k0);
     load_diag(A + k0 + (size_t)k0 * n, n, kb, S);
