@@ -793,6 +793,47 @@ HPLB_DEV void trsm_lower_unit(int w1, int ncols, const double* L, int64_t ldl, d
   }
 }
 
+// X (w1 x ncols, leading dimension ldx) <- U^-1 X for the upper-triangular
+// w1 x w1 U at U (leading dimension ldu), recursively, the mirror of
+// trsm_lower_unit: diagonal blocks bottom to top, and after the block that
+// starts at row pos the one node whose lower half starts at pos takes
+// X1 -= U12 X2 in one DMMA GEMM.
+HPLB_DEV void trsm_upper(int w1, int ncols, const double* U, int64_t ldu, double* X, int64_t ldx,
+                         double* G, Smem& S) {
+  if(w1 <= 0 || ncols <= 0) return;
+  int pos = w1;
+  while(pos > 0) {
+    int r0 = 0, h = w1;
+    while(h > kNbMax) {  // the diagonal block that ends at pos
+      const int h1 = trsm_split(h);
+      if(pos > r0 + h1) {
+        r0 += h1;
+        h -= h1;
+      } else {
+        h = h1;
+      }
+    }
+    load_diag(U + r0 + (size_t)r0 * ldu, ldu, h, S);
+    diag_solve<UPPER>(h, X + r0, ldx, ncols, S);
+    pos = r0;
+    r0 = 0, h = w1;
+    while(pos > 0 && h > kNbMax) {  // the node whose lower half starts at pos
+      const int h1 = trsm_split(h);
+      if(pos == r0 + h1) {
+        gemm_nn_sub(h1, ncols, h - h1, U + r0 + (size_t)(r0 + h1) * ldu, ldu, X + r0 + h1, ldx,
+                    X + r0, ldx, G);
+        break;
+      }
+      if(pos > r0 + h1) {
+        r0 += h1;
+        h -= h1;
+      } else {
+        h = h1;
+      }
+    }
+  }
+}
+
 // Width of the left half of a node of the recursive factorisation (w > 16):
 // about half, rounded up to a whole number of leaves.
 HPLB_DEV int rec_split(int w) {
@@ -847,14 +888,9 @@ HPLB_DEV void solve_system_rec(const Args& a, const Sys& y, double* P, double* G
       }
     }
   }
-  // L Y = B (forward, recursive), then U X = Y (backward, 32-row blocks).
+  // L Y = B, then U X = Y, both recursive.
   trsm_lower_unit(n, nrhs, A, n, B, n, G, S);
-  for(int k0 = (n - 1) / kNbMax * kNbMax; k0 >= 0; k0 -= kNbMax) {
-    const int kb = min(kNbMax, n - k0);
-    load_diag(A + k0 + (size_t)k0 * n, n, kb, S);
-    diag_solve<UPPER>(kb, B + k0, n, nrhs, S);
-    gemm_nn_sub(k0, nrhs, kb, A + (size_t)k0 * n, n, B + k0, n, B, n, G);
-  }
+  trsm_upper(n, nrhs, A, n, B, n, G, S);
   if(threadIdx.x == 0) a.info[&y - a.sys] = S.info;
 }
 
