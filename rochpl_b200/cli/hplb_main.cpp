@@ -438,8 +438,26 @@ void list(const Config& c, FILE* out) {
 
 }  // namespace
 
+const char* kUsage =
+    "usage: hplb [-N n] [-NB nb] [-P p] [-Q q] [-p p] [-q q] [-f frac] [-it k] [-i HPL.dat]\n"
+    "            [--progress] [--list] [--device d]\n"
+    "  -N, -NB        problem size and block size (default 45312, 384)\n"
+    "  -P, -Q         process grid; only 1 x 1 runs, other grids count as skipped tests\n"
+    "  -p, -q, -f     accepted for compatibility (node-local grid, panel fraction)\n"
+    "  -it k          timed repetitions of each test (after one warm-up)\n"
+    "  -i HPL.dat     read the parameter sweep from an HPL.dat\n"
+    "  --progress     per-step report (percent, column, step time, overall GFLOPS)\n"
+    "  --list         print the tests the sweep contains; no GPU is touched\n"
+    "  --device d     CUDA device (default 0)\n"
+    "exit status: 0 all passed, 1 bad input, 2 a residual check failed, 3 a library error\n";
+
 int main(int argc, char** argv) {
   std::vector<std::string> args(argv + 1, argv + argc);
+  for(const auto& a : args)
+    if(a == "-h" || a == "--help") {
+      std::fputs(kUsage, stdout);
+      return 0;
+    }
   bool                     progress = false, only_list = false;
   int                      device = 0;
   std::vector<std::string> rest;

@@ -121,3 +121,8 @@ def test_truncated_hpl_dat_and_bad_flags(cli, tmp_path):
                       (["-P", "0"], "Illegal value for P. Exiting ...")):
         r = _listed(cli, argv)
         assert r.returncode == 1 and r.stderr.strip() == msg
+
+
+def test_help(cli):
+    r = subprocess.run([cli, "--help"], capture_output=True, text=True, timeout=30)
+    assert r.returncode == 0 and r.stdout.startswith("usage: hplb")
