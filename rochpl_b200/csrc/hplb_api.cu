@@ -303,6 +303,8 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
   if(s != HPLB_OK) return s;
   if(info) *info = 0;
   ctx->timing = hplb_timing{};
+  ctx->step_col.clear();
+  ctx->step_ms.clear();
   if(n == 0) return HPLB_OK;
   if(!dA || (rhs && !dX)) return set_err(ctx, HPLB_ERR_ARG, "null matrix or solution");
   ENTER(ctx);
@@ -321,8 +323,6 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
   const int nb = algo->nb;
   std::vector<cudaEvent_t> step_end;
   step_end.reserve((size_t)(n + nb - 1) / nb);
-  ctx->step_col.clear();
-  ctx->step_ms.clear();
   if((s = S.panel(0, 0, ev_panel[0])) != HPLB_OK) return s;
   for(int j = 0; j < n; j += nb) {
     const int set = (j / nb) & 1;
