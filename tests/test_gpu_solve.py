@@ -165,6 +165,8 @@ def test_step_times(hlib, n, nb):
     assert all(ms > 0 for _, ms in steps)
     lu = hlib.last_timing()["lu_ms"]
     assert abs(sum(ms for _, ms in steps) - lu) <= 0.02 * lu + 0.05
+    hlib.pdgesv(Algo(nb, 16, 2, 2, 2, 1, 0).c(), 0, A.data_ptr(), ld, X.data_ptr())
+    assert hlib.last_steps() == []  # a call with N = 0 keeps no earlier steps
 
 
 def test_driver_on_the_gpu(hlib):
