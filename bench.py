@@ -11,22 +11,40 @@ repeats.  Timing is CUDA events on the launching streams, max over ranks.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Before the timed steps the generated N = 131072 [A|b] is checked bit for bit
+against the oracle's LCG (sampled entries over the whole matrix, column b and
+the last 512-column block, LCG state indices up to 1.7e10) and, for seed 100,
+against the reference generator's hashes in tests/golden/lcg_c2_golden.json.
+After them: the HPL config of N = 4096, NB = 256 ("c1"), and a parity solve at
+N = 16384, NB = 512 against the oracle's own solve of the same system (pivot
+divergences by column, x error against 64 N eps kappa; "parity").
+
 After the FP64 steps the same system is solved in the mixed-precision form
 (16-bit tensor-core LU, BF16 x3 and FP16 x3, + FP64 GMRES refinement to the
 same residual threshold); its time to solution, speed-up over the FP64 solve,
-iteration counts and distance to the FP64 x go under "mixed" in the line.
+iteration counts and distance to the FP64 x go under "mixed" in the line; the
+same at N = 32768 and 65536 against FP64 solves of those systems
+("mixed.by_n").
 
 Then the batched form (4096 LCG systems, N log-uniform in [32, 1024], nrhs
 1 / 16 / 64, one persistent graph-captured launch each) and the
 differentiable solve (N = 16384 with 32 RHS, forward and backward; 256
 systems with N in [64, 512] through the batched form) go under "batched" and
-"autograd".
+"autograd" (the N = 16384 gradients are checked against torch's FP64 solve
+and against central differences with step 1e-6).
 
 Multi-GPU runs are replicas (each rank solves its own system; P = Q = 1 has
 no inter-GPU data path), reported as weak scaling.
 
 --impl reference times the reference algorithm's CPU restatement (the oracle,
-host OpenBLAS on every host core) on bounded samples of the same workload.
+host OpenBLAS on every host core): N = 16384 on every step and N = 32768 once,
+then the N = 131072 time extrapolated from the N = 32768 point as N^3 (the host
+cannot hold the 137.5 GB matrix beside the run, and one host solve of it would
+take about an hour).
+
+--case NAME runs one small kernel case for profiling and prints its event-timed
+rate (dgemm, solve, gemm_lp, getrf, mixed, batch; sizes from --n / --nb / --k /
+--prec / --nrhs), so the same command can run plainly before it runs under ncu.
 """
 from __future__ import annotations
 
@@ -121,47 +139,92 @@ class ClockSampler:
 # CPU baseline: the oracle port with host OpenBLAS
 # ---------------------------------------------------------------------------
 
-def cpu_baseline(n: int, nb: int, steps: int = 1) -> dict:
+def host_info() -> dict:
+    """CPU model, logical cores and RAM of this host."""
+    model, ram = None, None
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                model = line.split(":", 1)[1].strip()
+                break
+        for line in open("/proc/meminfo"):
+            if line.startswith("MemTotal:"):
+                ram = int(line.split()[1]) * 1024 / 1e9
+                break
+    except OSError:
+        pass
+    return {"cpu_model": model, "nproc": os.cpu_count(), "ram_gb": ram}
+
+
+def oracle_solve(n: int, nb: int, seed: int = 100):
+    """One host solve by the oracle (generate, LU, back-solve, check), OpenBLAS
+    level 3 on every host core.  Returns (seconds, x, ipiv, resid, blas)."""
     from oracle import oracle as O
 
     O.lib()
     have_blas = O.use_blas(os.cpu_count())
-    best = None
-    for _ in range(steps):
-        t0 = time.perf_counter()
-        x, ipiv, info, resid = O.hpl_test(n, nb, 32, 2)
-        t = time.perf_counter() - t0
-        best = t if best is None else min(best, t)
-    return {"value": hpl_flops(n) / best / 1e12, "unit": UNIT, "cores": os.cpu_count(),
-            "kind": "port",
-            "sample": f"N={n} NB={nb} NBMIN=32 NDIV=2 R/R seed 100, generate+LU+back-solve+check "
-                      f"on the host, {'OpenBLAS' if have_blas else 'scalar'} level-3, "
-                      f"{os.cpu_count()} threads; value = (2/3N^3+2N^2)/t",
-            "resid": resid, "seconds": best}
+    t0 = time.perf_counter()
+    x, ipiv, info, resid = O.hpl_test(n, nb, 32, 2, seed=seed)
+    return time.perf_counter() - t0, x, ipiv, resid, have_blas
+
+
+def cpu_baseline(n: int, nb: int) -> tuple[dict, object, object]:
+    t, x, ipiv, resid, have_blas = oracle_solve(n, nb)
+    cb = {"value": hpl_flops(n) / t / 1e12, "unit": UNIT, "cores": os.cpu_count(),
+          "kind": "port",
+          "sample": f"N={n} NB={nb} NBMIN=32 NDIV=2 R/R seed 100, generate+LU+back-solve+check "
+                    f"on the host, {'OpenBLAS' if have_blas else 'scalar'} level-3, "
+                    f"{os.cpu_count()} threads; value = (2/3N^3+2N^2)/t",
+          "resid": resid, "seconds": t, "host": host_info()}
+    return cb, x, ipiv
 
 
 def run_reference(args):
+    """The reference algorithm (its CPU restatement) on the host cores: N =
+    cpu_n on every step, N = cpu_n_big once, and the rate at N = args.n
+    extrapolated from the largest measured point with t proportional to N^3."""
     rank, world, _ = dist_env()
     if rank != 0:
         return 0
-    n_sample = args.cpu_n
+    n_step, n_big, target = args.cpu_n, args.cpu_n_big, args.n
     for _ in range(args.warmup):
-        cpu_baseline(max(1024, n_sample // 4), args.nb)
-    vals = []
+        oracle_solve(max(256, n_step // 4), args.nb)
+    steps = []
     for _ in range(args.steps):
-        vals.append(cpu_baseline(n_sample, args.nb))
-    v = statistics.median([c["value"] for c in vals])
-    cb = dict(vals[-1])
-    cb["value"] = v
+        t, _x, _p, resid, have_blas = oracle_solve(n_step, args.nb)
+        steps.append((t, resid))
+    t_step = statistics.median(t for t, _ in steps)
+    points = [{"n": n_step, "seconds": t_step, "tflops": hpl_flops(n_step) / t_step / 1e12,
+               "steps": args.steps, "resid_max": max(r for _, r in steps)}]
+    base_n, base_t = n_step, t_step
+    if n_big > n_step:
+        t, _x, _p, resid, _b = oracle_solve(n_big, args.nb)
+        points.append({"n": n_big, "seconds": t, "tflops": hpl_flops(n_big) / t / 1e12,
+                       "steps": 1, "resid_max": resid})
+        base_n, base_t = n_big, t
+    t_target = base_t * hpl_flops(target) / hpl_flops(base_n)
+    v = hpl_flops(target) / t_target / 1e12
+    extrapolated = target != base_n
+    cb = {"value": v, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+          "sample": (f"N={n_step} x {args.steps} steps" +
+                     (f" and N={n_big} once" if n_big > n_step else "") +
+                     f", NB={args.nb} NBMIN=32 NDIV=2 R/R seed 100, generate+LU+back-solve+check "
+                     f"on the host, {'OpenBLAS' if have_blas else 'scalar'} level-3, "
+                     f"{os.cpu_count()} threads" +
+                     (f"; N={target} extrapolated from N={base_n} as N^3" if extrapolated else "")),
+          "resid": max(p["resid_max"] for p in points), "host": host_info(),
+          "measured_points": points}
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": statistics.median([c["seconds"] for c in vals]) * 1e3,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_target * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (HPL LCG, seed 100)",
-        "config": {"workload": f"HPL FP64 solve, bounded host sample N={n_sample} of the "
-                               f"N={args.n} NB={args.nb} workload", "n": n_sample, "nb": args.nb,
-                   "parallelism": "host threads"},
+        "config": {"workload": f"HPL FP64 solve N={target} NB={args.nb} NBMIN=32 NDIV=2 "
+                               f"PFACT=R RFACT=R depth 1 on the host cores" +
+                               (f" (extrapolated as N^3 from measured N={base_n})"
+                                if extrapolated else ""),
+                   "n": target, "nb": args.nb, "extrapolated": extrapolated,
+                   "measured_points": points, "parallelism": "host threads"},
         "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -196,6 +259,7 @@ def run_ours(args):
     dP = torch.zeros(n, dtype=torch.int32, device="cuda")
 
     dmma_peak, dfma_peak = lib.fp64_peak(20000)
+    lcg = None if args.no_parity else lcg_check(lib, dA, n, ld, seed, nb)
 
     def step():
         lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, nb)  # outside the timed region
@@ -230,19 +294,29 @@ def run_ours(args):
     if not args.no_e2e:
         e2e = end_to_end(lib, algo, n, ld, seed, dA, dX, barrier, max_over_ranks, world)
 
+    # The HPL config N = 4096 (the reference's CPU-runnable case) and the
+    # parity solve against the oracle: rank 0, outside every timed region.
+    c1 = parity = cb = None
+    if rank == 0 and not args.no_c1:
+        c1 = c1_leg(lib, dmma_peak)
+    if rank == 0 and not (args.no_cpu_baseline and args.no_parity):
+        cb, xo, po = cpu_baseline(args.cpu_n, nb)
+        if not args.no_parity:
+            parity = {"lcg": lcg, "solve": parity_leg(lib, args.cpu_n, nb, xo, po)}
+        if args.no_cpu_baseline:
+            cb = None
+
     mixed = None
     if not args.no_mixed:
         x64 = dX.double().cpu().numpy()
         dA = None  # the FP64 [A|b] cannot stay beside the FP32 factors at this N
         torch.cuda.empty_cache()
         mixed = mixed_leg(lib, algo, n, seed, x64, solve_ms, args, barrier, max_over_ranks)
+        if args.mixed_sizes:
+            mixed["by_n"] = mixed_sizes_leg(lib, args, seed, barrier, max_over_ranks)
 
     batched = None if args.no_batched else batched_leg(lib, args, ranks)
     autograd = None if args.no_autograd else autograd_leg(lib, args, max_over_ranks)
-
-    cb = None
-    if rank == 0 and not args.no_cpu_baseline:
-        cb = cpu_baseline(args.cpu_n, nb)
 
     if rank == 0:
         peak = dmma_peak
@@ -260,7 +334,7 @@ def run_ours(args):
             "resid": res["resid"], "resid_passed": res["resid"] < 16.0,
             "gflops_reference_formula": world * (2 / 3 * n ** 3 + 1.5 * n ** 2)
             / (solve_ms_max * 1e-3) / 1e9,
-            "roofline": {"kernel": "dgemm_sub_kernel (trailing-update DMMA DGEMM)",
+            "roofline": {"kernel": "dgemm_tma_kernel (trailing-update DMMA DGEMM, TMA-fed)",
                          "bound": "tensor", "achieved": gemm_tf, "peak": peak, "unit": "TFLOP/s",
                          "frac": gemm_tf / peak,
                          "traffic": (args.gemm_traffic if args.gemm_traffic is not None else
@@ -287,9 +361,124 @@ def run_ours(args):
             line["autograd"] = autograd
         if cb is not None:
             line["cpu_baseline"] = cb
+        if c1 is not None:
+            line["c1"] = c1
+        if parity is not None:
+            line["parity"] = parity
         print(json.dumps(line), flush=True)
     ranks.close()
     return 0
+
+
+def lcg_check(lib, dA, n, ld, seed, nb, samples=100000) -> dict:
+    """The generated [A|b] against the oracle's LCG, bit for bit: `samples`
+    entries drawn over the whole matrix, column b and the last 512-column
+    block (state indices up to n^2 + n, past 2^32 at N = 131072), and for seed
+    100 the reference generator's block hashes from tests/golden/."""
+    import numpy as np
+    import torch
+
+    from oracle import oracle as O
+
+    lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, nb)
+    torch.cuda.synchronize()
+    cols = dA.view(n + 1, ld)  # row j of this view is column j of [A|b]
+    rng = np.random.default_rng(seed)
+    ii = rng.integers(0, n, samples)
+    jj = rng.integers(0, n + 1, samples)
+    ii[:2], jj[:2] = (0, n - 1), (0, n)
+    got = dA[torch.from_numpy(ii + jj * ld).cuda()].cpu().numpy()
+    ref = np.array([O.lcg_value(O.lcg_state(seed, n, int(i), int(j))) for i, j in zip(ii, jj)])
+    bad = int(np.count_nonzero(got.view(np.uint64) != ref.view(np.uint64)))
+    w = min(512, n)
+    blocks = {"column b": (n, 1), "last column block": (n - w, w)}
+    gold_path = os.path.join(ROOT, "tests", "golden", "lcg_c2_golden.json")
+    golden = None
+    if seed == 100 and os.path.exists(gold_path):
+        g = json.load(open(gold_path))
+        if g["n"] == n:
+            golden = {b["name"]: b for b in g["blocks"]}
+            for b in g["blocks"]:
+                blocks[b["name"]] = (b["col0"], b["ncols"])
+    out = {"entries_sampled": samples, "sample_mismatches": bad,
+           "max_state_index": n * (n + 1), "blocks": {}}
+    for name, (c0, wc) in blocks.items():
+        A = np.ascontiguousarray(cols[c0:c0 + wc, :n].cpu().numpy()).T  # n x wc, Fortran order
+        ref_b = O.matgen_block(n, 0, c0, n, wc, seed)
+        ok = bool(np.array_equal(A.view(np.uint64), ref_b.view(np.uint64)))
+        rec = {"col0": c0, "ncols": wc, "bit_exact_vs_oracle": ok}
+        if golden and name in golden:
+            rec["fnv1a"] = f"{O.hash_block(A, n, wc):016x}"
+            rec["matches_reference_generator"] = rec["fnv1a"] == golden[name]["fnv1a"]
+        out["blocks"][name] = rec
+        bad += 0 if ok else 1
+    out["bit_exact"] = bad == 0 and all(b.get("matches_reference_generator", True)
+                                       for b in out["blocks"].values())
+    return out
+
+
+def parity_leg(lib, n, nb, xo, po, seed=100) -> dict:
+    """The GPU solve of the system the oracle just solved on the host (N = n,
+    seed 100): pivot divergences by column, ||x - x_oracle||oo / ||x_oracle||oo
+    against 64 n eps kappa_oo (kappa from an FP64 inverse on the device, a
+    check only), and the HPL residual."""
+    import numpy as np
+    import torch
+
+    from rochpl_b200.hpl import Algo, default_ld
+
+    ld = default_ld(n)
+    dA = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+    dP = torch.zeros(n, dtype=torch.int32, device="cuda")
+    lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, nb)
+    A = dA.view(n + 1, ld)[:n, :n].t()
+    anorm = float(A.abs().sum(dim=1).max())
+    ainv = torch.linalg.inv(A)
+    kappa = anorm * float(ainv.abs().sum(dim=1).max())
+    del ainv, A
+    torch.cuda.empty_cache()
+    lib.pdgesv(Algo(nb, 32, 2, 2, 2, 1, 0).c(), n, dA.data_ptr(), ld, dX.data_ptr(), dP.data_ptr())
+    x, ipiv = dX.cpu().numpy(), dP.cpu().numpy()
+    div = np.nonzero(ipiv != np.asarray(po))[0]
+    err = float(np.max(np.abs(x - xo)) / np.max(np.abs(xo)))
+    tol = 64 * n * 2.0 ** -53 * kappa
+    res = lib.residual_lcg(n, seed, dX.data_ptr())
+    return {"n": n, "nb": nb, "seed": seed, "pivot_divergences": int(div.size),
+            "first_divergent_column": int(div[0]) if div.size else None,
+            "x_rel_err_vs_oracle": err, "x_tolerance": tol, "kappa_inf": kappa,
+            "x_within_tolerance": err <= tol, "resid": res["resid"],
+            "note": "oracle = the C restatement of the reference algorithm on the host "
+                    "(OpenBLAS level 3); tolerance 64 N eps kappa_oo"}
+
+
+def c1_leg(lib, peak, steps=10, warmup=3) -> dict:
+    """The HPL config N = 4096, NB = 256, NBMIN = 32, NDIV = 2, R/R, depth 1,
+    seed 100: per-solve device time (median of `steps`), rate, residual."""
+    import torch
+
+    from rochpl_b200.hpl import Algo, default_ld
+
+    n, nb = 4096, 256
+    ld = default_ld(n)
+    algo = Algo(nb, 32, 2, 2, 2, 1, 0)
+    dA = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+    ts = []
+    for it in range(warmup + steps):
+        lib.matgen(n, n + 1, 100, dA.data_ptr(), ld, nb)
+        lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr())
+        if it >= warmup:
+            ts.append(lib.last_timing())
+    ms = statistics.median(t["total_ms"] for t in ts)
+    res = lib.residual_lcg(n, 100, dX.data_ptr())
+    v = hpl_flops(n) / (ms * 1e-3) / 1e12
+    return {"workload": "HPL FP64 solve N=4096 NB=256 NBMIN=32 NDIV=2 PFACT=R RFACT=R depth 1, "
+                        "seed 100", "ms_per_solve": ms, "value": v, "unit": UNIT,
+            "frac_of_fp64_peak": v / peak, "resid": res["resid"], "resid_passed": res["resid"] < 16,
+            "steps": steps,
+            "breakdown_ms": {k: statistics.median(t[k] for t in ts)
+                             for k in ("lu_ms", "trsv_ms", "gemm_ms", "panel_ms")}}
 
 
 def _measured_peaks() -> dict:
@@ -300,53 +489,114 @@ def _measured_peaks() -> dict:
         return {}
 
 
-def mixed_leg(lib, algo, n, seed, x64, fp64_ms, args, barrier, max_over_ranks):
-    """The mixed-precision form on the same system: low-precision LU + GMRES
-    refinement to the HPL residual threshold, timed on the device (first to
-    last event of hplb_pdgesv_mixed), against the FP64 solve just timed.  A is
-    regenerated from the LCG for r = b - A x (bit-identical to the stored FP64
-    A, which does not fit in HBM beside the FP32 factors at N = 131072)."""
+def mixed_one(lib, algo, n, seed, prec, x64, fp64_ms, steps, warmup, barrier, max_over_ranks,
+              bf16_peak) -> dict:
+    """One precision of the mixed-precision form: low-precision LU + GMRES
+    refinement to the HPL residual threshold on the LCG system of `seed`,
+    timed on the device (first to last event of hplb_pdgesv_mixed), against
+    the FP64 solve of the same system (time fp64_ms, solution x64)."""
     import numpy as np
     import torch
 
+    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+    for _ in range(warmup):
+        lib.pdgesv_mixed(algo.c(), n, dX.data_ptr(), seed=seed, precision=prec)
+    reps = []
+    for _ in range(steps):
+        torch.cuda.synchronize()
+        barrier()
+        reps.append(lib.pdgesv_mixed(algo.c(), n, dX.data_ptr(), seed=seed, precision=prec))
+    tm = lib.last_timing()
+    ms = max_over_ranks(statistics.mean(r["total_ms"] for r in reps))
+    r = reps[-1]
+    chk = lib.residual_lcg(n, seed, dX.data_ptr())
+    x = dX.cpu().numpy()
+    gemm_tf = r["gemm_flops"] / (r["gemm_ms"] * 1e-3) / 1e12 if r["gemm_ms"] > 0 else 0.0
+    return {
+        "time_to_solution_ms": ms, "speedup_vs_fp64": fp64_ms / ms,
+        "value": hpl_flops(n) / (ms * 1e-3) / 1e12, "unit": UNIT,
+        "converged": bool(r["converged"]), "resid": chk["resid"],
+        "resid_passed": chk["resid"] < 16.0, "resid_lu_only": r["resid_lu"],
+        "outer_iters": r["outer_iters"], "gmres_iters": r["gmres_iters"],
+        "rel_err_vs_fp64_x": float(np.max(np.abs(x - x64)) / np.max(np.abs(x64))),
+        "lu_ms": r["lu_ms"], "ir_ms": r["ir_ms"], "panel_ms": r["panel_ms"],
+        "roofline": {"kernel": "gemm_lp_kernel (tcgen05 16-bit trailing update" +
+                               (", x3 split)" if prec >= 2 else ")"),
+                     "bound": "tensor", "achieved": gemm_tf, "peak": bf16_peak,
+                     "unit": "TFLOP/s", "frac": gemm_tf / bf16_peak,
+                     "gemm_ms": r["gemm_ms"], "gemm_flops": r["gemm_flops"]},
+        "gpu_launches": tm["kernel_launches"], "steps": steps,
+    }
+
+
+def _bf16_peak():
+    peaks = _measured_peaks()
+    if peaks.get("bf16_tflops_sustained"):
+        return peaks["bf16_tflops_sustained"], "MEASURED_PEAKS.json bf16_tflops_sustained"
+    return 1394.6, "fallback 1394.6"
+
+
+MIXED_NOTE = ("time to HPL scaled residual < 16 (target 16.0); value = (2/3N^3+2N^2)/t, the "
+              "HPL-equivalent rate; speedup = FP64 solve time / mixed time; GMRES-IR in FP64, "
+              "A regenerated from the LCG for r = b - Ax")
+
+
+def mixed_leg(lib, algo, n, seed, x64, fp64_ms, args, barrier, max_over_ranks):
+    """The mixed-precision form on the system of the FP64 steps (BF16 x3 and
+    FP16 x3), against the FP64 solve just timed.  A is regenerated from the LCG
+    for r = b - A x (bit-identical to the stored FP64 A, which does not fit in
+    HBM beside the FP32 factors at N = 131072)."""
     from rochpl_b200.lib import PREC_BF16X3, PREC_FP16X3
 
-    peaks = _measured_peaks()
-    bf16_peak = peaks.get("bf16_tflops_sustained") or 1394.6
-    src = "MEASURED_PEAKS.json bf16_tflops_sustained" if peaks else "fallback 1394.6"
-    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
-    out = {"note": "time to HPL scaled residual < 16 (target 16.0); value = (2/3N^3+2N^2)/t, "
-                   "the HPL-equivalent rate; speedup = FP64 solve time / mixed time; "
-                   "GMRES-IR in FP64, A regenerated from the LCG for r = b - Ax",
-           "bf16_peak_tflops": bf16_peak, "bf16_peak_source": src}
+    peak, src = _bf16_peak()
+    out = {"note": MIXED_NOTE, "bf16_peak_tflops": peak, "bf16_peak_source": src}
     for name, prec in (("bf16x3", PREC_BF16X3), ("fp16x3", PREC_FP16X3)):
-        for _ in range(max(1, args.mixed_warmup)):
-            lib.pdgesv_mixed(algo.c(), n, dX.data_ptr(), seed=seed, precision=prec)
-        reps = []
-        for _ in range(args.mixed_steps):
+        out[name] = mixed_one(lib, algo, n, seed, prec, x64, fp64_ms, args.mixed_steps,
+                              args.mixed_warmup, barrier, max_over_ranks, peak)
+    return out
+
+
+def mixed_sizes_leg(lib, args, seed, barrier, max_over_ranks) -> dict:
+    """The mixed-precision form at the other sizes of its config (N = 32768
+    and 65536, NB = 512), each against an FP64 solve of the same system timed
+    here; the plain (single-pass) BF16 / FP16 forms at N <= 32768 too, where
+    their result (converged or not) is part of the record."""
+    import torch
+
+    from rochpl_b200.hpl import Algo, default_ld
+    from rochpl_b200.lib import PREC_BF16, PREC_BF16X3, PREC_FP16, PREC_FP16X3
+
+    peak, _ = _bf16_peak()
+    algo = Algo(512, 32, 2, 2, 2, 1, 0)
+    out = {}
+    for n in args.mixed_sizes:
+        ld = default_ld(n)
+        dA = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+        dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+        ms = []
+        for it in range(1 + 2):
+            lib.matgen(n, n + 1, seed, dA.data_ptr(), ld, 512)
             torch.cuda.synchronize()
             barrier()
-            reps.append(lib.pdgesv_mixed(algo.c(), n, dX.data_ptr(), seed=seed, precision=prec))
-        tm = lib.last_timing()
-        ms = max_over_ranks(statistics.mean(r["total_ms"] for r in reps))
-        r = reps[-1]
-        chk = lib.residual_lcg(n, seed, dX.data_ptr())
-        x = dX.cpu().numpy()
-        gemm_tf = r["gemm_flops"] / (r["gemm_ms"] * 1e-3) / 1e12 if r["gemm_ms"] > 0 else 0.0
-        out[name] = {
-            "time_to_solution_ms": ms, "speedup_vs_fp64": fp64_ms / ms,
-            "value": hpl_flops(n) / (ms * 1e-3) / 1e12, "unit": UNIT,
-            "resid": chk["resid"], "resid_passed": chk["resid"] < 16.0,
-            "resid_lu_only": r["resid_lu"], "outer_iters": r["outer_iters"],
-            "gmres_iters": r["gmres_iters"],
-            "rel_err_vs_fp64_x": float(np.max(np.abs(x - x64)) / np.max(np.abs(x64))),
-            "lu_ms": r["lu_ms"], "ir_ms": r["ir_ms"], "panel_ms": r["panel_ms"],
-            "roofline": {"kernel": "gemm_lp_kernel (tcgen05 16-bit trailing update, x3 split)",
-                         "bound": "tensor", "achieved": gemm_tf, "peak": bf16_peak,
-                         "unit": "TFLOP/s", "frac": gemm_tf / bf16_peak,
-                         "gemm_ms": r["gemm_ms"], "gemm_flops": r["gemm_flops"]},
-            "gpu_launches": tm["kernel_launches"], "steps": args.mixed_steps,
-        }
+            lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr())
+            if it >= 1:
+                ms.append(lib.last_timing()["total_ms"])
+        fp64_ms = max_over_ranks(statistics.mean(ms))
+        res64 = lib.residual_lcg(n, seed, dX.data_ptr())
+        x64 = dX.cpu().numpy()
+        del dA, dX
+        torch.cuda.empty_cache()
+        rec = {"fp64": {"ms_per_solve": fp64_ms, "value": hpl_flops(n) / (fp64_ms * 1e-3) / 1e12,
+                        "resid": res64["resid"]}}
+        precs = [("bf16x3", PREC_BF16X3), ("fp16x3", PREC_FP16X3)]
+        if n <= 32768:
+            precs += [("bf16", PREC_BF16), ("fp16", PREC_FP16)]
+        for name, prec in precs:
+            rec[name] = mixed_one(lib, algo, n, seed, prec, x64, fp64_ms,
+                                  1 if prec < 2 else args.mixed_steps, 0 if prec < 2 else 1,
+                                  barrier, max_over_ranks, peak)
+        out[str(n)] = rec
+        torch.cuda.empty_cache()
     return out
 
 
@@ -444,6 +694,8 @@ def autograd_leg(lib, args, max_over_ranks):
               "forward_tflops": f_fwd / (tf * 1e-3) / 1e12,
               "backward_flops": 4.0 * n ** 2 * nrhs, "abs_residual_max": r,
               "note": "torch CUDA events on the current stream around hpl_solve and backward()"}
+    if not args.no_parity:
+        single["checks"] = autograd_checks(A, B, X.detach(), Xbar)
     del A, B, X, Xbar
     torch.cuda.empty_cache()
     rng = np.random.default_rng(20261203)
@@ -472,6 +724,62 @@ def autograd_leg(lib, args, max_over_ranks):
              "forward_backward_ms_wall": max_over_ranks(statistics.mean(tfb)),
              "note": "wall clock incl. packing the 512 tensors into pools"}
     return {"single": single, "batched": batch}
+
+
+def autograd_checks(A, B, X, Xbar, h=1e-6, fd_tol=1e-4) -> dict:
+    """Gradients of L = <Xbar, X(A, B)> after backward(): against an FP64
+    reference from torch's own dense solve (a check, not the product path)
+    within 64 n eps kappa_oo, and directional derivatives along unit-norm
+    directions of A and of B (half seeded-random, half along the computed
+    gradient) against central differences with step h."""
+    import torch
+
+    from rochpl_b200.autograd import hpl_solve
+
+    n = A.shape[0]
+    with torch.no_grad():
+        Ad, Bd = A.detach(), B.detach()
+        Xr = torch.linalg.solve(Ad, Bd)
+        Bbar_r = torch.linalg.solve(Ad.t(), Xbar)
+        Abar_r = -Bbar_r @ Xr.t()
+        kappa = float(Ad.abs().sum(dim=1).max()) * float(
+            torch.linalg.inv(Ad).abs().sum(dim=1).max())
+
+    def rel(a, b):
+        return float((a - b).abs().max() / b.abs().max())
+
+    tol = 64 * n * 2.0 ** -53 * kappa
+    out = {"kappa_inf": kappa, "tolerance": tol, "x_rel_err": rel(X, Xr),
+           "abar_rel_err": rel(A.grad, Abar_r), "bbar_rel_err": rel(B.grad, Bbar_r)}
+    out["within_tolerance"] = max(out["x_rel_err"], out["abar_rel_err"], out["bbar_rel_err"]) <= tol
+    del Xr, Bbar_r, Abar_r
+    g = torch.Generator(device=A.device).manual_seed(n)
+    dA = torch.randn(A.shape, generator=g, dtype=torch.float64, device=A.device)
+    dB = torch.randn(B.shape, generator=g, dtype=torch.float64, device=A.device)
+    # The normalised sum of a random unit direction and the computed
+    # gradient's direction: the derivative is then of the order of the
+    # gradient's norm, far above the difference quotient's rounding floor.
+    dA = dA / dA.norm() + A.grad / A.grad.norm()
+    dB = dB / dB.norm() + B.grad / B.grad.norm()
+    dA /= dA.norm()
+    dB /= dB.norm()
+
+    def L(Ap, Bp):
+        with torch.no_grad():
+            return float((hpl_solve(Ap, Bp, nb=512) * Xbar).sum())
+
+    fdA = (L(Ad + h * dA, Bd) - L(Ad - h * dA, Bd)) / (2 * h)
+    fdB = (L(Ad, Bd + h * dB) - L(Ad, Bd - h * dB)) / (2 * h)
+    anA = float((A.grad * dA).sum())
+    anB = float((B.grad * dB).sum())
+    out["fd"] = {"step": h, "tolerance": fd_tol,
+                 "direction": "unit norm: seeded Gaussian + the computed gradient's direction",
+                 "dA": {"analytic": anA, "central_difference": fdA,
+                        "rel_err": abs(anA - fdA) / abs(fdA)},
+                 "dB": {"analytic": anB, "central_difference": fdB,
+                        "rel_err": abs(anB - fdB) / abs(fdB)}}
+    out["fd"]["passed"] = max(out["fd"]["dA"]["rel_err"], out["fd"]["dB"]["rel_err"]) <= fd_tol
+    return out
 
 
 def _cudart():
@@ -549,6 +857,160 @@ def end_to_end(lib, algo, n, ld, seed, dA, dX, barrier, max_over_ranks, world):
                     "host; wall clock"}
 
 
+# ---------------------------------------------------------------------------
+# Small single-kernel cases for profiling (--case)
+# ---------------------------------------------------------------------------
+
+def case_dgemm(args) -> None:
+    """3 x hplb_dgemm_sub, --n x --n x --nb (k), random operands."""
+    import torch
+
+    from rochpl_b200 import library
+
+    lib = library(0)
+    m = n = args.n
+    k = args.nb
+    A = torch.randn(m * k, dtype=torch.float64, device="cuda")
+    B = torch.randn(k * n, dtype=torch.float64, device="cuda")
+    C = torch.randn(m * n, dtype=torch.float64, device="cuda")
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        lib.dgemm_sub(m, n, k, A.data_ptr(), m, B.data_ptr(), k, C.data_ptr(), m)
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        print(f"dgemm_sub {m}x{n}x{k}: {ms:.3f} ms, {2.0 * m * n * k / ms / 1e9:.2f} TFLOP/s")
+
+
+def case_solve(args) -> None:
+    """One generate + hplb_pdgesv (--n, --nb), with its timing split."""
+    import torch
+
+    from rochpl_b200 import library
+    from rochpl_b200.hpl import Algo, default_ld
+
+    lib = library(0)
+    n, nb = args.n, args.nb
+    ld = default_ld(n)
+    dA = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+    lib.matgen(n, n + 1, 100, dA.data_ptr(), ld, nb)
+    lib.pdgesv(Algo(nb, 32, 2, 2, 2, 1, 0).c(), n, dA.data_ptr(), ld, dX.data_ptr())
+    t = lib.last_timing()
+    res = lib.residual_lcg(n, 100, dX.data_ptr())
+    print(f"solve N={n} NB={nb}: {t['total_ms']:.2f} ms, "
+          f"{hpl_flops(n) / t['total_ms'] / 1e9:.2f} TFLOP/s, trsv {t['trsv_ms']:.3f} ms, "
+          f"resid {res['resid']:.3e}")
+
+
+def case_gemm_lp(args) -> None:
+    """13 x hplb_gemm_lp_sub (FP16), --n x --n x --k, events over the last 10."""
+    import torch
+
+    from rochpl_b200 import library
+
+    lib = library(0)
+    m = n = args.n
+    k = args.k
+    A = (torch.rand(m, k, device="cuda") - 0.5).to(torch.float16)
+    B = (torch.rand(n, k, device="cuda") - 0.5).to(torch.float16)
+    sA = torch.ones((m + 127) // 128, device="cuda")
+    sB = torch.ones((n + 255) // 256, device="cuda")
+    C = torch.zeros(n, m, device="cuda")
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 13
+    for i in range(reps):
+        if i == 3:
+            torch.cuda.synchronize()
+            e0.record()
+        lib.gemm_lp_sub(False, m, n, k, A.data_ptr(), k, B.data_ptr(), k, sA.data_ptr(),
+                        sB.data_ptr(), C.data_ptr(), m)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / (reps - 3)
+    print(f"gemm_lp {m}x{n}x{k}: {ms:.3f} ms, {2.0 * m * n * k / ms / 1e9:.1f} TFLOP/s")
+
+
+def case_getrf(args) -> None:
+    """One hplb_getrf (--n, --nb): the leaves and the panel in context."""
+    import torch
+
+    from rochpl_b200 import library
+    from rochpl_b200.hpl import Algo
+
+    lib = library(0)
+    n, nb = args.n, args.nb
+    A = torch.empty(n * n, dtype=torch.float64, device="cuda")
+    lib.matgen(n, n, 100, A.data_ptr(), n)
+    ip = torch.zeros(n, dtype=torch.int32, device="cuda")
+    lib.getrf(Algo(nb, 32, 2, 2, 2, 1, 0).c(), n, A.data_ptr(), n, ip.data_ptr())
+    t = lib.last_timing()
+    print(f"getrf N={n} NB={nb}: {t['total_ms']:.1f} ms (panels {t['panel_ms']:.1f} ms)")
+
+
+def case_mixed(args) -> None:
+    """hplb_pdgesv_mixed (--n, --prec), with a per-kernel split from the torch
+    profiler's CUDA activity records."""
+    import collections
+
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    from rochpl_b200 import library
+    from rochpl_b200.hpl import Algo
+
+    lib = library(0)
+    n = args.n
+    x = torch.zeros(n, dtype=torch.float64, device="cuda")
+    algo = Algo(args.nb, 32, 2, 2, 2, 1, 0)
+    lib.pdgesv_mixed(algo.c(), n, x.data_ptr(), seed=100, precision=args.prec)
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        r = lib.pdgesv_mixed(algo.c(), n, x.data_ptr(), seed=100, precision=args.prec)
+        torch.cuda.synchronize()
+    print({k: round(v, 2) if isinstance(v, float) else v for k, v in r.items()})
+    agg = collections.defaultdict(lambda: [0.0, 0])
+    for e in prof.events():
+        if e.device_type.name != "CUDA":
+            continue
+        name = e.name.replace("void ", "").replace("hplb::(anonymous namespace)::", "")
+        name = name.split("(")[0][:48]
+        agg[name][0] += (e.time_range.end - e.time_range.start) / 1e3
+        agg[name][1] += 1
+    for name, (ms, cnt) in sorted(agg.items(), key=lambda kv: -kv[1][0])[:24]:
+        print(f"{name:50s} {ms:10.1f} ms {cnt:7d}")
+
+
+def case_batch(args) -> None:
+    """592 systems of one size (--n) with panel width --nb (64: the recursive
+    factorisation) and --nrhs right-hand sides; three launches."""
+    import numpy as np
+    import torch
+
+    from rochpl_b200 import library
+    from rochpl_b200.batch import BatchPlan
+
+    lib = library(0)
+    plan = BatchPlan(lib, np.full(148 * 4, args.n, dtype=np.int32), args.nrhs, [args.nb] * 6)
+    dA = torch.zeros(plan.a_elems, dtype=torch.float64, device="cuda")
+    dB = torch.zeros(plan.b_elems, dtype=torch.float64, device="cuda")
+    dP = torch.zeros(plan.p_elems, dtype=torch.int32, device="cuda")
+    dI = torch.zeros(plan.count, dtype=torch.int32, device="cuda")
+    seeds = np.arange(plan.count, dtype=np.uint64)
+    for _ in range(3):
+        plan.matgen(seeds, dA.data_ptr(), dB.data_ptr())
+        plan.gesv(dA.data_ptr(), dB.data_ptr(), dP.data_ptr(), dI.data_ptr())
+    print(f"batch {plan.count} x N={args.n} NB={int(plan.nb[0])} nrhs={args.nrhs}: "
+          f"{plan.last_ms:.2f} ms, {plan.flops() / plan.last_ms / 1e9:.2f} TFLOP/s")
+    plan.close()
+
+
+CASES = {"dgemm": case_dgemm, "solve": case_solve, "gemm_lp": case_gemm_lp,
+         "getrf": case_getrf, "mixed": case_mixed, "batch": case_batch}
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -558,7 +1020,22 @@ def main():
     ap.add_argument("--n", type=int, default=131072)
     ap.add_argument("--nb", type=int, default=512)
     ap.add_argument("--cpu-n", type=int, default=16384,
-                    help="host sample size for the CPU baseline / reference arm")
+                    help="host sample size for the CPU baseline / reference arm (every step) "
+                         "and of the parity solve")
+    ap.add_argument("--cpu-n-big", type=int, default=32768,
+                    help="reference arm: the larger host sample (once) the N^3 extrapolation "
+                         "starts from")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the LCG, parity-solve and gradient checks")
+    ap.add_argument("--no-c1", action="store_true", help="skip the N = 4096 config line")
+    ap.add_argument("--mixed-sizes", type=lambda v: [int(x) for x in v.split(",") if x],
+                    default=[32768, 65536],
+                    help="further N of the mixed-precision form (comma list; empty to skip)")
+    ap.add_argument("--case", choices=sorted(CASES), default=None,
+                    help="run one small profiling case instead of the benchmark")
+    ap.add_argument("--k", type=int, default=1536, help="--case gemm_lp: reduction size")
+    ap.add_argument("--prec", type=int, default=3, help="--case mixed: precision")
+    ap.add_argument("--nrhs", type=int, default=16, help="--case batch: right-hand sides")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
@@ -572,6 +1049,9 @@ def main():
     ap.add_argument("--gemm-traffic", type=float, default=None,
                     help="DRAM bytes per DGEMM launch from an ncu capture, if known")
     args = ap.parse_args()
+    if args.case:
+        CASES[args.case](args)
+        return 0
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

@@ -5,6 +5,7 @@
  * reference interface it replaces (paths are within the rocHPL tree):
  *
  *   hplb_matgen   <- HPL_pdrandmat / hpl_randmat   src/matgen/HPL_pdrandmat_device.cpp:84-201
+ *   hplb_matgen_block <- the local block of HPL_pdrandmat on a P x Q grid (same lines)
  *   hplb_pdgesv   <- HPL_pdgesv                     include/hpl_pgesv.hpp:162,
  *                                                   src/pgesv/HPL_pdgesv.cpp:19-368
  *   hplb_residual <- the check in HPL_pdtest        src/HPL_pdtest.cpp:307-438
@@ -89,6 +90,20 @@ void      hplb_destroy(hplb_ctx* ctx);
  * parameter.) */
 hplb_status hplb_set_stream(hplb_ctx* ctx, void* stream);
 
+/* Per-context options (no counterpart in the reference).
+ *   HPLB_OPT_LEAF: where the panel leaf keeps the rows of its NBMIN-wide slice
+ *   while it factors it -- HPLB_LEAF_AUTO (default: registers, else shared
+ *   memory, else global memory, the first that holds the slice on the GPU at
+ *   once), HPLB_LEAF_SHARED (shared memory first) or HPLB_LEAF_GLOBAL.  The
+ *   three perform the same operations in the same order and give identical
+ *   results; the choice only moves time.  The rocHPL leaf keeps its slice in
+ *   global memory (src/pfact/HPL_pdpanrlT_device.cpp:23-320). */
+#define HPLB_OPT_LEAF 1
+#define HPLB_LEAF_AUTO 0
+#define HPLB_LEAF_SHARED 1
+#define HPLB_LEAF_GLOBAL 2
+hplb_status hplb_set_option(hplb_ctx* ctx, int option, int value);
+
 const char* hplb_status_string(hplb_status s);
 /* Message of the last failing call on this context (never NULL). */
 const char* hplb_last_error(const hplb_ctx* ctx);
@@ -103,6 +118,16 @@ int64_t hplb_default_ld(int n);
  * nb is accepted for interface parity and does not change the values. */
 hplb_status hplb_matgen(hplb_ctx* ctx, int m, int n, int nb, uint64_t seed,
                         double* dA, int64_t ld);
+
+/* A block of the same LCG matrix: rows [i0, i0 + m) and columns [j0, j0 + n)
+ * of the global mg x ng matrix of `seed`, into the m x n column-major dA
+ * (leading dimension ld >= m).  Local entry (i, j) is the value of state
+ * X(1 + (i0 + i) + (j0 + j) mg), bit-identical to the same entry of
+ * hplb_matgen(mg, ng).  This is the local part a process of a P x Q grid
+ * generates in HPL_pdrandmat (src/matgen/HPL_pdrandmat_device.cpp:136-175,
+ * one block-cyclic block per call here). */
+hplb_status hplb_matgen_block(hplb_ctx* ctx, int64_t mg, int64_t ng, int64_t i0, int64_t j0,
+                              int m, int n, uint64_t seed, double* dA, int64_t ld);
 
 /* HPL_pdgesv at P = Q = 1: LU-factor the n x (n+1) [A|b] in dA (ld >= n) with
  * row partial pivoting and look-ahead depth 1, then back-solve U x = y into
@@ -313,7 +338,13 @@ hplb_status hplb_selftest_wait_timeout(hplb_ctx* ctx, uint64_t budget_ns);
  *   stream : a cudaStream_t (NULL = the default stream); the call waits for it
  *   out    : host results, as hplb_residual_lcg
  * The first call on each device looks up the scratch address on that device
- * (make it with that device current and before any stream capture).  All calls
+ * (make it with that device current and before any stream capture).  That
+ * address is kept for the life of the process and does not survive a
+ * cudaDeviceReset.  Under CUDA's default lazy module loading the library's
+ * device image, array included, is loaded by the first kernel launch or
+ * symbol lookup on a device: make the first call on each device before the
+ * device memory is handed to the caller's own pool, or run with
+ * CUDA_MODULE_LOADING=EAGER so the image loads when the context is made.  All calls
  * on a device share the one scratch array: calls that overlap on the GPU (two
  * host threads, or two streams) race and must be serialised by the caller. */
 hplb_status hplb_residual_lcg_noalloc(int n, uint64_t seed, const double* dX, void* stream,

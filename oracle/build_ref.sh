@@ -4,8 +4,14 @@
 # Only matgen, pivot bookkeeping and the single-process row swap are built:
 # the LU itself needs rocBLAS, MPI and HIP cooperative launches, so it is
 # not buildable here.  Test infrastructure only.
+#
+#   oracle/build_ref.sh [REFERENCE_TREE]
+#
+# REFERENCE_TREE is the rocHPL checkout (the directory holding src/ and
+# include/): the first argument, else $HPLB_REFERENCE, else /root/reference,
+# where the build container mounts it.  Without it nothing is built.
 set -euo pipefail
-REF=${HPLB_REFERENCE:-/root/reference}
+REF=${1:-${HPLB_REFERENCE:-/root/reference}}
 HERE=$(cd "$(dirname "$0")" && pwd)
 OUT="$HERE/_ref"
 if [ ! -d "$REF/src" ]; then

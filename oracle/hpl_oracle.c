@@ -94,6 +94,25 @@ void hplo_matgen(int M, int N, uint64_t seed, double* A, int64_t ld) {
   }
 }
 
+/* Rows [i0, i0 + m) x columns [j0, j0 + n) of the M-row matrix of hplo_matgen:
+ * the local block a process of a P x Q grid generates in HPL_pdrandmat
+ * (src/matgen/HPL_pdrandmat_device.cpp:136-175), entry (i, j) being state
+ * X(1 + (i0 + i) + (j0 + j) M). */
+void hplo_matgen_block(int64_t M, int64_t i0, int64_t j0, int m, int n, uint64_t seed,
+                       double* A, int64_t ld) {
+  uint64_t ac, cc; /* one column */
+  hplo_jump((uint64_t)M, &ac, &cc);
+  uint64_t col = hplo_lcg_state(seed, M, i0, j0);
+  for(int j = 0; j < n; ++j) {
+    uint64_t r = col;
+    for(int i = 0; i < m; ++i) {
+      A_(i, j) = hplo_lcg_value(r);
+      r        = HPLO_MULT * r + HPLO_IADD;
+    }
+    col = ac * col + cc;
+  }
+}
+
 /* FNV-1a over the bit patterns of the M x N block, column by column: a cheap
  * fingerprint for the golden files. */
 uint64_t hplo_hash(int M, int N, const double* A, int64_t ld) {

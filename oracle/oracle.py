@@ -41,6 +41,8 @@ def lib():
         L.hplo_lcg_state.argtypes = [C.c_uint64, C.c_int64, C.c_int64, C.c_int64]
         L.hplo_lcg_state.restype = C.c_uint64
         L.hplo_matgen.argtypes = [C.c_int, C.c_int, C.c_uint64, C.c_void_p, C.c_int64]
+        L.hplo_matgen_block.argtypes = [C.c_int64, C.c_int64, C.c_int64, C.c_int, C.c_int,
+                                        C.c_uint64, C.c_void_p, C.c_int64]
         L.hplo_hash.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int64]
         L.hplo_hash.restype = C.c_uint64
         L.hplo_use_blas.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
@@ -63,6 +65,9 @@ def ref():
         R = C.CDLL(REF_PATH)
         R.ref_pdrandmat.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int]
         R.ref_pdrandmat.restype = C.c_int
+        R.ref_pdrandmat_grid.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                         C.c_int, C.c_int, C.c_int, C.c_int]
+        R.ref_pdrandmat_grid.restype = C.c_int
         R.ref_xjumpm.argtypes = [C.c_int, C.c_uint64, C.c_uint64, C.c_uint64,
                                  C.POINTER(C.c_uint64), C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
         R.ref_pipid.argtypes = [C.c_int, C.c_int, C.c_void_p, C.POINTER(C.c_int), C.c_void_p]
@@ -98,6 +103,14 @@ def matgen(m: int, n: int, seed: int = 100, ld: int | None = None) -> np.ndarray
     A = np.zeros((ld, n), dtype=np.float64, order="F")
     lib().hplo_matgen(m, n, seed, A.ctypes.data, ld)
     return A
+
+
+def matgen_block(M: int, i0: int, j0: int, m: int, n: int, seed: int = 100) -> np.ndarray:
+    """Rows [i0, i0+m) x columns [j0, j0+n) of the M-row LCG matrix (m x n,
+    Fortran order)."""
+    A = np.zeros((max(m, 1), max(n, 1)), dtype=np.float64, order="F")
+    lib().hplo_matgen_block(M, i0, j0, m, n, seed, A.ctypes.data, max(m, 1))
+    return A[:m, :n]
 
 
 def hash_block(A: np.ndarray, m: int, n: int) -> int:

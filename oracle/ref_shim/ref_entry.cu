@@ -23,6 +23,16 @@ int ref_pdrandmat(int M, int N, int NB, double* dA, int lda, int iseed) {
   return (int)cudaDeviceSynchronize();
 }
 
+/* The local part of process (myrow, mycol) of an nprow x npcol grid, as
+ * HPL_pdrandmat generates it (NB x NB block-cyclic, starting in process (0,0)):
+ * LocP(M) rows and LocQ(N) columns into dA (leading dimension lda). */
+int ref_pdrandmat_grid(int M, int N, int NB, double* dA, int lda, int iseed, int nprow,
+                       int npcol, int myrow, int mycol) {
+  HPL_T_grid g{nprow, npcol, myrow, mycol};
+  HPL_pdrandmat(&g, M, N, NB, dA, lda, iseed);
+  return (int)cudaDeviceSynchronize();
+}
+
 /* HPL_xjumpm: constants to jump JUMPM steps from IRANN. */
 void ref_xjumpm(int jumpm, uint64_t mult, uint64_t iadd, uint64_t irann,
                 uint64_t* iranm, uint64_t* iam, uint64_t* icm) {

@@ -55,6 +55,7 @@ struct hplb_ctx {
   double* r_ws   = nullptr;  size_t r_ws_cap   = 0;  // block copies and inverses
   int*    r_perm = nullptr;  size_t r_perm_cap = 0;  // one panel's row map
 
+  int          leaf_kind = HPLB_LEAF_AUTO;  // hplb_set_option(HPLB_OPT_LEAF)
   cudaStream_t caller   = nullptr;  // hplb_set_stream (null: the legacy default stream)
   cudaEvent_t  ev_enter = nullptr;  // recorded on `caller` at every entry
 

@@ -202,11 +202,7 @@ static cudaError_t launch_dgemm_any(int m, int n, int k, const double* A, int64_
                                     const double* B, int64_t ldb, double* C, int64_t ldc,
                                     int* status, bool accumulate, cudaStream_t stream) {
   if(m <= 0 || n <= 0) return cudaSuccess;
-  static const int path = [] {
-    const char* e = getenv("HPLB_DGEMM_PATH");
-    return (e && strcmp(e, "cpasync") == 0) ? 1 : 0;
-  }();
-  if(k > 0 && status && path == 0 && dgemm_tma_eligible(m, n, k, A, lda, B, ldb)) {
+  if(k > 0 && status && dgemm_tma_eligible(m, n, k, A, lda, B, ldb)) {
     cudaError_t e = launch_dgemm_tma(m, n, k, A, lda, B, ldb, C, ldc, status, accumulate, stream);
     if(e == cudaSuccess) return e;
     cudaGetLastError();  // fall back to the cp.async kernel

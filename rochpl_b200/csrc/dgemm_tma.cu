@@ -321,14 +321,8 @@ bool get_encoder() {
 // the SMs, and the trailing update's CTAs retire every tile, so the
 // high-priority panel kernels (the critical path once the trailing matrix is
 // small) wait less for SMs.  Measured at N = 16384 (getrf, NB = 512, B200):
-// 251 ms with four, 208 ms with one, identical bits.  HPLB_DGEMM_TPC = 1, 2
-// or 4 fixes the choice.
+// 251 ms with four, 208 ms with one, identical bits.
 int tiles_per_cta(long long ntiles) {
-  static const int forced = [] {
-    const char* e = getenv("HPLB_DGEMM_TPC");
-    const int   v = e ? atoi(e) : 0;
-    return (v == 1 || v == 2 || v == 4) ? v : 0;
-  }();
   static const int sms = [] {
     int dev = 0, n = 148;
     if(cudaGetDevice(&dev) != cudaSuccess ||
@@ -338,7 +332,6 @@ int tiles_per_cta(long long ntiles) {
     }
     return n;
   }();
-  if(forced) return forced;
   return ntiles >= 256LL * sms ? 4 : 1;
 }
 

@@ -383,11 +383,7 @@ cudaError_t launch_gemm_lp(bool bf16, int m, int n, int k, const void* A16, int6
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if(sms < 1) sms = 1;
   }
-  static const int tmax = [] {
-    const char* e = getenv("HPLB_LP_TPC");
-    const int   v = e ? atoi(e) : 8;
-    return v < 1 ? 8 : v;
-  }();
+  constexpr int tmax = 8;  // tiles per CTA at most
   const long long waves = (ntiles + (long long)sms * tmax - 1) / ((long long)sms * tmax);
   const int tpc = (int)((ntiles + (long long)sms * waves - 1) / ((long long)sms * waves));
   const long long grid = (ntiles + tpc - 1) / tpc;

@@ -28,16 +28,6 @@ using namespace hplb;
 
 namespace {
 
-// U12 = L11^-1 (P A12) as a DMMA GEMM (default), or by the blocked
-// substitution kernel (HPLB_TRSM_PATH=substitution, kept for comparison).
-bool trsm_by_inverse() {
-  static const bool inv = [] {
-    const char* e = getenv("HPLB_TRSM_PATH");
-    return !(e && strcmp(e, "substitution") == 0);
-  }();
-  return inv;
-}
-
 hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
   hplb_status s;
   if((s = grow(ctx, &ctx->d_ipiv, &ctx->ipiv_cap, (size_t)std::max(n, 1))) != HPLB_OK) return s;
@@ -67,7 +57,7 @@ hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
     }
     ctx->nb_cap = nb;
   }
-  if(n > 0 && trsm_by_inverse() &&
+  if(n > 0 &&
      (s = grow(ctx, &ctx->d_w, &ctx->w_cap, (size_t)nb * (size_t)(n + 1))) != HPLB_OK)
     return s;
   return ensure_leaf_ws(ctx, n, nbmin);
@@ -90,7 +80,7 @@ struct Solve {
     hplb_ctx* ctx  = this->ctx;
     const int grid = leaf_grid_size(ctx->num_sms, n - r0);
     CK(launch_leaf(A, ld, r0, n, c0, w, ctx->d_ipiv, ctx->d_cand, ctx->d_cur, ctx->d_bar,
-                   ctx->d_status, grid, ctx->s_pan));
+                   ctx->d_status, grid, ctx->leaf_kind, ctx->s_pan));
     CK(launch_panel_swap(A, ld, ctx->d_ipiv, r0, c0, w, pc, pw, ctx->s_pan));
     ctx->launches += 2;
     return HPLB_OK;
@@ -155,11 +145,9 @@ struct Solve {
     CK(launch_perm(ctx->d_ipiv + j, j, jb, ctx->d_perm[set], ctx->s_pan));
     CK(launch_diag_inv(A, ld, j, j, jb, ctx->d_dinv[set], ctx->s_pan));
     ctx->launches += 2;
-    if(trsm_by_inverse()) {
-      CK(launch_unit_lower_inverse(a(j, j), ld, jb, ctx->d_dinv[set], ctx->d_linv[set], jb,
-                                   ctx->s_pan));
-      ctx->launches += 2;
-    }
+    CK(launch_unit_lower_inverse(a(j, j), ld, jb, ctx->d_dinv[set], ctx->d_linv[set], jb,
+                                 ctx->s_pan));
+    ctx->launches += 2;
     CK(cudaEventRecord(e1, ctx->s_pan));
     CK(cudaEventRecord(done, ctx->s_pan));
     panel_ev.emplace_back(e0, e1);
@@ -171,17 +159,12 @@ struct Solve {
     hplb_ctx* ctx = this->ctx;
     if(w <= 0) return HPLB_OK;
     const int jb = std::min(algo->nb, n - j);
-    if(trsm_by_inverse()) {
-      // Interchanges into W, then U12 = L11^-1 W straight into the top rows.
-      CK(launch_laswp_gather(A, ld, j, jb, ctx->d_perm[set], ctx->d_w, jb, c, w, ctx->s_upd));
-      CK(launch_dgemm_set(jb, w, jb, ctx->d_linv[set], jb, ctx->d_w, jb, a(j, c), ld,
-                          ctx->d_status, ctx->s_upd));
-      ctx->launches += 2;
-    } else {
-      CK(launch_laswp_trsm(A, ld, j, jb, j, ctx->d_perm[set], ctx->d_dinv[set], c, w,
-                           ctx->s_upd));
-      ctx->launches += 1;
-    }
+    // Interchanges into W, then U12 = L11^-1 W straight into the top rows
+    // (rocHPL: HPL_dlaswp00N + rocblas_dtrsm, src/pgesv/HPL_pdupdateTT.cpp:95-106).
+    CK(launch_laswp_gather(A, ld, j, jb, ctx->d_perm[set], ctx->d_w, jb, c, w, ctx->s_upd));
+    CK(launch_dgemm_set(jb, w, jb, ctx->d_linv[set], jb, ctx->d_w, jb, a(j, c), ld,
+                        ctx->d_status, ctx->s_upd));
+    ctx->launches += 2;
     const int m = n - (j + jb);
     if(m > 0) {
       cudaEvent_t e0 = next_event(ctx), e1 = next_event(ctx);
@@ -215,6 +198,18 @@ const char* hplb_status_string(hplb_status s) {
 }
 
 const char* hplb_last_error(const hplb_ctx* ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+hplb_status hplb_set_option(hplb_ctx* ctx, int option, int value) {
+  if(!ctx) return HPLB_ERR_ARG;
+  switch(option) {
+    case HPLB_OPT_LEAF:
+      if(value < HPLB_LEAF_AUTO || value > HPLB_LEAF_GLOBAL)
+        return set_err(ctx, HPLB_ERR_ARG, "hplb_set_option: leaf kind %d out of range", value);
+      ctx->leaf_kind = value;
+      return HPLB_OK;
+  }
+  return set_err(ctx, HPLB_ERR_ARG, "hplb_set_option: unknown option %d", option);
+}
 
 hplb_status hplb_set_stream(hplb_ctx* ctx, void* stream) {
   if(!ctx) return HPLB_ERR_ARG;
@@ -287,6 +282,20 @@ hplb_status hplb_matgen(hplb_ctx* ctx, int m, int n, int nb, uint64_t seed, doub
   if(m > 0 && n > 0 && !dA) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen: null matrix");
   ENTER(ctx);
   CK(launch_matgen(m, n, seed, dA, ld, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return HPLB_OK;
+}
+
+hplb_status hplb_matgen_block(hplb_ctx* ctx, int64_t mg, int64_t ng, int64_t i0, int64_t j0,
+                              int m, int n, uint64_t seed, double* dA, int64_t ld) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(m < 0 || n < 0 || mg < 0 || ng < 0 || i0 < 0 || j0 < 0 || i0 + m > mg || j0 + n > ng)
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen_block: block outside the %lld x %lld matrix",
+                   (long long)mg, (long long)ng);
+  if(ld < std::max(1, m)) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen_block: ld < max(1,m)");
+  if(m > 0 && n > 0 && !dA) return set_err(ctx, HPLB_ERR_ARG, "hplb_matgen_block: null matrix");
+  ENTER(ctx);
+  CK(launch_matgen_block(mg, i0, j0, m, n, seed, dA, ld, ctx->s_upd));
   CK(cudaStreamSynchronize(ctx->s_upd));
   return HPLB_OK;
 }

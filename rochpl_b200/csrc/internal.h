@@ -10,6 +10,9 @@ constexpr int kMaxLeaf = 128;  // widest leaf (NBMIN) the leaf kernel holds
 
 cudaError_t launch_matgen(int m, int n, uint64_t seed, double* A, int64_t ld,
                           cudaStream_t stream);
+// Rows [i0, i0 + m) x columns [j0, j0 + n) of the global mg-row LCG matrix.
+cudaError_t launch_matgen_block(int64_t mg, int64_t i0, int64_t j0, int m, int n, uint64_t seed,
+                                double* A, int64_t ld, cudaStream_t stream);
 
 // C -= A B.  Uses the TMA-fed warp-specialised kernel when the operands
 // qualify (dgemm_tma_eligible), the cp.async kernel otherwise.  status may be
@@ -33,10 +36,13 @@ cudaError_t launch_dgemm_cpasync(int m, int n, int k, const double* A, int64_t l
 int         leaf_grid_size(int num_sms, int rows);
 // The panel kernels exist for double (the FP64 solve) and float (the FP32
 // panel of the mixed-precision solve).
+// leaf_kind: where the leaf's rows live, HPLB_LEAF_* of include/hplb.h
+// (auto = registers, then shared memory, then global memory, the first that
+// holds the leaf; a forced kind falls through the same way when it does not).
 template <typename T>
 cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
                         double* cand, double* cur, int* bar, int* status, int grid,
-                        cudaStream_t stream);
+                        int leaf_kind, cudaStream_t stream);
 template <typename T>
 cudaError_t launch_panel_swap(T* A, int64_t ld, const int* ipiv, int r0, int c0, int w, int pc,
                               int pw, cudaStream_t stream);

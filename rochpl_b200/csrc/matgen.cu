@@ -26,10 +26,12 @@ struct MatgenTables {
   Jump step32;    // jump by 32
 };
 
+// Block (gi0, gj0) .. (gi0 + m, gj0 + n) of the global matrix with mg rows:
+// local entry (i, j) is global entry (gi0 + i, gj0 + j).
 template <typename T>
 __global__ void __launch_bounds__(kWarps * 32)
-matgen_kernel(int m, int n, int64_t ld, T* __restrict__ A, uint64_t x1,
-              MatgenTables Tab) {
+matgen_kernel(int m, int n, int64_t ld, T* __restrict__ A, uint64_t x1, uint64_t mg,
+              uint64_t gi0, uint64_t gj0, MatgenTables Tab) {
   __shared__ Jump s_pow2[64];
   __shared__ Jump s_lane[32];
   for(int i = threadIdx.x; i < 64; i += blockDim.x) s_pow2[i] = Tab.pow2[i];
@@ -43,10 +45,11 @@ matgen_kernel(int m, int n, int64_t ld, T* __restrict__ A, uint64_t x1,
   const int     j  = (int)(wg / runs);
   const int     i0 = (int)(wg % runs) * kRun;
 
-  // State of (i0, j): X(1 + i0 + j m) = jump(i0 + j m) applied to X(1).
+  // State of global (gi0 + i0, gj0 + j): X(1 + gi0 + i0 + (gj0 + j) mg), the
+  // jump by gi0 + i0 + (gj0 + j) mg (mod 2^64) applied to X(1).
   uint64_t s = 0;
   if(lane == 0) {
-    uint64_t k   = (uint64_t)i0 + (uint64_t)j * (uint64_t)m;
+    uint64_t k   = gi0 + (uint64_t)i0 + (gj0 + (uint64_t)j) * mg;
     Jump     acc = {1, 0};
     for(int b = 0; k; ++b, k >>= 1)
       if(k & 1) acc = compose(acc, s_pow2[b]);
@@ -75,8 +78,8 @@ matgen_kernel(int m, int n, int64_t ld, T* __restrict__ A, uint64_t x1,
 }  // namespace
 
 template <typename E>
-static cudaError_t matgen_any(int m, int n, uint64_t seed, E* A, int64_t ld,
-                              cudaStream_t stream) {
+static cudaError_t matgen_any(int m, int n, uint64_t seed, E* A, int64_t ld, int64_t mg,
+                              int64_t gi0, int64_t gj0, cudaStream_t stream) {
   if(m <= 0 || n <= 0) return cudaSuccess;
   MatgenTables T;
   Jump p{kLcgMult, kLcgAdd};
@@ -90,19 +93,25 @@ static cudaError_t matgen_any(int m, int n, uint64_t seed, E* A, int64_t ld,
   const int64_t runs  = (m + kRun - 1) / kRun;
   const int64_t warps = runs * (int64_t)n;
   const int64_t grid  = (warps + kWarps - 1) / kWarps;
-  matgen_kernel<E><<<(unsigned)grid, kWarps * 32, 0, stream>>>(m, n, ld, A, x1, T);
+  matgen_kernel<E><<<(unsigned)grid, kWarps * 32, 0, stream>>>(
+      m, n, ld, A, x1, (uint64_t)mg, (uint64_t)gi0, (uint64_t)gj0, T);
   return cudaGetLastError();
 }
 
 cudaError_t launch_matgen(int m, int n, uint64_t seed, double* A, int64_t ld,
                           cudaStream_t stream) {
-  return matgen_any<double>(m, n, seed, A, ld, stream);
+  return matgen_any<double>(m, n, seed, A, ld, m, 0, 0, stream);
+}
+
+cudaError_t launch_matgen_block(int64_t mg, int64_t i0, int64_t j0, int m, int n, uint64_t seed,
+                                double* A, int64_t ld, cudaStream_t stream) {
+  return matgen_any<double>(m, n, seed, A, ld, mg, i0, j0, stream);
 }
 
 // The same matrix rounded to FP32 (the working copy of the mixed-precision solve).
 cudaError_t launch_matgen_f32(int m, int n, uint64_t seed, float* W, int64_t ld,
                               cudaStream_t stream) {
-  return matgen_any<float>(m, n, seed, W, ld, stream);
+  return matgen_any<float>(m, n, seed, W, ld, m, 0, 0, stream);
 }
 
 }  // namespace hplb

@@ -24,16 +24,6 @@ using namespace hplb;
 
 namespace {
 
-// U12 = L11^-1 G by the FP32 SIMT GEMM instead of the tensor cores in the x3
-// modes (HPLB_MIXED_U12=simt, kept for comparison).
-bool u12_simt() {
-  static const bool v = [] {
-    const char* e = getenv("HPLB_MIXED_U12");
-    return e && strcmp(e, "simt") == 0;
-  }();
-  return v;
-}
-
 struct Mixed {
   hplb_ctx*        ctx;
   const hplb_algo* algo;
@@ -58,7 +48,7 @@ struct Mixed {
     hplb_ctx* ctx  = this->ctx;
     const int grid = leaf_grid_size(ctx->num_sms, n - r0);
     CK(launch_leaf<float>(W, ldw, r0, n, c0, wdt, ctx->d_ipiv, ctx->d_cand, ctx->d_cur,
-                          ctx->d_bar, ctx->d_status, grid, st));
+                          ctx->d_bar, ctx->d_status, grid, ctx->leaf_kind, st));
     CK(launch_panel_swap<float>(W, ldw, ctx->d_ipiv, r0, c0, wdt, pc, pw, st));
     ctx->launches += 2;
     return HPLB_OK;
@@ -142,7 +132,7 @@ struct Mixed {
     float*       sL = ctx->m_scale;
     float*       sU = ctx->m_scale + ((size_t)n + 127) / 128 + 1;
     CK(launch_laswp_gather<float>(W, ldw, j, jb, perm(p), ctx->m_g, jb, c, wd, su));
-    if(split && !u12_simt()) {
+    if(split) {
       // U12 = L11^-1 G on the tensor cores, with the split operands of the
       // trailing update (FP32-accurate): C = 0, then C -= (-L11^-1) G.
       float* sLi = sU + ((size_t)n + 255) / 256 + 1;

@@ -750,19 +750,6 @@ static int leaf_smem_budget() {
   return budget;
 }
 
-// Leaf kernel choice: registers (default), "smem" or "global" (HPLB_LEAF), the
-// latter two kept for comparison; each falls through to the next when the
-// leaf does not fit.
-static int leaf_mode() {
-  static const int mode = [] {
-    const char* e = getenv("HPLB_LEAF");
-    if(e && strcmp(e, "global") == 0) return 2;
-    if(e && strcmp(e, "smem") == 0) return 1;
-    return 0;
-  }();
-  return mode;
-}
-
 template <typename T, int RPT>
 static cudaError_t launch_leaf_reg(LeafParams<T> P, int g, cudaStream_t stream) {
   P.rpb         = RPT * kRegLeafThreads;
@@ -781,14 +768,7 @@ static cudaError_t try_leaf_reg(const LeafParams<T>& P, int rows, int sms, int g
                                 cudaStream_t stream, bool* done) {
   constexpr int kMaxRpt = sizeof(T) == 8 ? 3 : 4;
   *done                 = false;
-  // HPLB_LEAF_RPT=k starts the search at k rows per thread (fewer, fuller
-  // blocks: a smaller gang to co-schedule beside the trailing update).
-  static const int first = [] {
-    const char* e = getenv("HPLB_LEAF_RPT");
-    const int   v = e ? atoi(e) : 1;
-    return v < 1 ? 1 : v;
-  }();
-  for(int rpt = std::min(first, kMaxRpt); rpt <= kMaxRpt; ++rpt) {
+  for(int rpt = 1; rpt <= kMaxRpt; ++rpt) {
     const int cap = rpt * kRegLeafThreads;
     const int g   = (rows + cap - 1) / cap;
     if(g > sms || g > grid) continue;
@@ -806,12 +786,14 @@ static cudaError_t try_leaf_reg(const LeafParams<T>& P, int rows, int sms, int g
 template <typename T>
 cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
                         double* cand, double* cur, int* bar, int* status, int grid,
-                        cudaStream_t stream) {
+                        int leaf_kind, cudaStream_t stream) {
+  // 0: registers first; 1: shared memory first; 2: global memory.
+  const int mode = leaf_kind == HPLB_LEAF_SHARED ? 1 : (leaf_kind == HPLB_LEAF_GLOBAL ? 2 : 0);
   const int rows = end - r0;
   int       dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  if(w <= kRegLeafW && rows > 0 && leaf_mode() == 0) {
+  if(w <= kRegLeafW && rows > 0 && mode == 0) {
     LeafParams<T> P;
     P.A      = A;
     P.ld     = ld;
@@ -831,7 +813,7 @@ cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* i
   }
   // Resident-slice leaf: as few blocks as hold the leaf in shared memory (one
   // per SM at most).
-  if(w <= kSmemLeafW && rows > 0 && leaf_mode() <= 1) {
+  if(w <= kSmemLeafW && rows > 0 && mode <= 1) {
     const int budget = leaf_smem_budget<T>();
     const int rmax   = budget / (w * (int)sizeof(T));
     if(rmax >= 32) {
@@ -974,7 +956,7 @@ cudaError_t launch_laswp_gather(T* A, int64_t ld, int ia, int jb, const int* per
 
 #define HPLB_PANEL_INSTANTIATE(T)                                                              \
   template cudaError_t launch_leaf<T>(T*, int64_t, int, int, int, int, int*, double*, double*, \
-                                      int*, int*, int, cudaStream_t);                          \
+                                      int*, int*, int, int, cudaStream_t);                     \
   template cudaError_t launch_panel_swap<T>(T*, int64_t, const int*, int, int, int, int, int,  \
                                             cudaStream_t);                                     \
   template cudaError_t launch_diag_inv<T>(const T*, int64_t, int, int, int, T*, cudaStream_t); \

@@ -23,11 +23,11 @@ HPLB_ERR_UNSUPPORTED = 6
 # Every symbol include/hplb.h declares (checked by the CPU test suite).
 EXPORTS = [
     "hplb_create", "hplb_destroy", "hplb_status_string", "hplb_last_error",
-    "hplb_default_ld", "hplb_matgen", "hplb_pdgesv", "hplb_residual",
+    "hplb_default_ld", "hplb_matgen", "hplb_matgen_block", "hplb_pdgesv", "hplb_residual",
     "hplb_residual_lcg", "hplb_last_timing", "hplb_last_steps", "hplb_dgemm_sub", "hplb_laswp_trsm",
     "hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_residual_lcg_noalloc",
     "hplb_gemm_lp_sub", "hplb_pdgesv_mixed", "hplb_getrf", "hplb_getrs", "hplb_rank_k",
-    "hplb_set_stream", "hplb_batch_create", "hplb_batch_destroy", "hplb_batch_layout",
+    "hplb_set_stream", "hplb_set_option", "hplb_batch_create", "hplb_batch_destroy", "hplb_batch_layout",
     "hplb_batch_matgen", "hplb_batch_gesv", "hplb_batch_getrs", "hplb_batch_rank_k",
     "hplb_batch_residual", "hplb_batch_last_ms", "hplb_batch_tune",
 ]
@@ -69,6 +69,10 @@ class hplb_mixed_report(C.Structure):
 # hplb_mixed_opts.precision values
 PREC_BF16, PREC_FP16, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2, 3
 
+# hplb_set_option options and values
+HPLB_OPT_LEAF = 1
+LEAF_AUTO, LEAF_SHARED, LEAF_GLOBAL = 0, 1, 2
+
 
 class HplError(RuntimeError):
     def __init__(self, status: int, message: str):
@@ -100,6 +104,8 @@ def load() -> C.CDLL:
     L.hplb_default_ld.argtypes = [i32]
     L.hplb_default_ld.restype = i64
     L.hplb_matgen.argtypes = [vp, i32, i32, i32, u64, vp, i64]
+    L.hplb_matgen_block.argtypes = [vp, i64, i64, i64, i64, i32, i32, u64, vp, i64]
+    L.hplb_matgen_block.restype = i32
     L.hplb_pdgesv.argtypes = [vp, C.POINTER(hplb_algo), i32, vp, i64, vp, vp, C.POINTER(C.c_int)]
     L.hplb_residual.argtypes = [vp, i32, vp, i64, vp, C.POINTER(hplb_resid)]
     L.hplb_residual_lcg.argtypes = [vp, i32, u64, vp, C.POINTER(hplb_resid)]
@@ -136,6 +142,8 @@ def load() -> C.CDLL:
         getattr(L, name).restype = i32
     L.hplb_set_stream.argtypes = [vp, vp]
     L.hplb_set_stream.restype = i32
+    L.hplb_set_option.argtypes = [vp, i32, i32]
+    L.hplb_set_option.restype = i32
     L.hplb_getrf.argtypes = [vp, C.POINTER(hplb_algo), i32, vp, i64, vp, C.POINTER(C.c_int)]
     L.hplb_getrf.restype = i32
     L.hplb_getrs.argtypes = [vp, i32, i32, i32, i32, vp, i64, vp, vp, i64]
@@ -180,6 +188,11 @@ class Library:
     def matgen(self, m: int, n: int, seed: int, A: int, ld: int, nb: int = 0):
         self._check(self.L.hplb_matgen(self.ctx, m, n, nb, seed, A, ld))
 
+    def matgen_block(self, mg: int, ng: int, i0: int, j0: int, m: int, n: int, seed: int,
+                     A: int, ld: int):
+        """Rows [i0, i0+m) x columns [j0, j0+n) of the mg x ng LCG matrix."""
+        self._check(self.L.hplb_matgen_block(self.ctx, mg, ng, i0, j0, m, n, seed, A, ld))
+
     def pdgesv(self, algo: hplb_algo, n: int, A: int, ld: int, X: int, ipiv: int | None = None):
         info = C.c_int(0)
         st = self.L.hplb_pdgesv(self.ctx, C.byref(algo), n, A, ld, X, ipiv or None,
@@ -208,6 +221,10 @@ class Library:
         """Order later calls after the work queued on `stream` (a raw
         cudaStream_t, e.g. torch.cuda.current_stream().cuda_stream)."""
         self._check(self.L.hplb_set_stream(self.ctx, stream or None))
+
+    def set_leaf(self, kind: int):
+        """hplb_set_option(HPLB_OPT_LEAF): LEAF_AUTO, LEAF_SHARED or LEAF_GLOBAL."""
+        self._check(self.L.hplb_set_option(self.ctx, HPLB_OPT_LEAF, int(kind)))
 
     def getrf(self, algo: hplb_algo, n: int, A: int, ld: int, ipiv: int | None = None) -> int:
         """hplb_getrf: factor A alone; returns info (0, or the first zero pivot)."""

@@ -8,6 +8,9 @@ oracle/build_ref.sh into oracle/_ref/libhplref.so:
                        (needs a GPU: run as `python tests/golden/make_golden.py --lcg`
                        on the GPU box, copy the json back).
   jump_golden.json  -- HPL_xjumpm constants (host code).
+  lcg_c2_golden.json -- the same generator for four blocks of the N = 131072
+                       [A|b] (first, middle and last 512-column blocks and b),
+                       state indices up to 1.7e10 (GPU: `--lcg-c2`).
   perm_golden.json  -- HPL_pipid + the permU unrolling of HPL_pdpanel_swapids
                        for seeded random pivot vectors (host code).
 
@@ -59,6 +62,49 @@ def make_lcg(outdir: str) -> None:
         json.dump(out, f, indent=1)
 
 
+# Blocks of the N = 131072 [A|b] (NB = 512) whose LCG state indices i + j N
+# run up to 1.7e10, far past 2^32: as the local columns of processes of a
+# 1 x 256 grid, where process q owns column block q and process 0 also owns
+# block 256 (the single column b).
+C2_N, C2_NB, C2_Q = 131072, 512, 256
+C2_BLOCKS = [("first column block", 0, 0, 0, 512), ("column b", 0, 512, 131072, 1),
+             ("middle column block", 128, 0, 65536, 512),
+             ("last column block", 255, 0, 130560, 512)]
+
+
+def make_lcg_c2(outdir: str) -> None:
+    """The reference's own generator (HPL_pdrandmat on a CUDA device) for the
+    N = 131072 blocks above: FNV-1a hash plus sampled entries of each."""
+    import torch
+
+    R = O.ref()
+    assert R is not None, "oracle/_ref/libhplref.so not built"
+    rng = np.random.default_rng(131072)
+    n_cols = C2_N + 1
+    out = {"n": C2_N, "nb": C2_NB, "seed": 100, "q": C2_Q, "blocks": []}
+    local = {}
+    for mycol in sorted({b[1] for b in C2_BLOCKS}):
+        nq = 513 if mycol == 0 else 512
+        dA = torch.zeros(C2_N * nq, dtype=torch.float64, device="cuda")
+        rc = R.ref_pdrandmat_grid(C2_N, n_cols, C2_NB, dA.data_ptr(), C2_N, 100, 1, C2_Q, 0,
+                                  mycol)
+        assert rc == 0, rc
+        local[mycol] = np.asfortranarray(dA.view(nq, C2_N).T.cpu().numpy())
+        del dA
+    for name, mycol, lc0, gc0, w in C2_BLOCKS:
+        A = np.asfortranarray(local[mycol][:, lc0:lc0 + w])
+        h = O.hash_block(A, C2_N, w)
+        ii = rng.integers(0, C2_N, 24)
+        jj = rng.integers(0, w, 24)
+        samples = [[int(i), int(gc0 + j), A[i, j].hex()] for i, j in zip(ii, jj)]
+        samples += [[C2_N - 1, gc0 + w - 1, A[C2_N - 1, w - 1].hex()]]
+        out["blocks"].append({"name": name, "col0": gc0, "ncols": w, "fnv1a": f"{h:016x}",
+                              "samples": samples})
+        print(name, gc0, w, f"{h:016x}")
+    with open(os.path.join(outdir, "lcg_c2_golden.json"), "w") as f:
+        json.dump(out, f, indent=1)
+
+
 def make_jump(outdir: str) -> None:
     R = O.ref()
     out = []
@@ -92,8 +138,13 @@ def make_perm(outdir: str) -> None:
 if __name__ == "__main__":
     ap = argparse.ArgumentParser()
     ap.add_argument("--lcg", action="store_true", help="also run the reference LCG on a GPU")
+    ap.add_argument("--lcg-c2", action="store_true",
+                    help="only the N = 131072 blocks of the reference LCG (needs a GPU)")
     ap.add_argument("--out", default=HERE)
     a = ap.parse_args()
+    if a.lcg_c2:
+        make_lcg_c2(a.out)
+        sys.exit(0)
     make_jump(a.out)
     make_perm(a.out)
     if a.lcg:

@@ -168,6 +168,62 @@ def test_hpl_solve_central_finite_differences(hlib, oracle):
     assert abs(float((tB.grad * dB).sum()) - fdB) <= 1e-6 * max(1.0, abs(fdB))
 
 
+def test_hpl_solve_gradients_at_n16384_with_32_rhs(hlib):
+    """The differentiable solve at its own config size (N = 16384, 32 RHS, the
+    HPL LCG system of seed 100): X, Abar and Bbar against an FP64 reference
+    from torch's dense solve within 64 N eps kappa_oo, and directional
+    derivatives along unit-norm directions against central differences with
+    step 1e-6 (relative tolerance 1e-4)."""
+    import torch
+
+    from rochpl_b200.autograd import hpl_solve
+
+    n, nrhs = 16384, 32
+    M = torch.empty((n + nrhs) * n, dtype=torch.float64, device="cuda")
+    hlib.matgen(n, n + nrhs, 100, M.data_ptr(), n)
+    Mc = M.view(n + nrhs, n)
+    A = Mc[:n].t().contiguous().requires_grad_(True)
+    B = Mc[n:].t().contiguous().requires_grad_(True)
+    del M, Mc
+    g = torch.Generator(device="cuda").manual_seed(7)
+    Xbar = torch.randn(n, nrhs, generator=g, dtype=torch.float64, device="cuda")
+    X = hpl_solve(A, B, nb=512)
+    X.backward(Xbar)
+    with torch.no_grad():
+        Xr = torch.linalg.solve(A, B)
+        Bbar = torch.linalg.solve(A.t(), Xbar)
+        Abar = -Bbar @ Xr.t()
+        kappa = float(A.abs().sum(dim=1).max()) * float(
+            torch.linalg.inv(A).abs().sum(dim=1).max())
+    tol = 64 * n * EPS * kappa
+    for got, ref in ((X.detach(), Xr), (A.grad, Abar), (B.grad, Bbar)):
+        err = float((got - ref).abs().max() / ref.abs().max())
+        assert err <= tol, (err, tol)
+    del Xr, Bbar, Abar
+    # Directions: the normalised sum of the computed gradient's direction and a
+    # seeded random unit direction, so that the derivative is of the order of
+    # the gradient's norm and far above the rounding floor of the difference
+    # quotient (a purely random direction of this dimension sees a derivative
+    # about sqrt(N^2) times smaller).
+    h = 1e-6
+    dA = torch.randn(n, n, generator=g, dtype=torch.float64, device="cuda")
+    dB = torch.randn(n, nrhs, generator=g, dtype=torch.float64, device="cuda")
+    dA = dA / dA.norm() + A.grad / A.grad.norm()
+    dB = dB / dB.norm() + B.grad / B.grad.norm()
+    dA /= dA.norm()
+    dB /= dB.norm()
+
+    def L(Ap, Bp):
+        with torch.no_grad():
+            return float((hpl_solve(Ap, Bp, nb=512) * Xbar).sum())
+
+    Ad, Bd = A.detach(), B.detach()
+    fdA = (L(Ad + h * dA, Bd) - L(Ad - h * dA, Bd)) / (2 * h)
+    fdB = (L(Ad, Bd + h * dB) - L(Ad, Bd - h * dB)) / (2 * h)
+    assert abs(float((A.grad * dA).sum()) - fdA) <= 1e-4 * abs(fdA)
+    assert abs(float((B.grad * dB).sum()) - fdB) <= 1e-4 * abs(fdB)
+
+
 def test_hpl_solve_vector_rhs_and_errors(hlib, oracle):
     import torch
 

@@ -1,5 +1,8 @@
 """Kernel-level parity of the CUDA path against the oracle and against
 rocHPL's own matgen / row-swap code (oracle/_ref), through the C ABI."""
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -35,6 +38,62 @@ def test_matgen_bit_exact_vs_reference_kernel(hlib, oracle, m, n, nb):
     hlib.matgen(m, n, 100, d1.data_ptr(), ld, nb)
     assert R.ref_pdrandmat(m, n, nb, d2.data_ptr(), ld, 100) == 0
     assert torch.equal(d1.view(torch.int64), d2.view(torch.int64))
+
+
+@pytest.mark.parametrize("mg,ng,i0,j0,m,n", [(1000, 1001, 0, 0, 1000, 1001),
+                                              (1000, 1001, 17, 300, 500, 400),
+                                              (4096, 4097, 4095, 4096, 1, 1),
+                                              (5000, 37, 1234, 5, 3000, 32)])
+def test_matgen_block_equals_full_matrix(hlib, oracle, mg, ng, i0, j0, m, n):
+    """hplb_matgen_block is the sub-block of hplb_matgen, bit for bit, and the
+    oracle's block generator agrees."""
+    import torch
+
+    ld = m + 3
+    dA = torch.full((ld * n,), np.nan, dtype=torch.float64, device="cuda")
+    hlib.matgen_block(mg, ng, i0, j0, m, n, 100, dA.data_ptr(), ld)
+    got = from_dev(dA, ld, n)
+    full = oracle.matgen(mg, ng, 100)
+    assert np.array_equal(got[:m].view(np.uint64), full[i0:i0 + m, j0:j0 + n].view(np.uint64))
+    assert np.array_equal(got[:m].view(np.uint64),
+                          oracle.matgen_block(mg, i0, j0, m, n, 100).view(np.uint64))
+    assert np.all(np.isnan(got[m:]))
+
+
+def test_matgen_block_rejects_blocks_outside_the_matrix(hlib):
+    from rochpl_b200.lib import HplError
+
+    with pytest.raises(HplError):
+        hlib.matgen_block(100, 101, 90, 0, 20, 1, 100, 0, 20)
+    with pytest.raises(HplError):
+        hlib.matgen_block(100, 101, 0, 100, 100, 2, 100, 0, 100)
+
+
+C2_GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "lcg_c2_golden.json")
+
+
+@pytest.mark.skipif(not os.path.exists(C2_GOLD),
+                    reason="made on a GPU by tests/golden/make_golden.py --lcg-c2")
+def test_matgen_c2_blocks_match_reference_kernel(hlib, oracle):
+    """The N = 131072 [A|b] (LCG state indices up to 1.7e10, past 2^32): the
+    first, middle and last 512-column blocks and b, generated here as blocks of
+    the full matrix, against the reference generator's own output (hashes and
+    samples in the golden file) and against the oracle, bit for bit."""
+    import torch
+
+    g = json.load(open(C2_GOLD))
+    n = g["n"]
+    for b in g["blocks"]:
+        c0, w = b["col0"], b["ncols"]
+        dA = torch.empty(n * w, dtype=torch.float64, device="cuda")
+        hlib.matgen_block(n, n + 1, 0, c0, n, w, g["seed"], dA.data_ptr(), n)
+        A = from_dev(dA, n, w)
+        del dA
+        assert f"{oracle.hash_block(A, n, w):016x}" == b["fnv1a"], b["name"]
+        for i, j, hx in b["samples"]:
+            assert A[i, j - c0].hex() == hx, (b["name"], i, j)
+        ref = oracle.matgen_block(n, 0, c0, n, w, g["seed"])
+        assert np.array_equal(A.view(np.uint64), ref.view(np.uint64)), b["name"]
 
 
 DGEMM_SHAPES = [(1, 1, 1), (7, 5, 3), (128, 128, 16), (200, 300, 512), (1000, 513, 512),

@@ -52,6 +52,64 @@ def test_solve_parity(hlib, oracle, n, nb, nbmin):
     assert res["resid"] < 16.0
 
 
+def test_leaf_kinds_give_identical_results(hlib, oracle):
+    """The three places the leaf can keep its slice (hplb_set_option
+    HPLB_OPT_LEAF) perform the same operations in the same order: the same
+    pivots as the oracle and bit-identical x."""
+    import torch
+
+    from rochpl_b200.lib import LEAF_AUTO, LEAF_GLOBAL, LEAF_SHARED, HplError
+
+    xs = []
+    try:
+        for kind in (LEAF_AUTO, LEAF_SHARED, LEAF_GLOBAL):
+            hlib.set_leaf(kind)
+            r = solve_both(hlib, oracle, 2048, 256, 32)
+            assert np.array_equal(r["ipiv"], r["po"]), kind
+            xs.append(r["x"])
+    finally:
+        hlib.set_leaf(LEAF_AUTO)
+    assert all(np.array_equal(x.view(np.uint64), xs[0].view(np.uint64)) for x in xs)
+    with pytest.raises(HplError):
+        hlib.set_leaf(3)
+
+
+def test_solve_parity_n16384_against_the_oracle(hlib, oracle):
+    """The parity solve at N = 16384, NB = 512 (the size the bench's CPU leg
+    factors): identical pivot vectors, x within 64 N eps kappa_oo of the
+    oracle's x, residual < 16.  The oracle's level 3 runs in the host OpenBLAS
+    here (the scalar restatement would take half an hour at this size)."""
+    import torch
+
+    n, nb = 16384, 512
+    if not oracle.use_blas(0):
+        pytest.skip("no host OpenBLAS for the oracle")
+    try:
+        x_o, p_o, info_o, resid_o = oracle.hpl_test(n, nb, 32, 2)
+    finally:
+        oracle.no_blas()
+    from rochpl_b200.hpl import Algo
+
+    ld = oracle.default_ld(n)
+    dA = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+    hlib.matgen(n, n + 1, 100, dA.data_ptr(), ld, nb)
+    A = dA.view(n + 1, ld)[:n, :n].t()
+    kappa = float(A.abs().sum(dim=1).max()) * float(torch.linalg.inv(A).abs().sum(dim=1).max())
+    del A
+    dX = torch.zeros(n, dtype=torch.float64, device="cuda")
+    dP = torch.zeros(n, dtype=torch.int32, device="cuda")
+    info = hlib.pdgesv(Algo(nb, 32, 2, 2, 2, 1, 0).c(), n, dA.data_ptr(), ld, dX.data_ptr(),
+                       dP.data_ptr())
+    assert info == 0 and info_o == 0
+    div = np.nonzero(dP.cpu().numpy() != p_o)[0]
+    assert div.size == 0, f"pivot divergence at columns {div[:10]}"
+    x = dX.cpu().numpy()
+    err = np.max(np.abs(x - x_o)) / np.max(np.abs(x_o))
+    tol = 64 * n * EPS * kappa
+    assert err <= tol, (err, tol)
+    assert hlib.residual_lcg(n, 100, dX.data_ptr())["resid"] < 16.0 and resid_o < 16.0
+
+
 @pytest.mark.parametrize("pfact,rfact", [(0, 0), (1, 1), (2, 0), (0, 2), (1, 2), (2, 1)])
 def test_solve_variants(hlib, oracle, pfact, rfact):
     r = solve_both(hlib, oracle, 600, 128, 16, 2, pfact, rfact)

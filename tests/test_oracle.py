@@ -37,6 +37,27 @@ def test_lcg_matches_reference_kernel(oracle):
             assert A[i, j].hex() == hx
 
 
+@pytest.mark.skipif(not os.path.exists(os.path.join(GOLD, "lcg_c2_golden.json")),
+                    reason="made on a GPU by make_golden.py --lcg-c2")
+def test_lcg_c2_blocks_match_reference_kernel(oracle):
+    """The oracle's generator at N = 131072, where the state index i + j N
+    passes 2^32, against the reference generator's own blocks."""
+    g = json.load(open(os.path.join(GOLD, "lcg_c2_golden.json")))
+    n = g["n"]
+    for b in g["blocks"]:
+        A = oracle.matgen_block(n, 0, b["col0"], n, b["ncols"], g["seed"])
+        assert f"{oracle.hash_block(A, n, b['ncols']):016x}" == b["fnv1a"], b["name"]
+        for i, j, hx in b["samples"]:
+            assert A[i, j - b["col0"]].hex() == hx
+            assert oracle.lcg_value(oracle.lcg_state(g["seed"], n, i, j)).hex() == hx
+
+
+def test_matgen_block_is_a_block_of_matgen(oracle):
+    A = oracle.matgen(300, 301, 7)
+    for (i0, j0, m, n) in [(0, 0, 300, 301), (5, 9, 100, 200), (299, 300, 1, 1)]:
+        assert np.array_equal(oracle.matgen_block(300, i0, j0, m, n, 7), A[i0:i0 + m, j0:j0 + n])
+
+
 def test_lcg_value_range_and_state_index(oracle):
     # Entry (i, j) of an m-row matrix is state X(1 + i + j m) (P = Q = 1).
     A = oracle.matgen(37, 5, 100)

@@ -28,8 +28,10 @@ def _solution(n, nb=128):
     return lib, dX
 
 
-@pytest.mark.parametrize("n", [1000, 4096])
+@pytest.mark.parametrize("n", [1000, 4096, 16384])
 def test_noalloc_matches_context_residual_twice(n):
+    """n = 16384 is the limit itself: every chunk of the array's layout, the
+    table block and the output slot at its end are in use."""
     from rochpl_b200.lib import HPLB_OK, residual_lcg_noalloc
 
     lib, dX = _solution(n)
