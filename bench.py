@@ -884,8 +884,26 @@ def case_dgemm(args) -> None:
         print(f"dgemm_sub {m}x{n}x{k}: {ms:.3f} ms, {2.0 * m * n * k / ms / 1e9:.2f} TFLOP/s")
 
 
+def _kernel_split(prof, top=24):
+    """Per-kernel device time and launch count from a torch.profiler trace
+    (CUPTI activity records: concurrent streams as in production)."""
+    import collections
+
+    agg = collections.defaultdict(lambda: [0.0, 0])
+    for e in prof.events():
+        if e.device_type.name != "CUDA":
+            continue
+        name = e.name.replace("void ", "").replace("hplb::(anonymous namespace)::", "")
+        name = name.split("(")[0][:48]
+        agg[name][0] += (e.time_range.end - e.time_range.start) / 1e3
+        agg[name][1] += 1
+    for name, (ms, cnt) in sorted(agg.items(), key=lambda kv: -kv[1][0])[:top]:
+        print(f"{name:50s} {ms:10.2f} ms {cnt:7d}")
+
+
 def case_solve(args) -> None:
-    """One generate + hplb_pdgesv (--n, --nb), with its timing split."""
+    """generate + hplb_pdgesv (--n, --nb) twice, with the timing split of the
+    second; --breakdown adds a per-kernel split of a third solve."""
     import torch
 
     from rochpl_b200 import library
@@ -894,15 +912,27 @@ def case_solve(args) -> None:
     lib = library(0)
     n, nb = args.n, args.nb
     ld = default_ld(n)
+    algo = Algo(nb, 32, 2, 2, 2, 1, 0)
     dA = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
     dX = torch.zeros(n, dtype=torch.float64, device="cuda")
-    lib.matgen(n, n + 1, 100, dA.data_ptr(), ld, nb)
-    lib.pdgesv(Algo(nb, 32, 2, 2, 2, 1, 0).c(), n, dA.data_ptr(), ld, dX.data_ptr())
+    for _ in range(2):
+        lib.matgen(n, n + 1, 100, dA.data_ptr(), ld, nb)
+        lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr())
     t = lib.last_timing()
     res = lib.residual_lcg(n, 100, dX.data_ptr())
     print(f"solve N={n} NB={nb}: {t['total_ms']:.2f} ms, "
-          f"{hpl_flops(n) / t['total_ms'] / 1e9:.2f} TFLOP/s, trsv {t['trsv_ms']:.3f} ms, "
-          f"resid {res['resid']:.3e}")
+          f"{hpl_flops(n) / t['total_ms'] / 1e9:.2f} TFLOP/s, lu {t['lu_ms']:.2f} ms, "
+          f"panel {t['panel_ms']:.2f} ms, gemm {t['gemm_ms']:.2f} ms, trsv {t['trsv_ms']:.3f} ms "
+          f"({n * n / 2 * 8 / (t['trsv_ms'] * 1e-3) / 1e9:.0f} GB/s), resid {res['resid']:.3e}")
+    if args.breakdown:
+        from torch.profiler import ProfilerActivity, profile
+
+        lib.matgen(n, n + 1, 100, dA.data_ptr(), ld, nb)
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            lib.pdgesv(algo.c(), n, dA.data_ptr(), ld, dX.data_ptr())
+            torch.cuda.synchronize()
+        _kernel_split(prof)
 
 
 def case_gemm_lp(args) -> None:
@@ -953,8 +983,6 @@ def case_getrf(args) -> None:
 def case_mixed(args) -> None:
     """hplb_pdgesv_mixed (--n, --prec), with a per-kernel split from the torch
     profiler's CUDA activity records."""
-    import collections
-
     import torch
     from torch.profiler import ProfilerActivity, profile
 
@@ -971,16 +999,7 @@ def case_mixed(args) -> None:
         r = lib.pdgesv_mixed(algo.c(), n, x.data_ptr(), seed=100, precision=args.prec)
         torch.cuda.synchronize()
     print({k: round(v, 2) if isinstance(v, float) else v for k, v in r.items()})
-    agg = collections.defaultdict(lambda: [0.0, 0])
-    for e in prof.events():
-        if e.device_type.name != "CUDA":
-            continue
-        name = e.name.replace("void ", "").replace("hplb::(anonymous namespace)::", "")
-        name = name.split("(")[0][:48]
-        agg[name][0] += (e.time_range.end - e.time_range.start) / 1e3
-        agg[name][1] += 1
-    for name, (ms, cnt) in sorted(agg.items(), key=lambda kv: -kv[1][0])[:24]:
-        print(f"{name:50s} {ms:10.1f} ms {cnt:7d}")
+    _kernel_split(prof)
 
 
 def case_batch(args) -> None:
@@ -1036,6 +1055,8 @@ def main():
     ap.add_argument("--k", type=int, default=1536, help="--case gemm_lp: reduction size")
     ap.add_argument("--prec", type=int, default=3, help="--case mixed: precision")
     ap.add_argument("--nrhs", type=int, default=16, help="--case batch: right-hand sides")
+    ap.add_argument("--breakdown", action="store_true",
+                    help="--case solve: per-kernel split of one more solve (torch profiler)")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",

@@ -34,6 +34,8 @@ struct hplb_ctx {
   double* d_cand       = nullptr;
   double* d_cur        = nullptr;
   size_t  cand_cap     = 0;  // doubles
+  int*    d_trsv       = nullptr;  // back-solve flags and ticket
+  size_t  trsv_cap     = 0;        // ints
   double* d_res        = nullptr;
   size_t  res_cap      = 0;  // doubles
 

@@ -60,6 +60,8 @@ hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
   if(n > 0 &&
      (s = grow(ctx, &ctx->d_w, &ctx->w_cap, (size_t)nb * (size_t)(n + 1))) != HPLB_OK)
     return s;
+  if((s = grow(ctx, &ctx->d_trsv, &ctx->trsv_cap, trsv_flag_ints(std::max(n, 1)))) != HPLB_OK)
+    return s;
   return ensure_leaf_ws(ctx, n, nbmin);
 }
 
@@ -265,7 +267,7 @@ void hplb_destroy(hplb_ctx* ctx) {
                   ctx->d_w,       ctx->m_w,       ctx->m_linv,        ctx->m_uinv,
                   ctx->m_perm,    ctx->m_g,       ctx->m_l16,         ctx->m_u16,
                   ctx->m_scale,   ctx->m_small,   ctx->m_vec,         ctx->r_t,
-                  ctx->r_ws,      ctx->r_perm,    ctx->m_li16};
+                  ctx->r_ws,      ctx->r_perm,    ctx->m_li16,        ctx->d_trsv};
   for(void* b : bufs)
     if(b) cudaFree(b);
   if(ctx->s_upd) cudaStreamDestroy(ctx->s_upd);
@@ -354,7 +356,7 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
     ctx->step_col.push_back(j);
   }
   CK(cudaEventRecord(ev_lu, ctx->s_upd));
-  if(rhs) CK(launch_trsv(dA, ld, n, dX, ctx->d_status, ctx->s_upd, &ctx->launches));
+  if(rhs) CK(launch_trsv(dA, ld, n, dX, ctx->d_trsv, ctx->d_status, ctx->s_upd, &ctx->launches));
   if(ipiv_out)
     CK(cudaMemcpyAsync(ipiv_out, ctx->d_ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice,
                        ctx->s_upd));

@@ -71,7 +71,9 @@ cudaError_t launch_laswp_gather(T* A, int64_t ld, int ia, int jb, const int* per
                                 int64_t ldw, int c0, int n, cudaStream_t stream);
 
 // Back-solve U x = y, y = column n of A, x written to X.
-cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* status,
+// The back-solve's flags: one per 64-row block plus the ticket counter.
+size_t      trsv_flag_ints(int n);
+cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* flags, int* status,
                         cudaStream_t stream, int* launches);
 
 // Residual check.  ws must hold residual_ws_doubles(n) doubles.

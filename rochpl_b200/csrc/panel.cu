@@ -677,27 +677,45 @@ laswp_trsm_kernel(T* A, int64_t ld, int ia, int jb, const T* L, int64_t ldl,
 // Row interchanges of the panel applied to columns [c0, c0+n), with the new
 // top jb rows gathered into W (jb x n, leading dimension ldw) instead of being
 // written back: W then feeds U12 = L11^-1 W as a DMMA GEMM that writes the top
-// rows of A.  Displaced top rows go straight to their new rows below.  Each
-// CTA owns kGatherCols columns; its gathers from rows >= jb read exactly the
-// rows its displaced writes overwrite, hence the barrier between the two.
-constexpr int kGatherCols = 8;
+// rows of A.  Displaced top rows go straight to their new rows below.  The
+// row map sits in shared memory; each warp owns whole columns (lane = row, so
+// every W store and every unpermuted read is a 256-byte segment), gathers a
+// column's jb rows into registers before any of its displaced writes (which
+// overwrite exactly rows the gather may read: the warp's own column only, so a
+// __syncwarp orders them), and moves on to its next column.
+constexpr int kGatherWarps = 8;
+constexpr int kGatherRegs  = 16;  // rows per lane held at once (jb <= 512 in one pass)
 template <typename T>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(kGatherWarps * 32)
 laswp_gather_kernel(T* A, int64_t ld, int ia, int jb, const int* __restrict__ permU,
                     T* __restrict__ W, int64_t ldw, int c0, int n) {
-  const int cb = c0 + blockIdx.x * kGatherCols;
-  const int nc = min(kGatherCols, c0 + n - cb);
-  for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
-    const int c = idx / jb, x = idx % jb;
-    W[(size_t)x + (size_t)(cb - c0 + c) * ldw] =
-        A[(size_t)(ia + permU[x]) + (size_t)(cb + c) * ld];
-  }
+  extern __shared__ int s_perm[];  // 2 jb ints
+  for(int i = threadIdx.x; i < 2 * jb; i += blockDim.x) s_perm[i] = permU[i];
   __syncthreads();
-  for(int idx = threadIdx.x; idx < nc * jb; idx += blockDim.x) {
-    const int c = idx / jb, s = idx % jb;
-    const int dst = permU[jb + s];
-    if(dst >= 0)
-      A[(size_t)(ia + dst) + (size_t)(cb + c) * ld] = A[(size_t)(ia + s) + (size_t)(cb + c) * ld];
+  const int lane = threadIdx.x & 31;
+  const int warps = gridDim.x * kGatherWarps;
+  for(int c = blockIdx.x * kGatherWarps + (threadIdx.x >> 5); c < n; c += warps) {
+    T*       col = A + (size_t)ia + (size_t)(c0 + c) * (size_t)ld;
+    T*       wc  = W + (size_t)c * (size_t)ldw;
+    for(int x0 = 0; x0 < jb; x0 += 32 * kGatherRegs) {
+      T v[kGatherRegs];
+#pragma unroll
+      for(int k = 0; k < kGatherRegs; ++k) {
+        const int x = x0 + 32 * k + lane;
+        v[k] = x < jb ? col[s_perm[x]] : (T)0;
+      }
+#pragma unroll
+      for(int k = 0; k < kGatherRegs; ++k) {
+        const int x = x0 + 32 * k + lane;
+        if(x < jb) wc[x] = v[k];
+      }
+    }
+    __syncwarp();
+    for(int x = lane; x < jb; x += 32) {
+      const int dst = s_perm[jb + x];
+      if(dst >= 0) col[dst] = col[x];
+    }
+    __syncwarp();
   }
 }
 
@@ -949,7 +967,14 @@ template <typename T>
 cudaError_t launch_laswp_gather(T* A, int64_t ld, int ia, int jb, const int* permU, T* W,
                                 int64_t ldw, int c0, int n, cudaStream_t stream) {
   if(n <= 0 || jb <= 0) return cudaSuccess;
-  laswp_gather_kernel<T><<<(n + kGatherCols - 1) / kGatherCols, 256, 0, stream>>>(
+  // One column per warp, capped at 8 CTAs per SM (wide updates then give each
+  // warp several columns instead of re-staging the row map per column).
+  int sms = 0, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int want = (n + kGatherWarps - 1) / kGatherWarps;
+  const int grid = std::max(1, std::min(want, 8 * std::max(sms, 1)));
+  laswp_gather_kernel<T><<<grid, kGatherWarps * 32, 2 * jb * sizeof(int), stream>>>(
       A, ld, ia, jb, permU, W, ldw, c0, n);
   return cudaGetLastError();
 }

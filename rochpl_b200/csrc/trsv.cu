@@ -1,10 +1,26 @@
 // Back-solve U x = y at P = Q = 1 (src/pgesv/HPL_pdtrsv_device.cpp:29-346).
 //
-// y is column n of the factored [A|b]; x is written to X.  Blocked from the
-// bottom up in kTb-row blocks: a one-warp kernel solves the diagonal block out
-// of shared memory, then a row-parallel GEMV removes that block's contribution
-// from every row above it (rocblas_dtrsv + rocblas_dgemv in the reference).
-// The GEMVs stream the upper triangle once: n^2/2 * 8 bytes, HBM-bound.
+// y is column n of the factored [A|b]; x is written to X; A is not modified.
+// The reference solves bottom-up in NB blocks: rocblas_dtrsv on the diagonal
+// block, then rocblas_dgemv to remove that block's contribution from every row
+// above, two serial library calls per block.  Here the whole solve is ONE
+// persistent kernel, HBM-bound on the single pass over the upper triangle
+// (n^2/2 * 8 bytes):
+//
+//  * CTA k (in the order CTAs start, from an atomic ticket) owns row block
+//    bi = nblk - 1 - k of kTb rows, so row blocks are taken bottom first.
+//  * It streams its row panel U[bi, j] for j = nblk-1 down to bi+1, 16-byte
+//    column segments, the next tile loaded while it waits for the current one's
+//    x block, and accumulates U[bi, j] x_j in registers (each warp owns 8 of
+//    the 64 columns of every tile, each lane 2 rows).
+//  * x_j is published by the CTA that owns row block j: a release store of
+//    flag j after x_j is written; readers acquire it.  A CTA only waits for
+//    row blocks below its own, whose tickets were taken by CTAs that started
+//    before it, so every wait ends; each is also bounded (status site 41).
+//  * While the first flag is awaited the CTA inverts its own diagonal block
+//    U_ii in shared memory (off the critical path), so the serial chain
+//    through the blocks costs one 64 x 64 product per block instead of a
+//    64-step substitution: x_i = U_ii^-1 (y_i - sum_j U_ij x_j).
 #include "common.cuh"
 #include "internal.h"
 
@@ -12,69 +28,169 @@ namespace hplb {
 
 namespace {
 
-constexpr int kTb = 64;
+constexpr int kTb          = 64;   // rows (and columns) per block
+constexpr int kTrsvThreads = 256;  // 8 warps
+constexpr int kTrsvWarps   = kTrsvThreads / 32;
+constexpr int kColsPerWarp = kTb / kTrsvWarps;  // columns of a tile per warp
+constexpr int kTrsvSite    = 41;
 
-// Solve the kb x kb upper block at (s, s) in place on X[s : s+kb].
-__global__ void __launch_bounds__(32) trsv_diag_kernel(const double* A, int64_t ld, int s,
-                                                       int kb, double* X) {
-  __shared__ double U[kTb][kTb + 1];  // U[r][c]
-  const int lane = threadIdx.x;
-  for(int c = 0; c < kb; ++c)
-    for(int r = lane; r < kb; r += 32) U[r][c] = A[(size_t)(s + r) + (size_t)(s + c) * ld];
-  double y0 = lane < kb ? X[s + lane] : 0.0;
-  double y1 = lane + 32 < kb ? X[s + lane + 32] : 0.0;
-  __syncwarp();
-  for(int i = kb - 1; i >= 0; --i) {
-    const double yi = __shfl_sync(0xffffffffu, i < 32 ? y0 : y1, i & 31);
-    const double xi = yi / U[i][i];
-    if(lane == (i & 31)) {
-      if(i < 32)
-        y0 = xi;
-      else
-        y1 = xi;
+struct TrsvSmem {
+  double T[kTb][kTb + 1];          // U_ii, then U_ii^-1 (upper triangular)
+  double red[kTrsvWarps][kTb];     // per-warp partial row sums
+  double r[kTb];                   // right-hand side of the diagonal block
+  double tmp[kTb];
+  int    ticket;
+};
+
+// Spin (bounded) until flag == 1; false once this or any block timed out.
+HPLB_DEV bool wait_flag(const int* flag, int* status) {
+  if(ld_acquire_gpu(flag) != 0) return true;
+  const unsigned long long t0 = globaltimer();
+  for(unsigned polls = 1;; ++polls) {
+    if(ld_acquire_gpu(flag) != 0) return true;
+    if((polls & 31u) == 0) {
+      if(ld_acquire_gpu(status + ST_TIMEOUT) != 0) return false;
+      if(globaltimer() - t0 > kWaitBudgetNs) {
+        atomicCAS(status + ST_TIMEOUT, 0, kTrsvSite);
+        return false;
+      }
     }
-    if(lane < i) y0 -= U[lane][i] * xi;
-    if(lane + 32 < i) y1 -= U[lane + 32][i] * xi;
+    __nanosleep(32);
   }
-  if(lane < kb) X[s + lane] = y0;
-  if(lane + 32 < kb) X[s + lane + 32] = y1;
 }
 
-// X[0:s] -= U[0:s, s:s+kb] X[s:s+kb]; one thread per row, coalesced columns.
-__global__ void __launch_bounds__(256) trsv_gemv_kernel(const double* A, int64_t ld, int s,
-                                                        int kb, double* X) {
-  __shared__ double xs[kTb];
-  if(threadIdx.x < kb) xs[threadIdx.x] = X[s + threadIdx.x];
+template <bool VEC>
+HPLB_DEV void load_tile(const double* __restrict__ A, int64_t ld, int r0, int c0, int kc,
+                        int lane, int warp, double2 (&v)[kColsPerWarp]) {
+#pragma unroll
+  for(int q = 0; q < kColsPerWarp; ++q) {
+    const int c = warp + kTrsvWarps * q;
+    if(c < kc) {
+      const double* p = A + (size_t)(r0 + 2 * lane) + (size_t)(c0 + c) * (size_t)ld;
+      if(VEC) {
+        v[q] = __ldcs(reinterpret_cast<const double2*>(p));
+      } else {
+        v[q].x = __ldcs(p);
+        v[q].y = __ldcs(p + 1);
+      }
+    } else {
+      v[q] = make_double2(0.0, 0.0);
+    }
+  }
+}
+
+// In-place inverse of the upper triangular kTb x kTb block in S.T (column by
+// column, left to right: column j of the inverse is -T_jj^-1 times the
+// already-inverted leading block applied to column j of U).
+HPLB_DEV void invert_upper(TrsvSmem& S) {
+  const int t = threadIdx.x, row = t >> 2, part = t & 3;
+  for(int j = 0; j < kTb; ++j) {
+    double s = 0.0;
+    if(row < j)
+      for(int k = row + part; k < j; k += 4) s = fma(S.T[row][k], S.T[k][j], s);
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    const double d = 1.0 / S.T[j][j];
+    __syncthreads();
+    if(part == 0 && row < j) S.T[row][j] = -d * s;
+    if(t == 0) S.T[j][j] = d;
+    __syncthreads();
+  }
+}
+
+template <bool VEC>
+__global__ void __launch_bounds__(kTrsvThreads)
+trsv_kernel(const double* __restrict__ A, int64_t ld, int n, double* __restrict__ X, int* flags,
+            int* status) {
+  __shared__ TrsvSmem S;
+  const int nblk = (n + kTb - 1) / kTb;
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  if(t == 0) S.ticket = atomicAdd(flags + nblk, 1);
   __syncthreads();
-  const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if(r >= s) return;
-  const double* a = A + (size_t)r + (size_t)s * ld;
-  double acc = 0.0;
-#pragma unroll 8
-  for(int c = 0; c < kb; ++c) acc += a[(size_t)c * ld] * xs[c];
-  X[r] -= acc;
+  const int bi = nblk - 1 - S.ticket;
+  const int r0 = bi * kTb;
+  const int kb = min(kTb, n - r0);
+
+  // First tile of the row panel in flight before anything else.
+  double2 cur[kColsPerWarp], nxt[kColsPerWarp];
+#pragma unroll
+  for(int q = 0; q < kColsPerWarp; ++q) cur[q] = nxt[q] = make_double2(0.0, 0.0);
+  int     j = nblk - 1;
+  if(j > bi) load_tile<VEC>(A, ld, r0, j * kTb, min(kTb, n - j * kTb), lane, warp, cur);
+
+  // Diagonal block (identity beyond kb), inverted while the loads fly.
+  for(int idx = t; idx < kTb * kTb; idx += kTrsvThreads) {
+    const int c = idx / kTb, r = idx % kTb;
+    double    v = (r == c) ? 1.0 : 0.0;
+    if(r < kb && c < kb) v = r <= c ? A[(size_t)(r0 + r) + (size_t)(r0 + c) * (size_t)ld] : 0.0;
+    S.T[r][c] = v;
+  }
+  if(t < kTb) S.r[t] = t < kb ? A[(size_t)(r0 + t) + (size_t)n * (size_t)ld] : 0.0;
+  __syncthreads();
+  invert_upper(S);
+
+  // Row panel: acc = sum_j U[bi, j] x_j over the rows 2 lane, 2 lane + 1.
+  double acc0 = 0.0, acc1 = 0.0;
+  bool   alive = true;
+  for(; j > bi; --j) {
+    if(j - 1 > bi) load_tile<VEC>(A, ld, r0, (j - 1) * kTb, kTb, lane, warp, nxt);
+    if(alive) alive = wait_flag(flags + j, status);
+    const double* xj = X + (size_t)j * kTb;
+    const int     kc = min(kTb, n - j * kTb);
+#pragma unroll
+    for(int q = 0; q < kColsPerWarp; ++q) {
+      const int    c  = warp + kTrsvWarps * q;
+      const double xc = c < kc ? __ldcg(xj + c) : 0.0;
+      acc0            = fma(cur[q].x, xc, acc0);
+      acc1            = fma(cur[q].y, xc, acc1);
+    }
+#pragma unroll
+    for(int q = 0; q < kColsPerWarp; ++q) cur[q] = nxt[q];
+  }
+
+  // r = y_i - sum_j U_ij x_j, then x_i = U_ii^-1 r.
+  S.red[warp][2 * lane]     = acc0;
+  S.red[warp][2 * lane + 1] = acc1;
+  __syncthreads();
+  if(t < kTb) {
+    double s = 0.0;
+#pragma unroll
+    for(int w = 0; w < kTrsvWarps; ++w) s += S.red[w][t];
+    S.tmp[t] = S.r[t] - s;
+  }
+  __syncthreads();
+  {
+    const int m = t & (kTb - 1), q = t / kTb;  // 4 quarters of the 64 columns
+    double    s = 0.0;
+#pragma unroll
+    for(int k = 0; k < kTb / 4; ++k) s = fma(S.T[m][q * (kTb / 4) + k], S.tmp[q * (kTb / 4) + k], s);
+    S.red[q][m] = s;
+  }
+  __syncthreads();
+  if(t < kb) {
+    X[r0 + t] = (S.red[0][t] + S.red[1][t]) + (S.red[2][t] + S.red[3][t]);
+    __threadfence();
+  }
+  __syncthreads();
+  if(t == 0) st_release_gpu(flags + bi, 1);
 }
 
 }  // namespace
 
-cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* status,
+size_t trsv_flag_ints(int n) { return (size_t)(n + kTb - 1) / kTb + 1; }
+
+cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* flags, int* status,
                         cudaStream_t stream, int* launches) {
-  (void)status;
   if(n <= 0) return cudaSuccess;
-  cudaError_t e = cudaMemcpyAsync(X, A + (size_t)n * ld, (size_t)n * sizeof(double),
-                                  cudaMemcpyDeviceToDevice, stream);
+  const int   nblk = (n + kTb - 1) / kTb;
+  cudaError_t e    = cudaMemsetAsync(flags, 0, trsv_flag_ints(n) * sizeof(int), stream);
   if(e != cudaSuccess) return e;
-  const int nblk = (n + kTb - 1) / kTb;
-  for(int b = nblk - 1; b >= 0; --b) {
-    const int s  = b * kTb;
-    const int kb = min(kTb, n - s);
-    trsv_diag_kernel<<<1, 32, 0, stream>>>(A, ld, s, kb, X);
-    ++*launches;
-    if(s > 0) {
-      trsv_gemv_kernel<<<(s + 255) / 256, 256, 0, stream>>>(A, ld, s, kb, X);
-      ++*launches;
-    }
-  }
+  const bool vec = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ld % 2 == 0);
+  if(vec)
+    trsv_kernel<true><<<nblk, kTrsvThreads, 0, stream>>>(A, ld, n, X, flags, status);
+  else
+    trsv_kernel<false><<<nblk, kTrsvThreads, 0, stream>>>(A, ld, n, X, flags, status);
+  ++*launches;
   return cudaGetLastError();
 }
 
