@@ -13,10 +13,17 @@
 //   warps 2..9  epilogue: tcgen05.ld of the accumulator rows their TMEM lane
 //               group may read, scale, and C -= in FP32.  Two accumulators let
 //               the epilogue of one tile (HBM-bound: 128 KB read + 128 KB
-//               written) overlap the MMAs of the next.
+//               written) overlap the MMAs of the next.  When C allows a TMA
+//               map (16-byte aligned base, ldc a multiple of 4) the epilogue
+//               writes -scale * acc in 16-column chunks to a per-warp staging
+//               buffer and hands each to a TMA reduce-add
+//               (cp.reduce.async.bulk.tensor ... .add), so the read-modify-write
+//               of C happens in L2 and the epilogue warps never wait on a C
+//               load; otherwise they load, subtract and store C themselves.
 // Every mbarrier wait is bounded; on expiry the CTA records the site, the
 // roles leave their loops, TMEM is released and the CTA exits.
 #include <cstdlib>
+#include <cstring>
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -35,6 +42,10 @@ constexpr int LA_BYTES = LBM * LBK * 2;  // 16 KB
 constexpr int LB_BYTES = LBN * LBK * 2;  // 32 KB
 constexpr int LSTAGE_BYTES = LA_BYTES + LB_BYTES;
 constexpr int L_SMEM = LSTAGES * LSTAGE_BYTES + 1024 + 256;
+constexpr int L_EPI_COLS = 16;                        // columns per staged chunk
+constexpr int L_STG_BYTES = L_EPI_COLS * 32 * 4;      // one warp's chunk: 2 KB
+constexpr int L_STG_TOTAL = L_EPI_WARPS * 2 * L_STG_BYTES;  // double-buffered: 32 KB
+constexpr int L_SMEM_TMA = L_SMEM + L_STG_TOTAL;
 constexpr int L_GROUP_N = 8;  // column tiles per group (A and B stay in L2)
 
 HPLB_DEV uint32_t su32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -103,6 +114,16 @@ HPLB_DEV void umma_commit(uint64_t* bar) {
       : "memory");
 }
 
+// C(x, y) += smem chunk, x = row (inner), y = column; out-of-range parts of
+// the box are skipped by the TMA unit.
+HPLB_DEV void tma_reduce_add2d(const CUtensorMap* map, const void* src, int c0, int c1) {
+  asm volatile(
+      "cp.reduce.async.bulk.tensor.2d.global.shared::cta.add.tile.bulk_group"
+      " [%0, {%2, %3}], [%1];" ::"l"(map),
+      "r"(su32(src)), "r"(c0), "r"(c1)
+      : "memory");
+}
+
 HPLB_DEV void tile_of(int t, int tiles_m, int tiles_n, int& tm, int& tn) {
   const int per = tiles_m * L_GROUP_N;
   const int grp = t / per;
@@ -112,17 +133,18 @@ HPLB_DEV void tile_of(int t, int tiles_m, int tiles_n, int& tm, int& tn) {
   tn            = grp * L_GROUP_N + (r - tm * gn);
 }
 
-template <bool BF16>
+template <bool BF16, bool TMA_EPI>
 __global__ void __launch_bounds__(L_THREADS, 1)
 gemm_lp_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
-               int m, int n, int k, float* __restrict__ C, int64_t ldc,
-               const float* __restrict__ sA, const float* __restrict__ sB, int tiles_m,
-               int tiles_n, int tpc, int* status) {
+               const __grid_constant__ CUtensorMap tmC, int m, int n, int k,
+               float* __restrict__ C, int64_t ldc, const float* __restrict__ sA,
+               const float* __restrict__ sB, int tiles_m, int tiles_n, int tpc, int* status) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* ringA = base;
   unsigned char* ringB = base + LSTAGES * LA_BYTES;
-  uint64_t* full  = (uint64_t*)(base + LSTAGES * LSTAGE_BYTES);
+  unsigned char* stage = base + LSTAGES * LSTAGE_BYTES;  // TMA_EPI: epilogue staging
+  uint64_t* full  = (uint64_t*)(stage + (TMA_EPI ? L_STG_TOTAL : 0));
   uint64_t* empty = full + LSTAGES;
   uint64_t* accf  = empty + LSTAGES;  // accumulator ready (MMA -> epilogue)
   uint64_t* acce  = accf + 2;         // accumulator drained (epilogue -> MMA)
@@ -254,7 +276,7 @@ gemm_lp_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
     const int ew   = warp - 2;              // 0..7
     const int sub  = warp & 3;              // TMEM lane group this warp may read
     const int half = ew >> 2;               // column half of the tile
-    int it = 0;
+    int it = 0, chunk = 0;
     for(int t = t_begin; t < t_end; ++t, ++it) {
       const int buf = it & 1;
       if(!bar_wait(&accf[buf], (uint32_t)((it >> 1) & 1), &s_abort)) {
@@ -267,6 +289,38 @@ gemm_lp_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
       tile_of(t, tiles_m, tiles_n, tm, tn);
       const int   row   = tm * LBM + sub * 32 + lane;
       const float scale = sA[tm] * sB[tn];
+      if constexpr(TMA_EPI) {
+        // Chunks of 16 columns: TMEM -> registers -> -scale * acc into this
+        // warp's staging buffer (column-major, 32 rows x 16) -> TMA reduce-add
+        // into C.  Two buffers per warp; a buffer is rewritten only after the
+        // reduce issued from it two chunks ago has read it.
+        unsigned char* mine = stage + ew * 2 * L_STG_BYTES;
+        for(int c0 = half * (LBN / 2); c0 < (half + 1) * (LBN / 2); c0 += L_EPI_COLS) {
+          uint32_t r[L_EPI_COLS];
+          const uint32_t taddr =
+              tmem + ((uint32_t)(sub * 32) << 16) + (uint32_t)(buf * LBN + c0);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,"
+              "%12,%13,%14,%15}, [%16];"
+              : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]),
+                "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]),
+                "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+              : "r"(taddr));
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+          float* sbuf = reinterpret_cast<float*>(mine + (chunk & 1) * L_STG_BYTES);
+          if(lane == 0) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");
+          __syncwarp();
+#pragma unroll
+          for(int j = 0; j < L_EPI_COLS; ++j) sbuf[j * 32 + lane] = -scale * __uint_as_float(r[j]);
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          __syncwarp();
+          if(lane == 0) {
+            tma_reduce_add2d(&tmC, sbuf, tm * LBM + sub * 32, tn * LBN + c0);
+            asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+          }
+          ++chunk;
+        }
+      } else {
       for(int c0 = half * (LBN / 2); c0 < (half + 1) * (LBN / 2); c0 += 32) {
         uint32_t r[32];
         const uint32_t taddr = tmem + ((uint32_t)(sub * 32) << 16) + (uint32_t)(buf * LBN + c0);
@@ -294,10 +348,15 @@ gemm_lp_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ 
               C[(size_t)row + (size_t)(col0 + j) * ldc] = cv[j] - scale * __uint_as_float(r[j]);
         }
       }
+      }
       asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
       __syncwarp();
       if(lane == 0) bar_arrive(&acce[buf]);
     }
+    // Every reduce this warp issued has finished (its staging reads and its
+    // writes) before the CTA's shared memory goes away.
+    if(TMA_EPI && lane == 0) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
+    __syncwarp();
   }
 
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -361,15 +420,39 @@ cudaError_t launch_gemm_lp(bool bf16, int m, int n, int k, const void* A16, int6
              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
       return cudaErrorInvalidValue;
   }
-  static bool attr[2] = {false, false};
-  cudaError_t e = cudaSuccess;
-  if(!attr[bf16]) {
-    e = bf16 ? cudaFuncSetAttribute(gemm_lp_kernel<true>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM)
-             : cudaFuncSetAttribute(gemm_lp_kernel<false>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM);
+  // C for the reduce-add epilogue: FP32, column-major, boxes of 32 rows x 16
+  // columns (one epilogue warp's chunk).  Needs a 16-byte aligned base and a
+  // leading dimension in whole 16-byte units; otherwise the plain epilogue.
+  CUtensorMap mC;
+  memset(&mC, 0, sizeof mC);
+  bool tma_epi = (uintptr_t)C % 16 == 0 && (ldc * 4) % 16 == 0;
+  if(tma_epi) {
+    cuuint64_t dims[2]    = {(cuuint64_t)m, (cuuint64_t)n};
+    cuuint64_t strides[1] = {(cuuint64_t)ldc * 4};
+    cuuint32_t box[2]     = {32, L_EPI_COLS};
+    cuuint32_t es[2]      = {1, 1};
+    tma_epi = g_enc(&mC, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)C, dims, strides, box, es,
+                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  }
+  static bool attr[4] = {false, false, false, false};
+  const int   kind    = (bf16 ? 1 : 0) + (tma_epi ? 2 : 0);
+  cudaError_t e       = cudaSuccess;
+  if(!attr[kind]) {
+    switch(kind) {
+      case 0: e = cudaFuncSetAttribute(gemm_lp_kernel<false, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM); break;
+      case 1: e = cudaFuncSetAttribute(gemm_lp_kernel<true, false>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM); break;
+      case 2: e = cudaFuncSetAttribute(gemm_lp_kernel<false, true>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM_TMA);
+              break;
+      default: e = cudaFuncSetAttribute(gemm_lp_kernel<true, true>,
+                                        cudaFuncAttributeMaxDynamicSharedMemorySize, L_SMEM_TMA);
+    }
     if(e != cudaSuccess) return e;
-    attr[bf16] = true;
+    attr[kind] = true;
   }
   const int tiles_m = (m + LBM - 1) / LBM, tiles_n = (n + LBN - 1) / LBN;
   const long long ntiles = (long long)tiles_m * tiles_n;
@@ -387,12 +470,23 @@ cudaError_t launch_gemm_lp(bool bf16, int m, int n, int k, const void* A16, int6
   const long long waves = (ntiles + (long long)sms * tmax - 1) / ((long long)sms * tmax);
   const int tpc = (int)((ntiles + (long long)sms * waves - 1) / ((long long)sms * waves));
   const long long grid = (ntiles + tpc - 1) / tpc;
-  if(bf16)
-    gemm_lp_kernel<true><<<(unsigned)grid, L_THREADS, L_SMEM, stream>>>(
-        mA, mB, m, n, k, C, ldc, sA, sB, tiles_m, tiles_n, tpc, status);
-  else
-    gemm_lp_kernel<false><<<(unsigned)grid, L_THREADS, L_SMEM, stream>>>(
-        mA, mB, m, n, k, C, ldc, sA, sB, tiles_m, tiles_n, tpc, status);
+  switch(kind) {
+    case 0:
+      gemm_lp_kernel<false, false><<<(unsigned)grid, L_THREADS, L_SMEM, stream>>>(
+          mA, mB, mC, m, n, k, C, ldc, sA, sB, tiles_m, tiles_n, tpc, status);
+      break;
+    case 1:
+      gemm_lp_kernel<true, false><<<(unsigned)grid, L_THREADS, L_SMEM, stream>>>(
+          mA, mB, mC, m, n, k, C, ldc, sA, sB, tiles_m, tiles_n, tpc, status);
+      break;
+    case 2:
+      gemm_lp_kernel<false, true><<<(unsigned)grid, L_THREADS, L_SMEM_TMA, stream>>>(
+          mA, mB, mC, m, n, k, C, ldc, sA, sB, tiles_m, tiles_n, tpc, status);
+      break;
+    default:
+      gemm_lp_kernel<true, true><<<(unsigned)grid, L_THREADS, L_SMEM_TMA, stream>>>(
+          mA, mB, mC, m, n, k, C, ldc, sA, sB, tiles_m, tiles_n, tpc, status);
+  }
   return cudaGetLastError();
 }
 

@@ -11,7 +11,10 @@ pytestmark = pytest.mark.gpu
                                    (1000, 513, 512), (4096, 2048, 512), (77, 1000, 128),
                                    (1500, 40, 256), (2048, 4096, 192)])
 @pytest.mark.parametrize("bf16", [True, False])
-def test_gemm_lp_matches_torch_fp32(hlib, m, n, k, bf16):
+@pytest.mark.parametrize("ldc_kind", ["odd", "aligned"])
+def test_gemm_lp_matches_torch_fp32(hlib, m, n, k, bf16, ldc_kind):
+    """ldc_kind "aligned" (a 16-byte leading dimension) takes the TMA
+    reduce-add epilogue, "odd" the epilogue that loads and stores C itself."""
     import torch
 
     g = torch.Generator(device="cpu").manual_seed(m + 3 * n + 7 * k + bf16)
@@ -22,7 +25,10 @@ def test_gemm_lp_matches_torch_fp32(hlib, m, n, k, bf16):
     tm, tn = (m + 127) // 128, (n + 255) // 256
     sA = (2.0 ** torch.randint(-3, 4, (tm,), generator=g).float()).cuda()
     sB = (2.0 ** torch.randint(-3, 4, (tn,), generator=g).float()).cuda()
-    ldc = m + 5
+    if ldc_kind == "aligned":
+        ldc = (m + 3) // 4 * 4 + 4
+    else:
+        ldc = m + 5 if (m + 5) % 4 else m + 6
     C = (torch.rand(n, ldc, generator=g) - 0.5).cuda()  # column-major C: C.T[:m]
     C0 = C.clone()
     hlib.gemm_lp_sub(bf16, m, n, k, A.data_ptr(), lda, B.data_ptr(), lda, sA.data_ptr(),
