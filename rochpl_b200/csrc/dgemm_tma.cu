@@ -2,7 +2,7 @@
 //
 // The hot kernel of the solve (rocblas_dgemm of src/pgesv/HPL_pdupdateTT.cpp:
 // 131-163).  The Tensor Memory Accelerator streams A and B k-slices into a
-// 6-deep shared memory ring with cp.async.bulk.tensor (no multicast), signalling "full"
+// 6-deep shared memory ring with cp.async.bulk.tensor (each CTA loads its own tiles), signalling "full"
 // mbarriers through the transaction count; eight warps wait on them and run
 // m16n8k8 f64 MMAs out of the swizzled tiles.  There is no dedicated producer
 // warp (a ninth warp would cap every warp at 168 registers): the warp that is

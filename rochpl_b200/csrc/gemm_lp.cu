@@ -14,7 +14,7 @@
 //   warp 0      TMA producer (both CTAs): its A and B halves of each 64-deep
 //               k-block (128-byte rows, 128B swizzle) into a 6-stage ring; the
 //               loads of both CTAs complete on CTA 0's "full" barrier, whose
-//               transaction count CTA 0 posts for the pair.  No multicast.
+//               transaction count CTA 0 posts for the pair; each CTA loads only its own halves.
 //   warp 1      allocates 512 TMEM columns in both CTAs (two accumulators,
 //               collectively for the pair); in CTA 0 one lane issues the MMAs
 //               and tcgen05.commit's with multicast to both CTAs' "empty" ring
