@@ -223,6 +223,46 @@ hplb_status hplb_batch_last_ms(const hplb_batch* b, double* ms);
  * may be NULL) receives every timing, -1 where a candidate does not fit. */
 hplb_status hplb_batch_tune(hplb_ctx* ctx, int nrhs, int* nb_by_class, double* ms_table);
 
+/* ---------------------------------------------------------------------------
+ * Building blocks of HPL_pdgesv on a 1 x Q process grid (P = 1, Q > 1; one
+ * process per GPU).  [A|b] is distributed in NB-wide column blocks, block c
+ * on process c mod Q (the block-cyclic layout of HPL_pdmatgen,
+ * src/matgen/HPL_pdmatgen.cpp:85-383, at P = 1); each process holds all n rows
+ * of its blocks in a local column-major array (local column lc of a block =
+ * its position among the process's blocks times NB).  Global row indices
+ * throughout.  The per-panel driver (factor on the owner, broadcast, update
+ * everywhere, then the distributed back-solve) is rochpl_b200/grid.py.
+ * ------------------------------------------------------------------------ */
+
+/* HPL_pdfact on the process that owns the panel (src/pfact/HPL_pdfact.cpp:20-110;
+ * at P = 1 the pivot search needs no other process): factor global rows
+ * [j, n) of local columns [lc, lc + jb) in place with the recursion and leaf
+ * of algo; d_ipiv (device, jb ints) receives the global rows swapped into rows
+ * j .. j + jb - 1.  A zero pivot sets *info to its global column (1-based) and
+ * returns HPLB_ERR_SINGULAR. */
+hplb_status hplb_panel_factor(hplb_ctx* ctx, const hplb_algo* algo, int n, int j, int jb,
+                              double* dA, int64_t ld, int lc, int* d_ipiv, int* info);
+
+/* HPL_pdupdateTT on one process's columns (src/pgesv/HPL_pdupdateTT.cpp:19-168,
+ * with the P = 1 row interchanges of src/pgesv/HPL_pdlaswp.cpp:300-389): the
+ * factored panel of global rows [j, n) in dL (leading dimension ldl >= n - j;
+ * row 0 of dL is global row j: unit lower L11 in its top jb rows, L21 below)
+ * with its pivots d_ipiv (device, jb global rows, each checked to lie in
+ * [j + k, n)), applied to local columns [c0, c0 + ncols) of dA: the
+ * interchanges, U12 = L11^-1 A12 in the top rows, A22 -= L21 U12. */
+hplb_status hplb_panel_update(hplb_ctx* ctx, int n, int j, int jb, const double* dL,
+                              int64_t ldl, const int* d_ipiv, double* dA, int64_t ld, int c0,
+                              int ncols);
+
+/* One block step of the distributed back-solve (HPL_pdtrsv,
+ * src/pgesv/HPL_pdtrsv_device.cpp:29-346) on the process owning the column
+ * block [j, j + jb) at local column lc: x[j : j+jb] = U_jj^-1 (y[j : j+jb] -
+ * s), then z[0 : j] += U[0 : j, block] x[j : j+jb].  dy, dx, dz: n doubles
+ * (device, global indexing); ds: jb doubles, the sum over all processes of
+ * their z[j : j+jb]. */
+hplb_status hplb_trsv_block(hplb_ctx* ctx, int n, int j, int jb, const double* dA, int64_t ld,
+                            int lc, const double* dy, const double* ds, double* dx, double* dz);
+
 /* The HPL residual check: dA must hold the regenerated [A|b] (hplb_matgen with
  * the seed of the solve), dX the solution.  Results go to *out (host). */
 hplb_status hplb_residual(hplb_ctx* ctx, int n, const double* dA, int64_t ld,

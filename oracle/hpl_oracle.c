@@ -377,6 +377,54 @@ static void rpanel(panel_t* P, int r0, int end, int c0, int N) {
   }
 }
 
+/* HPL_pdfact for one process of a 1 x Q grid (P = 1: the process holds every
+ * row of its columns): factor the panel of global rows [j, N) held in local
+ * columns [lc, lc + jb) of A, with the recursion and leaf of rpanel.  ipiv[k]
+ * (k < jb) receives the global row swapped into row j + k.  Returns the first
+ * zero-pivot global column (1-based), or 0.  src/pfact/HPL_pdfact.cpp:20-110. */
+int hplo_panel_factor(int N, int j, int jb, int nbmin, int ndiv, int pfact, int rfact,
+                      double* A, int64_t ld, int lc, int* ipiv) {
+  panel_t P;
+  memset(&P, 0, sizeof P);
+  int* piv = (int*)calloc((size_t)(lc + jb > 0 ? lc + jb : 1), sizeof(int));
+  P.A     = A;
+  P.ld    = ld;
+  P.nbmin = nbmin < 1 ? 1 : nbmin;
+  P.ndiv  = ndiv < 2 ? 2 : ndiv;
+  P.pfact = pfact;
+  P.rfact = rfact;
+  P.ipiv  = piv; /* indexed by local column */
+  P.pr    = j;
+  P.pc    = lc;
+  P.pw    = jb;
+  rpanel(&P, j, N, lc, jb);
+  for(int k = 0; k < jb; ++k) ipiv[k] = piv[lc + k];
+  free(piv);
+  return P.info ? j + (P.info - 1 - lc) + 1 : 0;
+}
+
+/* HPL_pdupdateTT for one process of a 1 x Q grid: the panel of global rows
+ * [j, N) (jb columns; L(i, k) is global row j + i, leading dimension ldl, unit
+ * lower L11 in its top jb rows, L21 below) with pivots ipiv (global rows),
+ * applied to local columns [c0, c0 + ncols) of A: the row interchanges in
+ * order, U12 = L11^-1 A12, A22 -= L21 U12.  The same operations, per column,
+ * as the single-process loop of hplo_pdgesv.  src/pgesv/HPL_pdupdateTT.cpp:91-163,
+ * src/pgesv/HPL_pdlaswp.cpp:300-389. */
+void hplo_panel_update(int N, int j, int jb, const double* L, int64_t ldl, const int* ipiv,
+                       double* A, int64_t ld, int c0, int ncols) {
+  for(int k = 0; k < jb; ++k) {
+    const int r = j + k, p = ipiv[k];
+    if(p == r) continue;
+    for(int c = c0; c < c0 + ncols; ++c) {
+      double t = A_(r, c);
+      A_(r, c) = A_(p, c);
+      A_(p, c) = t;
+    }
+  }
+  trsm_llu(jb, ncols, L, ldl, &A_(j, c0), ld);
+  gemm_sub(N - (j + jb), ncols, jb, L + jb, ldl, &A_(j, c0), ld, &A_(j + jb, c0), ld);
+}
+
 /* Single-process HPL_pdgesv: factor the N x (N+1) [A|b] in place (b in column
  * N), then back-solve U x = y into x.  ipiv[j] receives the global row that
  * was swapped into row j.  Returns info (first zero-pivot column, 1-based).

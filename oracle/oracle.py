@@ -49,6 +49,11 @@ def lib():
         L.hplo_use_blas.restype = C.c_int
         L.hplo_pdgesv.argtypes = [C.c_int] * 6 + [C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
         L.hplo_pdgesv.restype = C.c_int
+        L.hplo_panel_factor.argtypes = [C.c_int] * 7 + [C.c_void_p, C.c_int64, C.c_int,
+                                                        C.c_void_p]
+        L.hplo_panel_factor.restype = C.c_int
+        L.hplo_panel_update.argtypes = [C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int64,
+                                        C.c_void_p, C.c_void_p, C.c_int64, C.c_int, C.c_int]
         L.hplo_swapids.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_void_p]
         L.hplo_residual.argtypes = [C.c_int, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
         L.hplo_hpl_test.argtypes = [C.c_int] * 6 + [C.c_uint64, C.c_void_p, C.c_int64,

@@ -445,6 +445,98 @@ hplb_status hplb_residual_lcg(hplb_ctx* ctx, int n, uint64_t seed, const double*
   return residual_common(ctx, n, nullptr, 0, true, seed, dX, out);
 }
 
+// ---------------------------------------------------------------------------
+// Building blocks of the solve on a 1 x Q process grid (one process per GPU,
+// block-cyclic columns; the driver is rochpl_b200/grid.py).
+// ---------------------------------------------------------------------------
+
+hplb_status hplb_panel_factor(hplb_ctx* ctx, const hplb_algo* algo, int n, int j, int jb,
+                              double* dA, int64_t ld, int lc, int* d_ipiv, int* info) {
+  if(!ctx) return HPLB_ERR_ARG;
+  hplb_status s = check_algo(ctx, algo, n, ld, true);
+  if(s != HPLB_OK) return s;
+  if(j < 0 || jb < 1 || jb > 2048 || j + jb > n || lc < 0 || !dA || !d_ipiv)
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_panel_factor: bad panel (j %d, jb %d, lc %d, n %d)",
+                   j, jb, lc, n);
+  if(info) *info = 0;
+  ENTER(ctx);
+  if((s = ensure_solve_ws(ctx, n, std::max(algo->nb, jb), algo->nbmin)) != HPLB_OK) return s;
+  if((s = grow(ctx, &ctx->d_ipiv, &ctx->ipiv_cap, (size_t)std::max(n, lc + jb))) != HPLB_OK)
+    return s;
+  ctx->ev_next  = 0;
+  ctx->launches = 0;
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_pan));
+  Solve S{ctx, algo, dA, ld, n, {}, {}, {}};
+  if((s = S.rpanel(j, lc, jb, lc, jb)) != HPLB_OK) return s;
+  CK(cudaMemcpyAsync(d_ipiv, ctx->d_ipiv + lc, (size_t)jb * sizeof(int),
+                     cudaMemcpyDeviceToDevice, ctx->s_pan));
+  CK(cudaStreamSynchronize(ctx->s_pan));
+  int inf = 0;
+  if((s = read_status(ctx, &inf)) != HPLB_OK) return s;
+  if(inf != 0) {
+    const int col = j + (inf - 1 - lc) + 1;  // the leaf records local columns
+    if(info) *info = col;
+    return set_err(ctx, HPLB_ERR_SINGULAR, "zero pivot in column %d", col);
+  }
+  return HPLB_OK;
+}
+
+hplb_status hplb_panel_update(hplb_ctx* ctx, int n, int j, int jb, const double* dL,
+                              int64_t ldl, const int* d_ipiv, double* dA, int64_t ld, int c0,
+                              int ncols) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(n < 1 || j < 0 || jb < 1 || jb > 2048 || j + jb > n || ldl < n - j || ld < n || c0 < 0 ||
+     ncols < 0 || ncols > n + 1 || !dL || !d_ipiv || (ncols > 0 && !dA))
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_panel_update: bad argument");
+  if(ncols == 0) return HPLB_OK;
+  ENTER(ctx);
+  hplb_status s = ensure_solve_ws(ctx, n, jb, 1);
+  if(s != HPLB_OK) return s;
+  cudaStream_t st = ctx->s_upd;
+  // Pivots index rows: check them before any kernel uses them.
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), st));
+  CK(launch_check_ipiv_range(jb, j, n, d_ipiv, ctx->d_status, st));
+  CK(cudaStreamSynchronize(st));
+  int bad = 0;
+  if((s = read_status(ctx, &bad)) != HPLB_OK) return s;
+  if(bad) return set_err(ctx, HPLB_ERR_ARG, "hplb_panel_update: ipiv[%d] outside [%d, n)", bad - 1,
+                         j + bad - 1);
+  double* top = dA + (size_t)j + (size_t)c0 * (size_t)ld;
+  CK(launch_perm(d_ipiv, j, jb, ctx->d_perm[0], st));
+  CK(launch_diag_inv(dL, ldl, 0, 0, jb, ctx->d_dinv[0], st));
+  CK(launch_unit_lower_inverse(dL, ldl, jb, ctx->d_dinv[0], ctx->d_linv[0], jb, st));
+  CK(launch_laswp_gather(dA, ld, j, jb, ctx->d_perm[0], ctx->d_w, jb, c0, ncols, st));
+  CK(launch_dgemm_set(jb, ncols, jb, ctx->d_linv[0], jb, ctx->d_w, jb, top, ld, ctx->d_status,
+                      st));
+  if(n - j - jb > 0)
+    CK(launch_dgemm_sub(n - j - jb, ncols, jb, dL + jb, ldl, top, ld, top + jb, ld,
+                        ctx->d_status, st));
+  CK(cudaStreamSynchronize(st));
+  return read_status(ctx, nullptr);
+}
+
+hplb_status hplb_trsv_block(hplb_ctx* ctx, int n, int j, int jb, const double* dA, int64_t ld,
+                            int lc, const double* dy, const double* ds, double* dx, double* dz) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(n < 1 || j < 0 || jb < 1 || j + jb > n || lc < 0 || ld < n || !dA || !dy || !ds || !dx ||
+     !dz)
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_trsv_block: bad argument");
+  ENTER(ctx);
+  hplb_status s;
+  if((s = grow(ctx, &ctx->d_trsv, &ctx->trsv_cap, trsv_flag_ints(jb))) != HPLB_OK ||
+     (s = grow(ctx, &ctx->d_w, &ctx->w_cap, (size_t)jb)) != HPLB_OK)
+    return s;
+  cudaStream_t  st = ctx->s_upd;
+  const double* U  = dA + (size_t)lc * (size_t)ld;  // this block's columns, all rows
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), st));
+  CK(launch_vsub(jb, dy + j, ds, ctx->d_w, st));
+  int launches = 0;
+  CK(launch_trsv_y(U + j, ld, jb, ctx->d_w, dx + j, ctx->d_trsv, ctx->d_status, st, &launches));
+  CK(launch_gemv_acc(j, jb, U, ld, dx + j, dz, st));
+  CK(cudaStreamSynchronize(st));
+  return read_status(ctx, nullptr);
+}
+
 hplb_status hplb_last_timing(const hplb_ctx* ctx, hplb_timing* out) {
   if(!ctx || !out) return HPLB_ERR_ARG;
   *out = ctx->timing;

@@ -75,6 +75,13 @@ cudaError_t launch_laswp_gather(T* A, int64_t ld, int ia, int jb, const int* per
 size_t      trsv_flag_ints(int n);
 cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* flags, int* status,
                         cudaStream_t stream, int* launches);
+// The same back-solve with the right-hand side y in its own vector (n doubles).
+cudaError_t launch_trsv_y(const double* A, int64_t ld, int n, const double* Y, double* X,
+                          int* flags, int* status, cudaStream_t stream, int* launches);
+// z[0:m] += U[0:m, 0:k] x (U column-major, leading dimension ld); r = y - s.
+cudaError_t launch_gemv_acc(int m, int k, const double* U, int64_t ld, const double* x,
+                            double* z, cudaStream_t stream);
+cudaError_t launch_vsub(int n, const double* y, const double* s, double* r, cudaStream_t stream);
 
 // Residual check.  ws must hold residual_ws_doubles(n) doubles.
 size_t      residual_ws_doubles(int n);
@@ -171,6 +178,8 @@ cudaError_t launch_rank_k(int m, int n, int k, double alpha, const double* A, in
                           cudaStream_t st);
 // status[ST_INFO] = first i (1-based) with ipiv[i] outside [i, n), else untouched.
 cudaError_t launch_check_ipiv(int n, const int* ipiv, int* status, cudaStream_t st);
+cudaError_t launch_check_ipiv_range(int count, int first, int nrows, const int* ipiv,
+                                    int* status, cudaStream_t st);
 
 // Batched solver kernels (batch.cu); the plan and C ABI are in batch_api.cu.
 size_t      batch_static_smem();

@@ -307,9 +307,12 @@ __global__ void splitk_reduce_kernel(int jb, int nrhs, int nchunks, int ncb,
   }
 }
 
-__global__ void check_ipiv_kernel(int n, const int* __restrict__ ipiv, int* status) {
-  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-    if(ipiv[i] < i || ipiv[i] >= n) record_info(status, i + 1);
+// Entry i of ipiv (count entries) must lie in [first + i, nrows); the first
+// entry that does not is recorded 1-based in status[ST_INFO].
+__global__ void check_ipiv_kernel(int count, int first, int nrows, const int* __restrict__ ipiv,
+                                  int* status) {
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x)
+    if(ipiv[i] < first + i || ipiv[i] >= nrows) record_info(status, i + 1);
 }
 
 }  // namespace
@@ -403,11 +406,16 @@ cudaError_t launch_rows_sub(int m, int nrhs, int K, const double* M, int64_t ldm
   return cudaGetLastError();
 }
 
-cudaError_t launch_check_ipiv(int n, const int* ipiv, int* status, cudaStream_t st) {
-  if(n <= 0) return cudaSuccess;
-  check_ipiv_kernel<<<(n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024, 256, 0, st>>>(n, ipiv,
-                                                                                     status);
+cudaError_t launch_check_ipiv_range(int count, int first, int nrows, const int* ipiv,
+                                    int* status, cudaStream_t st) {
+  if(count <= 0) return cudaSuccess;
+  const int grid = (count + 255) / 256 < 1024 ? (count + 255) / 256 : 1024;
+  check_ipiv_kernel<<<grid, 256, 0, st>>>(count, first, nrows, ipiv, status);
   return cudaGetLastError();
+}
+
+cudaError_t launch_check_ipiv(int n, const int* ipiv, int* status, cudaStream_t st) {
+  return launch_check_ipiv_range(n, 0, n, ipiv, status, st);
 }
 
 }  // namespace hplb

@@ -1,6 +1,7 @@
 // Back-solve U x = y at P = Q = 1 (src/pgesv/HPL_pdtrsv_device.cpp:29-346).
 //
-// y is column n of the factored [A|b]; x is written to X; A is not modified.
+// y is column n of the factored [A|b] (or a vector of its own); x is written
+// to X; A and y are not modified.
 // The reference solves bottom-up in NB blocks: rocblas_dtrsv on the diagonal
 // block, then rocblas_dgemv to remove that block's contribution from every row
 // above, two serial library calls per block.  Here the whole solve is ONE
@@ -100,8 +101,8 @@ HPLB_DEV void invert_upper(TrsvSmem& S) {
 
 template <bool VEC>
 __global__ void __launch_bounds__(kTrsvThreads)
-trsv_kernel(const double* __restrict__ A, int64_t ld, int n, double* __restrict__ X, int* flags,
-            int* status) {
+trsv_kernel(const double* __restrict__ A, int64_t ld, int n, const double* __restrict__ Y,
+            double* __restrict__ X, int* flags, int* status) {
   __shared__ TrsvSmem S;
   const int nblk = (n + kTb - 1) / kTb;
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -125,7 +126,7 @@ trsv_kernel(const double* __restrict__ A, int64_t ld, int n, double* __restrict_
     if(r < kb && c < kb) v = r <= c ? A[(size_t)(r0 + r) + (size_t)(r0 + c) * (size_t)ld] : 0.0;
     S.T[r][c] = v;
   }
-  if(t < kTb) S.r[t] = t < kb ? A[(size_t)(r0 + t) + (size_t)n * (size_t)ld] : 0.0;
+  if(t < kTb) S.r[t] = t < kb ? Y[r0 + t] : 0.0;
   __syncthreads();
   invert_upper(S);
 
@@ -175,21 +176,67 @@ trsv_kernel(const double* __restrict__ A, int64_t ld, int n, double* __restrict_
   if(t == 0) st_release_gpu(flags + bi, 1);
 }
 
+// z[r] += sum_c U[r, c] x[c] for r < m, c < k: a thread per row (coalesced
+// down each column), x staged in shared memory in chunks of 1024.
+__global__ void __launch_bounds__(256)
+gemv_acc_kernel(int m, int k, const double* __restrict__ U, int64_t ld,
+                const double* __restrict__ x, double* __restrict__ z) {
+  __shared__ double xs[1024];
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double    acc = 0.0;
+  for(int c0 = 0; c0 < k; c0 += 1024) {
+    const int kc = min(1024, k - c0);
+    __syncthreads();
+    for(int i = threadIdx.x; i < kc; i += blockDim.x) xs[i] = x[c0 + i];
+    __syncthreads();
+    if(r < m) {
+      const double* u = U + (size_t)r + (size_t)c0 * (size_t)ld;
+#pragma unroll 8
+      for(int c = 0; c < kc; ++c) acc = fma(u[(size_t)c * (size_t)ld], xs[c], acc);
+    }
+  }
+  if(r < m) z[r] += acc;
+}
+
+__global__ void vsub_kernel(int n, const double* __restrict__ y, const double* __restrict__ s,
+                            double* __restrict__ r) {
+  for(int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    r[i] = y[i] - s[i];
+}
+
 }  // namespace
 
 size_t trsv_flag_ints(int n) { return (size_t)(n + kTb - 1) / kTb + 1; }
 
+cudaError_t launch_gemv_acc(int m, int k, const double* U, int64_t ld, const double* x,
+                            double* z, cudaStream_t stream) {
+  if(m <= 0 || k <= 0) return cudaSuccess;
+  gemv_acc_kernel<<<(m + 255) / 256, 256, 0, stream>>>(m, k, U, ld, x, z);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_vsub(int n, const double* y, const double* s, double* r, cudaStream_t stream) {
+  if(n <= 0) return cudaSuccess;
+  vsub_kernel<<<(n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024, 256, 0, stream>>>(n, y, s, r);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* flags, int* status,
                         cudaStream_t stream, int* launches) {
+  return launch_trsv_y(A, ld, n, A + (size_t)n * (size_t)ld, X, flags, status, stream, launches);
+}
+
+cudaError_t launch_trsv_y(const double* A, int64_t ld, int n, const double* Y, double* X,
+                          int* flags, int* status, cudaStream_t stream, int* launches) {
   if(n <= 0) return cudaSuccess;
   const int   nblk = (n + kTb - 1) / kTb;
   cudaError_t e    = cudaMemsetAsync(flags, 0, trsv_flag_ints(n) * sizeof(int), stream);
   if(e != cudaSuccess) return e;
   const bool vec = (reinterpret_cast<uintptr_t>(A) % 16 == 0) && (ld % 2 == 0);
   if(vec)
-    trsv_kernel<true><<<nblk, kTrsvThreads, 0, stream>>>(A, ld, n, X, flags, status);
+    trsv_kernel<true><<<nblk, kTrsvThreads, 0, stream>>>(A, ld, n, Y, X, flags, status);
   else
-    trsv_kernel<false><<<nblk, kTrsvThreads, 0, stream>>>(A, ld, n, X, flags, status);
+    trsv_kernel<false><<<nblk, kTrsvThreads, 0, stream>>>(A, ld, n, Y, X, flags, status);
   ++*launches;
   return cudaGetLastError();
 }

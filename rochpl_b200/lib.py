@@ -30,6 +30,7 @@ EXPORTS = [
     "hplb_set_stream", "hplb_set_option", "hplb_batch_create", "hplb_batch_destroy", "hplb_batch_layout",
     "hplb_batch_matgen", "hplb_batch_gesv", "hplb_batch_getrs", "hplb_batch_rank_k",
     "hplb_batch_residual", "hplb_batch_last_ms", "hplb_batch_tune",
+    "hplb_panel_factor", "hplb_panel_update", "hplb_trsv_block",
 ]
 
 HPLB_BATCH_CLASSES = 6
@@ -148,6 +149,13 @@ def load() -> C.CDLL:
     L.hplb_getrf.restype = i32
     L.hplb_getrs.argtypes = [vp, i32, i32, i32, i32, vp, i64, vp, vp, i64]
     L.hplb_getrs.restype = i32
+    L.hplb_panel_factor.argtypes = [vp, C.POINTER(hplb_algo), i32, i32, i32, vp, i64, i32, vp,
+                                    C.POINTER(C.c_int)]
+    L.hplb_panel_factor.restype = i32
+    L.hplb_panel_update.argtypes = [vp, i32, i32, i32, vp, i64, vp, vp, i64, i32, i32]
+    L.hplb_panel_update.restype = i32
+    L.hplb_trsv_block.argtypes = [vp, i32, i32, i32, vp, i64, i32, vp, vp, vp, vp]
+    L.hplb_trsv_block.restype = i32
     L.hplb_rank_k.argtypes = [vp, i32, i32, i32, C.c_double, vp, i64, vp, i64, vp, i64, i32]
     L.hplb_rank_k.restype = i32
     for name in ("hplb_fp64_peak", "hplb_selftest_wait_timeout", "hplb_matgen", "hplb_pdgesv", "hplb_residual", "hplb_residual_lcg",
@@ -251,6 +259,24 @@ class Library:
         r = hplb_resid()
         self._check(self.L.hplb_residual_lcg(self.ctx, n, seed, X, C.byref(r)))
         return {k: getattr(r, k) for k, _ in hplb_resid._fields_}
+
+    def panel_factor(self, algo: hplb_algo, n: int, j: int, jb: int, A: int, ld: int, lc: int,
+                     ipiv: int) -> int:
+        """hplb_panel_factor; returns info (0, or the zero pivot's global column)."""
+        info = C.c_int(0)
+        st = self.L.hplb_panel_factor(self.ctx, C.byref(algo), n, j, jb, A, ld, lc, ipiv,
+                                      C.byref(info))
+        self._check(st, allow=(HPLB_OK, HPLB_ERR_SINGULAR))
+        return info.value
+
+    def panel_update(self, n: int, j: int, jb: int, Lp: int, ldl: int, ipiv: int, A: int,
+                     ld: int, c0: int, ncols: int):
+        self._check(self.L.hplb_panel_update(self.ctx, n, j, jb, Lp, ldl, ipiv, A, ld, c0,
+                                             ncols))
+
+    def trsv_block(self, n: int, j: int, jb: int, A: int, ld: int, lc: int, y: int, s: int,
+                   x: int, z: int):
+        self._check(self.L.hplb_trsv_block(self.ctx, n, j, jb, A, ld, lc, y, s, x, z))
 
     def last_timing(self) -> dict:
         t = hplb_timing()
