@@ -33,8 +33,9 @@ systems with N in [64, 512] through the batched form) go under "batched" and
 "autograd" (the N = 16384 gradients are checked against torch's FP64 solve
 and against central differences with step 1e-6).
 
-Multi-GPU runs are replicas (each rank solves its own system; P = Q = 1 has
-no inter-GPU data path), reported as weak scaling.
+Multi-GPU runs are replicas for the headline (each rank solves its own system,
+reported as weak scaling); with --gpus N > 1 a further leg ("grid") solves ONE
+N = 131072 system across all N GPUs on a 1 x N process grid (strong scaling).
 
 --impl reference times the reference algorithm's CPU restatement (the oracle,
 host OpenBLAS on every host core): N = 16384 on every step and N = 32768 once,
@@ -315,6 +316,12 @@ def run_ours(args):
         if args.mixed_sizes:
             mixed["by_n"] = mixed_sizes_leg(lib, args, seed, barrier, max_over_ranks)
 
+    grid = None
+    if world > 1 and not args.no_grid:
+        dA = None
+        torch.cuda.empty_cache()
+        grid = grid_leg(lib, args, ranks)
+
     batched = None if args.no_batched else batched_leg(lib, args, ranks)
     autograd = None if args.no_autograd else autograd_leg(lib, args, max_over_ranks)
 
@@ -355,6 +362,8 @@ def run_ours(args):
             line["e2e"] = e2e
         if mixed is not None:
             line["mixed"] = mixed
+        if grid is not None:
+            line["grid"] = grid
         if batched is not None:
             line["batched"] = batched
         if autograd is not None:
@@ -598,6 +607,46 @@ def mixed_sizes_leg(lib, args, seed, barrier, max_over_ranks) -> dict:
         out[str(n)] = rec
         torch.cuda.empty_cache()
     return out
+
+
+def grid_leg(lib, args, ranks) -> dict:
+    """One system across all ranks: HPL_pdgesv on a 1 x world process grid
+    (rochpl_b200.grid; NB-wide column blocks cyclic over the GPUs, the panel
+    broadcast over NCCL), N = args.grid_n, seed 100.  Device time from CUDA
+    events around the whole solve, max over ranks; the residual against the
+    regenerated LCG matrix on rank 0."""
+    import torch
+
+    from rochpl_b200.grid import DeviceBackend, DistGroup, Grid1xQ, matgen_local, pdgesv_grid
+    from rochpl_b200.hpl import Algo, default_ld
+
+    n, nb = args.grid_n, args.nb
+    algo = Algo(nb, 32, 2, 2, 2, 1, 0)
+    g = Grid1xQ(n, nb, ranks.rank, ranks.world)
+    ld = default_ld(n)
+    be, comm = DeviceBackend(lib), DistGroup()
+    A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64, device="cuda")
+    ms = []
+    for it in range(1 + args.grid_steps):
+        matgen_local(be, g, 100, A, ld)
+        torch.cuda.synchronize()
+        ranks.barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        x, ipiv, info = pdgesv_grid(be, comm, g, algo, A, ld)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= 1:
+            ms.append(e0.elapsed_time(e1))
+    t = ranks.max(statistics.mean(ms))
+    res = lib.residual_lcg(n, 100, x.data_ptr()) if ranks.rank == 0 else {"resid": None}
+    del A
+    torch.cuda.empty_cache()
+    return {"workload": f"one HPL system N={n} NB={nb} on a 1 x {ranks.world} process grid "
+                        "(column blocks cyclic over the GPUs, panel broadcast over NCCL)",
+            "scaling": "strong (one system)", "ms_per_solve": t,
+            "value": hpl_flops(n) / (t * 1e-3) / 1e12, "unit": UNIT, "info": info,
+            "resid": res["resid"], "steps": args.grid_steps}
 
 
 def batched_leg(lib, args, ranks):
@@ -1047,6 +1096,10 @@ def main():
     ap.add_argument("--no-parity", action="store_true",
                     help="skip the LCG, parity-solve and gradient checks")
     ap.add_argument("--no-c1", action="store_true", help="skip the N = 4096 config line")
+    ap.add_argument("--no-grid", action="store_true",
+                    help="skip the one-system-across-all-GPUs leg (runs only with --gpus > 1)")
+    ap.add_argument("--grid-n", type=int, default=131072)
+    ap.add_argument("--grid-steps", type=int, default=1)
     ap.add_argument("--mixed-sizes", type=lambda v: [int(x) for x in v.split(",") if x],
                     default=[32768, 65536],
                     help="further N of the mixed-precision form (comma list; empty to skip)")

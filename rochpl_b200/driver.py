@@ -12,12 +12,16 @@
   progress    the per-step report of src/pgesv/HPL_pdgesv.cpp:136-341
               (HPL_PROGRESS_REPORT), from hplb_last_steps
 
-Grids other than 1 x 1 are counted as skipped tests: this library is the
-single-process solve.  The solve itself, the generator and the residual run on
-the GPU through libhplb200.so (GpuSolver); the driver only formats and counts,
-so its loops and output are tested with a stand-in solver on the CPU.
+One process runs the 1 x 1 grids (GpuSolver).  Launched as W processes (one
+per GPU, torchrun), the driver runs the 1 x W grids as one distributed solve
+(GridSolver: rochpl_b200.grid, NB-wide column blocks cyclic over the GPUs,
+the panel broadcast over NCCL) and rank 0 writes the output.  Other grids are
+counted as skipped tests.  The solve itself, the generator and the residual run
+on the GPU through libhplb200.so; the driver only formats and counts, so its
+loops and output are tested with a stand-in solver on the CPU.
 
     python -m rochpl_b200.driver [-N 45312] [-NB 384] [-it 1] [-i HPL.dat] [--progress]
+    torchrun --nproc-per-node Q -m rochpl_b200.driver -N 65536 -NB 512 -P 1 -Q Q
 """
 from __future__ import annotations
 
@@ -132,10 +136,11 @@ def sweep(cfg: HplConfig):
                                                                 cfg.l1notran)
 
 
-def skipped(p: int, q: int, algo: Algo) -> bool:
-    """Tests this driver counts as skipped: grids beyond one process, and
-    values the library does not take (NBMIN > 128, NB > 2048, DEPTH != 1)."""
-    return p * q != 1 or algo.nbmin > 128 or algo.nb > 2048 or algo.depth != 1
+def skipped(p: int, q: int, algo: Algo, world: int = 1) -> bool:
+    """Tests this driver counts as skipped: grids other than 1 x (the number
+    of processes), and values the library does not take (NBMIN > 128,
+    NB > 2048, DEPTH != 1)."""
+    return p != 1 or q != world or algo.nbmin > 128 or algo.nb > 2048 or algo.depth != 1
 
 
 class GpuSolver:
@@ -196,7 +201,66 @@ class GpuSolver:
         return out
 
 
-def run(cfg: HplConfig, out=None, solver=None, progress: bool = False) -> dict:
+class GridSolver:
+    """This process's part of one system on the 1 x W grid of all processes
+    (torch.distributed already initialised, one GPU each).  The solve is timed
+    by the wall clock between two barriers, the slowest process's time (as
+    HPL_ptimer_combine takes the maximum); the residual is computed on rank 0
+    against the regenerated matrix."""
+
+    def __init__(self, device: int = 0):
+        import torch
+        import torch.distributed as dist
+
+        from .grid import DeviceBackend, DistGroup
+        from .lib import library
+
+        self.torch, self.dist = torch, dist
+        self.device = device
+        self.lib = library(device)
+        self.backend = DeviceBackend(self.lib)
+        self.comm = DistGroup()
+        self.rank, self.world = dist.get_rank(), dist.get_world_size()
+
+    def _solve(self, algo: Algo, n: int, seed: int):
+        from .grid import Grid1xQ, matgen_local, pdgesv_grid
+
+        torch = self.torch
+        g = Grid1xQ(n, algo.nb, self.rank, self.world)
+        ld = default_ld(n)
+        A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64,
+                        device=torch.device("cuda", self.device))
+        matgen_local(self.backend, g, seed, A, ld)
+        torch.cuda.synchronize(self.device)
+        self.dist.barrier()
+        t_start = time.time()
+        t0 = time.perf_counter()
+        x, ipiv, info = pdgesv_grid(self.backend, self.comm, g, algo, A, ld)
+        torch.cuda.synchronize(self.device)
+        w = torch.tensor([time.perf_counter() - t0], dtype=torch.float64,
+                         device=torch.device("cuda", self.device))
+        self.dist.all_reduce(w, op=self.dist.ReduceOp.MAX)
+        return x, info, float(w.item()), t_start, time.time()
+
+    def warmup(self, algo: Algo, n: int) -> None:
+        self._solve(algo, min(n, 2 * algo.nb * self.world + 1), HPL_ISEED)
+
+    def __call__(self, algo: Algo, n: int, seed: int = HPL_ISEED, progress: bool = False) -> dict:
+        x, info, wtime, t_start, t_end = self._solve(algo, n, seed)
+        res = (self.lib.residual_lcg(n, seed, x.data_ptr()) if self.rank == 0 else
+               {"resid": 0.0})
+        return {"wtime": wtime, "t_start": t_start, "t_end": t_end, "info": info, **res}
+
+
+class _Discard:
+    def write(self, s):
+        return len(s)
+
+    def flush(self):
+        return None
+
+
+def run(cfg: HplConfig, out=None, solver=None, progress: bool = False, world: int = 1) -> dict:
     """Run every test of the sweep; write the reference's output to `out`
     (default stdout); return the tally.  `solver(algo, n, progress=...)` returns
     a dict with wtime, t_start, t_end, resid and the norms (GpuSolver by
@@ -206,7 +270,7 @@ def run(cfg: HplConfig, out=None, solver=None, progress: bool = False) -> dict:
     kpass = kfail = kskip = 0
     first = True
     for n, p, q, bc, algo in sweep(cfg):
-        if skipped(p, q, algo):
+        if skipped(p, q, algo, world):
             kskip += 1
             continue
         warm = getattr(solver, "warmup", None)
@@ -260,11 +324,30 @@ def main(argv=None) -> int:
     except HplInputError as e:
         print(e, file=sys.stderr)
         return 1
-    if cfg.outfile:
-        with open(cfg.outfile, "w") as f:
-            tally = run(cfg, f, progress=progress)
-    else:
-        tally = run(cfg, sys.stdout, progress=progress)
+    import os
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    solver, rank = None, 0
+    if world > 1:  # one process per GPU under torchrun: the 1 x world grids
+        import torch
+        import torch.distributed as dist
+
+        rank, local = int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+        solver = GridSolver(local)
+    try:
+        if rank != 0:
+            tally = run(cfg, _Discard(), solver=solver, world=world)
+        elif cfg.outfile:
+            with open(cfg.outfile, "w") as f:
+                tally = run(cfg, f, solver=solver, progress=progress, world=world)
+        else:
+            tally = run(cfg, sys.stdout, solver=solver, progress=progress and world == 1,
+                        world=world)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
     return 0 if tally["failed"] == 0 else 2
 
 

@@ -148,3 +148,14 @@ def test_hpl_dat_drives_the_sweep():
     assert tally == {"passed": 4, "failed": 0, "skipped": 4}
     codes = [ln.split()[0] for ln in out.getvalue().splitlines() if ln.startswith("WR")]
     assert codes == ["WR10C2R16", "WR13C2R16"] * 2
+
+
+def test_grids_run_when_they_match_the_process_count():
+    """Under W processes the driver runs the 1 x W grids and skips the rest
+    (1 x 1 with W = 1, as before)."""
+    cfg = HplConfig(ns=[100], nbs=[32], ps=[1, 1, 2, 1], qs=[1, 2, 1, 4])
+    for world, runs in ((1, 1), (2, 1), (4, 1), (3, 0)):
+        s = FakeSolver()
+        tally = run(cfg, io.StringIO(), solver=s, world=world)
+        assert tally == {"passed": runs, "failed": 0, "skipped": 4 - runs}, world
+        assert len(s.calls) == runs
