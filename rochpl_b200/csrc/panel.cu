@@ -510,11 +510,53 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
 }
 
 // Apply the w interchanges of leaf columns [c0, c0+w) to the panel columns
-// outside the leaf, in order.  One thread per column.
+// outside the leaf, one thread per column.  For w <= 32 the interchange
+// sequence is traced once per block into a row map (src[x]: the row whose
+// value ends in row r0 + x; dst[x]: where the old row r0 + x ends when it
+// leaves the top w rows, else -1), and every column then reads all the rows it
+// needs before writing any, so its w reads are in flight together instead of
+// forming a chain of w dependent swaps.  Wider leaves swap in order.
 template <typename T>
 __global__ void panel_swap_kernel(T* A, int64_t ld, const int* ipiv, int r0, int c0,
                                   int w, int pc, int pw) {
+  constexpr int kMap = 32;
+  __shared__ int s_src[kMap], s_dst[kMap];
   const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if(w <= kMap) {
+    if(threadIdx.x < w) {
+      const int x = threadIdx.x;
+      int       pos = x;
+      for(int i = w - 1; i >= 0; --i) {
+        const int p = ipiv[c0 + i] - r0;
+        pos         = (pos == i) ? p : (pos == p ? i : pos);
+      }
+      s_src[x] = pos;
+      pos      = x;
+      for(int i = 0; i < w; ++i) {
+        const int p = ipiv[c0 + i] - r0;
+        pos         = (pos == i) ? p : (pos == p ? i : pos);
+      }
+      s_dst[x] = pos >= w ? pos : -1;
+    }
+    __syncthreads();
+    if(j >= pw - w) return;
+    const int col = (pc + j < c0) ? pc + j : pc + j + w;
+    T*        a   = A + (size_t)col * ld + r0;
+    T         v[kMap], o[kMap];
+#pragma unroll
+    for(int x = 0; x < kMap; ++x)
+      if(x < w) {
+        v[x] = a[s_src[x]];
+        o[x] = s_dst[x] >= 0 ? a[x] : (T)0;
+      }
+#pragma unroll
+    for(int x = 0; x < kMap; ++x)
+      if(x < w && s_dst[x] >= 0) a[s_dst[x]] = o[x];
+#pragma unroll
+    for(int x = 0; x < kMap; ++x)
+      if(x < w) a[x] = v[x];
+    return;
+  }
   if(j >= pw - w) return;
   const int col = (pc + j < c0) ? pc + j : pc + j + w;
   T*        a   = A + (size_t)col * ld;
