@@ -92,16 +92,19 @@ hplb_status hplb_set_stream(hplb_ctx* ctx, void* stream);
 
 /* Per-context options (no counterpart in the reference).
  *   HPLB_OPT_LEAF: where the panel leaf keeps the rows of its NBMIN-wide slice
- *   while it factors it -- HPLB_LEAF_AUTO (default: registers, else shared
- *   memory, else global memory, the first that holds the slice on the GPU at
- *   once), HPLB_LEAF_SHARED (shared memory first) or HPLB_LEAF_GLOBAL.  The
- *   three perform the same operations in the same order and give identical
- *   results; the choice only moves time.  The rocHPL leaf keeps its slice in
- *   global memory (src/pfact/HPL_pdpanrlT_device.cpp:23-320). */
+ *   while it factors it -- HPLB_LEAF_AUTO (default: in the registers of one
+ *   thread-block cluster of up to 16 SMs when the slice fits there, else in
+ *   registers across the GPU, else shared memory, else global memory),
+ *   HPLB_LEAF_REGISTERS (registers across the GPU first, never the cluster),
+ *   HPLB_LEAF_SHARED (shared memory first) or HPLB_LEAF_GLOBAL.  All perform
+ *   the same operations in the same order and give identical results; the
+ *   choice only moves time.  The rocHPL leaf keeps its slice in global memory
+ *   (src/pfact/HPL_pdpanrlT_device.cpp:23-320). */
 #define HPLB_OPT_LEAF 1
 #define HPLB_LEAF_AUTO 0
 #define HPLB_LEAF_SHARED 1
 #define HPLB_LEAF_GLOBAL 2
+#define HPLB_LEAF_REGISTERS 3
 hplb_status hplb_set_option(hplb_ctx* ctx, int option, int value);
 
 const char* hplb_status_string(hplb_status s);

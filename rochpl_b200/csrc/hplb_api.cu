@@ -205,7 +205,7 @@ hplb_status hplb_set_option(hplb_ctx* ctx, int option, int value) {
   if(!ctx) return HPLB_ERR_ARG;
   switch(option) {
     case HPLB_OPT_LEAF:
-      if(value < HPLB_LEAF_AUTO || value > HPLB_LEAF_GLOBAL)
+      if(value < HPLB_LEAF_AUTO || value > HPLB_LEAF_REGISTERS)
         return set_err(ctx, HPLB_ERR_ARG, "hplb_set_option: leaf kind %d out of range", value);
       ctx->leaf_kind = value;
       return HPLB_OK;

@@ -509,6 +509,169 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
         if(c < w) P.A[(size_t)row[q] + (size_t)(P.c0 + c) * ld] = x[q][c];
 }
 
+// The register leaf on ONE thread-block cluster (up to 16 CTAs, one per SM,
+// co-scheduled by the hardware): the rows stay in registers exactly as in
+// leaf_reg_kernel and every column performs the same operations in the same
+// order (hence the same bits), but the exchange per column is on chip:
+//   * each CTA's candidate (value, row) and its candidate row's leaf values go
+//     to its own shared memory, the diagonal row to its owner's, in one of two
+//     buffers by column parity;
+//   * one hardware cluster barrier (arrive.release / wait.acquire) replaces
+//     the grid-wide atomic barrier;
+//   * warp 0 of every CTA reads the G candidates, then the winning row and the
+//     diagonal row, from the peers' shared memory (ld.shared::cluster).
+// A CTA writes buffer k & 1 only after the barrier of column k - 1, which
+// every peer reaches after its last read of buffer (k - 2) & 1, so one barrier
+// per column suffices; a last barrier keeps every CTA resident until its
+// peers' final reads are done.  No wait here is a spin on memory.
+HPLB_DEV unsigned cluster_ctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+HPLB_DEV unsigned cluster_nctarank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+HPLB_DEV void cluster_barrier() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n"
+               "barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// A double in CTA `rank`'s shared memory at the offset of `local`.
+HPLB_DEV double ld_peer(const double* local, unsigned rank) {
+  uint32_t a = (uint32_t)__cvta_generic_to_shared(local), r;
+  double   v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(a), "r"(rank));
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(r) : "memory");
+  return v;
+}
+
+constexpr int kClusterLeafMax = 16;  // CTAs per cluster at most (non-portable above 8)
+
+template <typename T, int RPT>
+__global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafParams<T> P) {
+  __shared__ double s_v[32];
+  __shared__ int    s_r[32];
+  __shared__ double s_slot[2][2 + kRegLeafW];  // (value, row, candidate row) per parity
+  __shared__ double s_diag[2][kRegLeafW];      // the diagonal row, on its owner
+  __shared__ double s_u[kRegLeafW];
+  __shared__ double s_cur[kRegLeafW];
+  __shared__ double s_piv;
+  __shared__ int    s_p;
+
+  const unsigned G    = cluster_nctarank();
+  const unsigned me   = cluster_ctarank();
+  const int      lane = threadIdx.x & 31;
+  const int      lo   = P.r0 + (int)me * P.rpb;
+  const size_t   ld   = (size_t)P.ld;
+  const int      w    = P.w;
+
+  T   x[RPT][kRegLeafW];
+  int row[RPT];
+#pragma unroll
+  for(int q = 0; q < RPT; ++q) {
+    row[q]         = lo + threadIdx.x + q * blockDim.x;
+    const bool in  = row[q] < P.end && threadIdx.x + q * blockDim.x < P.rpb;
+    if(!in) row[q] = -1;
+#pragma unroll
+    for(int c = 0; c < kRegLeafW; ++c)
+      x[q][c] = (in && c < w) ? P.A[(size_t)row[q] + (size_t)(P.c0 + c) * ld] : (T)0;
+  }
+
+#pragma unroll 1
+  for(int k = 0; k < w; ++k) {
+    const int par = k & 1;
+    const int d   = P.r0 + k;
+    double v = 0.0;
+    int    r = -1;
+#pragma unroll
+    for(int q = 0; q < RPT; ++q) {
+      const double xk = (double)pick_col(x[q], k);
+      if(row[q] >= d && better(xk, row[q], v, r)) {
+        v = xk;
+        r = row[q];
+      }
+    }
+    block_argmax(v, r, s_v, s_r);
+    if(threadIdx.x == 0) {
+      s_slot[par][0] = v;
+      s_slot[par][1] = (double)r;
+    }
+#pragma unroll
+    for(int q = 0; q < RPT; ++q) {
+      if(r >= 0 && row[q] == r)
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c)
+          if(c < w) s_slot[par][2 + c] = (double)x[q][c];
+      if(row[q] == d)
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c)
+          if(c < w) s_diag[par][c] = (double)x[q][c];
+    }
+    cluster_barrier();
+
+    if(threadIdx.x < 32) {
+      double bv = 0.0;
+      int    br = -1;
+      if(lane < (int)G) {
+        bv = ld_peer(&s_slot[par][0], (unsigned)lane);
+        br = (int)ld_peer(&s_slot[par][1], (unsigned)lane);
+      }
+      const int wl = warp_argmax(bv, br);
+      int       bs = wl < 0 ? 0 : wl;  // the winning CTA
+      if(wl < 0) {  // unreachable while the leaf has rows >= d; keeps reads in bounds
+        bv = 0.0;
+        br = d;
+      }
+      if(threadIdx.x == 0) {
+        s_piv = bv;
+        s_p   = br;
+      }
+      const unsigned owner = (unsigned)min((int)G - 1, (d - P.r0) / P.rpb);
+      if(lane < w) {
+        s_u[lane]   = ld_peer(&s_slot[par][2 + lane], (unsigned)bs);
+        s_cur[lane] = ld_peer(&s_diag[par][lane], owner);
+      }
+    }
+    __syncthreads();
+    const T   piv = (T)s_piv;
+    const int p   = s_p;
+    if(me == 0 && threadIdx.x == 0) {
+      P.ipiv[P.c0 + k] = p;
+      if(piv == (T)0) record_info(P.status, P.c0 + k + 1);
+    }
+#pragma unroll
+    for(int q = 0; q < RPT; ++q) {
+      if(row[q] == d) {
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_u[c];
+      } else if(row[q] == p) {
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_cur[c];
+      }
+      if(row[q] > d) {
+        const T l = pick_col(x[q], k) / piv;
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) {
+          if(c == k)
+            x[q][c] = l;
+          else if(c > k)
+            x[q][c] = x[q][c] - l * (T)s_u[c];
+        }
+      }
+    }
+  }
+  cluster_barrier();
+
+#pragma unroll
+  for(int q = 0; q < RPT; ++q)
+    if(row[q] >= 0)
+#pragma unroll
+      for(int c = 0; c < kRegLeafW; ++c)
+        if(c < w) P.A[(size_t)row[q] + (size_t)(P.c0 + c) * ld] = x[q][c];
+}
+
 // Apply the w interchanges of leaf columns [c0, c0+w) to the panel columns
 // outside the leaf, one thread per column.  For w <= 32 the interchange
 // sequence is traced once per block into a row map (src[x]: the row whose
@@ -672,8 +835,21 @@ laswp_trsm_kernel(T* A, int64_t ld, int ia, int jb, const T* L, int64_t ldl,
     for(int q = 0; q < CPT; ++q) acc[q] = (T)0;
     const int gr = row0 + r;
     if(gr < jb) {
+      // Row gr of L from global memory, 16 loads in flight before their FMAs
+      // (the sum still runs over kk in order, so the bits do not change).
       const T* Lrow = L + (size_t)gr;
-      for(int kk = 0; kk < row0; ++kk) {
+      int      kk   = 0;
+      for(; kk + 16 <= row0; kk += 16) {
+        T l[16];
+#pragma unroll
+        for(int u = 0; u < 16; ++u) l[u] = Lrow[(size_t)(kk + u) * (size_t)ldl];
+#pragma unroll
+        for(int u = 0; u < 16; ++u)
+#pragma unroll
+          for(int q = 0; q < CPT; ++q)
+            acc[q] += l[u] * sx[(size_t)(cg * CPT + q) * ldx + kk + u];
+      }
+      for(; kk < row0; ++kk) {
         const T l = Lrow[(size_t)kk * (size_t)ldl];
 #pragma unroll
         for(int q = 0; q < CPT; ++q) acc[q] += l * sx[(size_t)(cg * CPT + q) * ldx + kk];
@@ -696,10 +872,16 @@ laswp_trsm_kernel(T* A, int64_t ld, int ia, int jb, const T* L, int64_t ldl,
     const T* D = dinv + (size_t)b * kTri * kTri;
 #pragma unroll
     for(int q = 0; q < CPT; ++q) acc[q] = (T)0;
-    for(int kk = 0; kk < kTri && row0 + kk < jb; ++kk) {
-      const T dv = D[(size_t)kk * kTri + r];
+    {
+      T dv[kTri];  // row r of Dinv_b, all loads in flight at once
 #pragma unroll
-      for(int q = 0; q < CPT; ++q) acc[q] += dv * sx[(size_t)(cg * CPT + q) * ldx + row0 + kk];
+      for(int kk = 0; kk < kTri; ++kk) dv[kk] = D[(size_t)kk * kTri + r];
+#pragma unroll
+      for(int kk = 0; kk < kTri; ++kk)
+        if(row0 + kk < jb)
+#pragma unroll
+          for(int q = 0; q < CPT; ++q)
+            acc[q] += dv[kk] * sx[(size_t)(cg * CPT + q) * ldx + row0 + kk];
     }
     __syncthreads();
 #pragma unroll
@@ -843,17 +1025,102 @@ static cudaError_t try_leaf_reg(const LeafParams<T>& P, int rows, int sms, int g
   return cudaSuccess;
 }
 
+// The cluster leaf with RPT rows per thread on g CTAs.  Whether a cluster of g
+// such CTAs can be placed at all is asked once per (type, RPT, g); a launch
+// that cannot be placed, or fails, falls through to the next leaf kind.
+template <typename T, int RPT>
+static cudaError_t launch_leaf_cluster(LeafParams<T> P, int g, cudaStream_t stream, bool* done) {
+  static signed char placeable[kClusterLeafMax + 1] = {};  // 0 unknown, 1 yes, -1 no
+  *done = false;
+  if(g < 1 || g > kClusterLeafMax) return cudaSuccess;
+  P.rpb = RPT * kRegLeafThreads;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim  = dim3((unsigned)g);
+  cfg.blockDim = dim3(kRegLeafThreads);
+  cfg.stream   = stream;
+  cudaLaunchAttribute at[1];
+  at[0].id               = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)g;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs              = at;
+  cfg.numAttrs           = 1;
+  if(placeable[g] == 0) {
+    int n = 0;
+    if(g > 8 && cudaFuncSetAttribute((const void*)leaf_cluster_kernel<T, RPT>,
+                                     cudaFuncAttributeNonPortableClusterSizeAllowed,
+                                     1) != cudaSuccess) {
+      cudaGetLastError();
+      placeable[g] = -1;
+    } else if(cudaOccupancyMaxActiveClusters(&n, (const void*)leaf_cluster_kernel<T, RPT>, &cfg) !=
+                  cudaSuccess ||
+              n < 1) {
+      cudaGetLastError();
+      placeable[g] = -1;
+    } else {
+      placeable[g] = 1;
+    }
+  }
+  if(placeable[g] < 0) return cudaSuccess;
+  cudaError_t e = cudaLaunchKernelEx(&cfg, leaf_cluster_kernel<T, RPT>, P);
+  if(e != cudaSuccess) {
+    cudaGetLastError();
+    placeable[g] = -1;
+    return cudaSuccess;
+  }
+  *done = true;
+  return cudaSuccess;
+}
+
+// Rows per thread: the smaller of two forms whose cluster (at most 16 CTAs)
+// holds the rows; the smaller form keeps its rows in registers without
+// spilling (FP64: 2 rows of 32 doubles per thread; FP32: 3 of 32 floats), the
+// larger reaches further (FP64: 3 rows, 12288 in all; FP32: 4 rows, 16384).
+template <typename T>
+static cudaError_t try_leaf_cluster(const LeafParams<T>& P, int rows, cudaStream_t stream,
+                                    bool* done) {
+  constexpr int kLo = sizeof(T) == 8 ? 2 : 3, kHi = kLo + 1;
+  *done = false;
+  const int glo = (rows + kLo * kRegLeafThreads - 1) / (kLo * kRegLeafThreads);
+  if(glo <= kClusterLeafMax) return launch_leaf_cluster<T, kLo>(P, glo, stream, done);
+  const int ghi = (rows + kHi * kRegLeafThreads - 1) / (kHi * kRegLeafThreads);
+  if(ghi <= kClusterLeafMax) return launch_leaf_cluster<T, kHi>(P, ghi, stream, done);
+  return cudaSuccess;
+}
+
 template <typename T>
 cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
                         double* cand, double* cur, int* bar, int* status, int grid,
                         int leaf_kind, cudaStream_t stream) {
-  // 0: registers first; 1: shared memory first; 2: global memory.
-  const int mode = leaf_kind == HPLB_LEAF_SHARED ? 1 : (leaf_kind == HPLB_LEAF_GLOBAL ? 2 : 0);
+  // 0: cluster, then registers; 3: registers (grid-wide); 1: shared memory
+  // first; 2: global memory.
+  const int mode = leaf_kind == HPLB_LEAF_SHARED      ? 1
+                   : leaf_kind == HPLB_LEAF_GLOBAL    ? 2
+                   : leaf_kind == HPLB_LEAF_REGISTERS ? 3
+                                                      : 0;
   const int rows = end - r0;
   int       dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   if(w <= kRegLeafW && rows > 0 && mode == 0) {
+    LeafParams<T> P;
+    P.A      = A;
+    P.ld     = ld;
+    P.r0     = r0;
+    P.end    = end;
+    P.c0     = c0;
+    P.w      = w;
+    P.rpb    = 0;
+    P.ipiv   = ipiv;
+    P.cand   = cand;
+    P.cur    = cur;
+    P.bar    = bar;
+    P.status = status;
+    bool              done = false;
+    const cudaError_t e    = try_leaf_cluster<T>(P, rows, stream, &done);
+    if(done || e != cudaSuccess) return e;
+  }
+  if(w <= kRegLeafW && rows > 0 && (mode == 0 || mode == 3)) {
     LeafParams<T> P;
     P.A      = A;
     P.ld     = ld;

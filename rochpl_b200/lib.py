@@ -72,7 +72,7 @@ PREC_BF16, PREC_FP16, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2, 3
 
 # hplb_set_option options and values
 HPLB_OPT_LEAF = 1
-LEAF_AUTO, LEAF_SHARED, LEAF_GLOBAL = 0, 1, 2
+LEAF_AUTO, LEAF_SHARED, LEAF_GLOBAL, LEAF_REGISTERS = 0, 1, 2, 3
 
 
 class HplError(RuntimeError):
@@ -231,7 +231,8 @@ class Library:
         self._check(self.L.hplb_set_stream(self.ctx, stream or None))
 
     def set_leaf(self, kind: int):
-        """hplb_set_option(HPLB_OPT_LEAF): LEAF_AUTO, LEAF_SHARED or LEAF_GLOBAL."""
+        """hplb_set_option(HPLB_OPT_LEAF): LEAF_AUTO, LEAF_REGISTERS, LEAF_SHARED or
+        LEAF_GLOBAL."""
         self._check(self.L.hplb_set_option(self.ctx, HPLB_OPT_LEAF, int(kind)))
 
     def getrf(self, algo: hplb_algo, n: int, A: int, ld: int, ipiv: int | None = None) -> int:

@@ -53,16 +53,17 @@ def test_solve_parity(hlib, oracle, n, nb, nbmin):
 
 
 def test_leaf_kinds_give_identical_results(hlib, oracle):
-    """The three places the leaf can keep its slice (hplb_set_option
-    HPLB_OPT_LEAF) perform the same operations in the same order: the same
-    pivots as the oracle and bit-identical x."""
+    """The places the leaf can keep its slice (hplb_set_option HPLB_OPT_LEAF:
+    one cluster's registers, registers across the GPU, shared memory, global
+    memory) perform the same operations in the same order: the same pivots as
+    the oracle and bit-identical x."""
     import torch
 
-    from rochpl_b200.lib import LEAF_AUTO, LEAF_GLOBAL, LEAF_SHARED, HplError
+    from rochpl_b200.lib import LEAF_AUTO, LEAF_GLOBAL, LEAF_REGISTERS, LEAF_SHARED, HplError
 
     xs = []
     try:
-        for kind in (LEAF_AUTO, LEAF_SHARED, LEAF_GLOBAL):
+        for kind in (LEAF_AUTO, LEAF_REGISTERS, LEAF_SHARED, LEAF_GLOBAL):
             hlib.set_leaf(kind)
             r = solve_both(hlib, oracle, 2048, 256, 32)
             assert np.array_equal(r["ipiv"], r["po"]), kind
@@ -71,7 +72,7 @@ def test_leaf_kinds_give_identical_results(hlib, oracle):
         hlib.set_leaf(LEAF_AUTO)
     assert all(np.array_equal(x.view(np.uint64), xs[0].view(np.uint64)) for x in xs)
     with pytest.raises(HplError):
-        hlib.set_leaf(3)
+        hlib.set_leaf(4)
 
 
 def test_solve_parity_n16384_against_the_oracle(hlib, oracle):
