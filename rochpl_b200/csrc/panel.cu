@@ -362,10 +362,98 @@ constexpr int kRegLeafThreads = 256;
 
 template <typename T, int N>
 HPLB_DEV T pick_col(const T (&x)[N], int c) {
-  T s = x[0];
+  if constexpr(N == 32) {
+    // A select tree on the bits of c: depth 5 instead of a 31-long chain.
+    T a[16], b[8], e[4], f[2];
 #pragma unroll
-  for(int q = 1; q < N; ++q) s = (q == c) ? x[q] : s;
-  return s;
+    for(int i = 0; i < 16; ++i) a[i] = (c & 1) ? x[2 * i + 1] : x[2 * i];
+#pragma unroll
+    for(int i = 0; i < 8; ++i) b[i] = (c & 2) ? a[2 * i + 1] : a[2 * i];
+#pragma unroll
+    for(int i = 0; i < 4; ++i) e[i] = (c & 4) ? b[2 * i + 1] : b[2 * i];
+#pragma unroll
+    for(int i = 0; i < 2; ++i) f[i] = (c & 8) ? e[2 * i + 1] : e[2 * i];
+    return (c & 16) ? f[1] : f[0];
+  } else {
+    T s = x[0];
+#pragma unroll
+    for(int q = 1; q < N; ++q) s = (q == c) ? x[q] : s;
+    return s;
+  }
+}
+
+// One column step's work on the rows a thread holds, shared by the register
+// leaves.  d = r0 + k is the diagonal row, p the pivot row; s_u holds the
+// pivot row's w values, s_uz the same with the entries of columns <= k set
+// to zero, s_cur the old diagonal row.
+//   * the interchange: only the warps that hold row d or row p take the branch;
+//   * below the diagonal: l = a_k / pivot, then a_c -= l u_c for c > k.  With
+//     a finite l every column is updated against s_uz (columns <= k see a zero
+//     u and keep their value), one select per entry putting l in column k;
+//     a non-finite l (a zero pivot) keeps the predicated form, so columns
+//     before k stay untouched exactly as in the other leaves.
+template <typename T, int RPT>
+HPLB_DEV void leaf_rows_step(T (&x)[RPT][kRegLeafW], const int (&row)[RPT], int k, int d, int p,
+                             T piv, const double* s_u, const double* s_uz, const double* s_cur) {
+  bool touch = false;
+#pragma unroll
+  for(int q = 0; q < RPT; ++q) touch |= (row[q] == d) | (row[q] == p);
+  if(__any_sync(0xffffffffu, touch)) {
+#pragma unroll
+    for(int q = 0; q < RPT; ++q) {
+      if(row[q] == d) {
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_u[c];
+      } else if(row[q] == p) {
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_cur[c];
+      }
+    }
+  }
+#pragma unroll
+  for(int q = 0; q < RPT; ++q) {
+    if(row[q] > d) {
+      const T l = pick_col(x[q], k) / piv;
+      if(isfinite((double)l)) {
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) {
+          const T nx = x[q][c] - l * (T)s_uz[c];
+          x[q][c]    = (c == k) ? l : nx;
+        }
+      } else {
+#pragma unroll
+        for(int c = 0; c < kRegLeafW; ++c) {
+          if(c == k)
+            x[q][c] = l;
+          else if(c > k)
+            x[q][c] = x[q][c] - l * (T)s_u[c];
+        }
+      }
+    }
+  }
+}
+
+// Publish the rows a column step needs from this block: its candidate row
+// (to slot, w values) and, on the owner, the diagonal row (to cur).  Only the
+// warps holding one of the two take the branch.
+template <typename T, int RPT>
+HPLB_DEV void leaf_rows_publish(const T (&x)[RPT][kRegLeafW], const int (&row)[RPT], int r, int d,
+                                int w, double* slot, double* cur) {
+  bool touch = false;
+#pragma unroll
+  for(int q = 0; q < RPT; ++q) touch |= (r >= 0 && row[q] == r) | (row[q] == d);
+  if(!__any_sync(0xffffffffu, touch)) return;
+#pragma unroll
+  for(int q = 0; q < RPT; ++q) {
+    if(r >= 0 && row[q] == r)
+#pragma unroll
+      for(int c = 0; c < kRegLeafW; ++c)
+        if(c < w) slot[c] = (double)x[q][c];
+    if(row[q] == d)
+#pragma unroll
+      for(int c = 0; c < kRegLeafW; ++c)
+        if(c < w) cur[c] = (double)x[q][c];
+  }
 }
 
 template <typename T, int RPT>
@@ -373,6 +461,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
   __shared__ double s_v[32];
   __shared__ int    s_r[32];
   __shared__ double s_u[kRegLeafW];
+  __shared__ double s_uz[kRegLeafW];
   __shared__ double s_cur[kRegLeafW];
   __shared__ double s_piv;
   __shared__ int    s_p;
@@ -414,17 +503,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
     block_argmax(v, r, s_v, s_r);
     double* slot = P.cand + ((size_t)par * G + blockIdx.x) * sw;
     if(threadIdx.x == 0) *reinterpret_cast<double2*>(slot) = make_double2(v, (double)r);
-#pragma unroll
-    for(int q = 0; q < RPT; ++q) {
-      if(r >= 0 && row[q] == r)
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c)
-          if(c < w) slot[2 + c] = x[q][c];
-      if(row[q] == d)
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c)
-          if(c < w) P.cur[par * w + c] = x[q][c];
-    }
+    leaf_rows_publish(x, row, r, d, w, slot + 2, P.cur + par * w);
     if(!grid_sync(P.bar, G, k + 1, P.status, 15)) return;
 
     if(threadIdx.x < 32) {
@@ -468,7 +547,9 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
       }
       const double* sl = P.cand + ((size_t)par * G + bs) * sw;
       if(threadIdx.x < w) {
-        s_u[threadIdx.x]   = __ldcg(sl + 2 + threadIdx.x);
+        const double u     = __ldcg(sl + 2 + threadIdx.x);
+        s_u[threadIdx.x]   = u;
+        s_uz[threadIdx.x]  = (int)threadIdx.x > k ? u : 0.0;
         s_cur[threadIdx.x] = __ldcg(P.cur + par * w + threadIdx.x);
       }
     }
@@ -479,26 +560,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
       P.ipiv[P.c0 + k] = p;
       if(piv == (T)0) record_info(P.status, P.c0 + k + 1);
     }
-#pragma unroll
-    for(int q = 0; q < RPT; ++q) {
-      if(row[q] == d) {
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_u[c];
-      } else if(row[q] == p) {
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_cur[c];
-      }
-      if(row[q] > d) {
-        const T l = pick_col(x[q], k) / piv;
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c) {
-          if(c == k)
-            x[q][c] = l;
-          else if(c > k)
-            x[q][c] = x[q][c] - l * (T)s_u[c];
-        }
-      }
-    }
+    leaf_rows_step(x, row, k, d, p, piv, s_u, s_uz, s_cur);
   }
 
 #pragma unroll
@@ -556,6 +618,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafPa
   __shared__ double s_slot[2][2 + kRegLeafW];  // (value, row, candidate row) per parity
   __shared__ double s_diag[2][kRegLeafW];      // the diagonal row, on its owner
   __shared__ double s_u[kRegLeafW];
+  __shared__ double s_uz[kRegLeafW];
   __shared__ double s_cur[kRegLeafW];
   __shared__ double s_piv;
   __shared__ int    s_p;
@@ -598,17 +661,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafPa
       s_slot[par][0] = v;
       s_slot[par][1] = (double)r;
     }
-#pragma unroll
-    for(int q = 0; q < RPT; ++q) {
-      if(r >= 0 && row[q] == r)
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c)
-          if(c < w) s_slot[par][2 + c] = (double)x[q][c];
-      if(row[q] == d)
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c)
-          if(c < w) s_diag[par][c] = (double)x[q][c];
-    }
+    leaf_rows_publish(x, row, r, d, w, &s_slot[par][2], &s_diag[par][0]);
     cluster_barrier();
 
     if(threadIdx.x < 32) {
@@ -630,8 +683,10 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafPa
       }
       const unsigned owner = (unsigned)min((int)G - 1, (d - P.r0) / P.rpb);
       if(lane < w) {
-        s_u[lane]   = ld_peer(&s_slot[par][2 + lane], (unsigned)bs);
-        s_cur[lane] = ld_peer(&s_diag[par][lane], owner);
+        const double u = ld_peer(&s_slot[par][2 + lane], (unsigned)bs);
+        s_u[lane]      = u;
+        s_uz[lane]     = lane > k ? u : 0.0;
+        s_cur[lane]    = ld_peer(&s_diag[par][lane], owner);
       }
     }
     __syncthreads();
@@ -641,26 +696,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafPa
       P.ipiv[P.c0 + k] = p;
       if(piv == (T)0) record_info(P.status, P.c0 + k + 1);
     }
-#pragma unroll
-    for(int q = 0; q < RPT; ++q) {
-      if(row[q] == d) {
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_u[c];
-      } else if(row[q] == p) {
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c) x[q][c] = (T)s_cur[c];
-      }
-      if(row[q] > d) {
-        const T l = pick_col(x[q], k) / piv;
-#pragma unroll
-        for(int c = 0; c < kRegLeafW; ++c) {
-          if(c == k)
-            x[q][c] = l;
-          else if(c > k)
-            x[q][c] = x[q][c] - l * (T)s_u[c];
-        }
-      }
-    }
+    leaf_rows_step(x, row, k, d, p, piv, s_u, s_uz, s_cur);
   }
   cluster_barrier();
 
