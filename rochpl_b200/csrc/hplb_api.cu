@@ -81,10 +81,14 @@ struct Solve {
   hplb_status leaf(int r0, int c0, int w, int pc, int pw) {
     hplb_ctx* ctx  = this->ctx;
     const int grid = leaf_grid_size(ctx->num_sms, n - r0);
-    CK(launch_leaf(A, ld, r0, n, c0, w, ctx->d_ipiv, ctx->d_cand, ctx->d_cur, ctx->d_bar,
-                   ctx->d_status, grid, ctx->leaf_kind, ctx->s_pan));
-    CK(launch_panel_swap(A, ld, ctx->d_ipiv, r0, c0, w, pc, pw, ctx->s_pan));
-    ctx->launches += 2;
+    bool swapped = false;
+    CK(launch_leaf(A, ld, r0, n, c0, w, pc, pw, ctx->d_ipiv, ctx->d_cand, ctx->d_cur,
+                   ctx->d_bar, ctx->d_status, grid, ctx->leaf_kind, ctx->s_pan, &swapped));
+    ctx->launches += 1;
+    if(!swapped) {
+      CK(launch_panel_swap(A, ld, ctx->d_ipiv, r0, c0, w, pc, pw, ctx->s_pan));
+      ctx->launches += 1;
+    }
     return HPLB_OK;
   }
 

@@ -39,10 +39,13 @@ int         leaf_grid_size(int num_sms, int rows);
 // leaf_kind: where the leaf's rows live, HPLB_LEAF_* of include/hplb.h
 // (auto = registers, then shared memory, then global memory, the first that
 // holds the leaf; a forced kind falls through the same way when it does not).
+// pc, pw: the panel the leaf belongs to.  *swapped is set when the leaf also
+// applied its interchanges to the panel's other columns (the cluster leaf
+// does; otherwise the caller runs launch_panel_swap).
 template <typename T>
-cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
-                        double* cand, double* cur, int* bar, int* status, int grid,
-                        int leaf_kind, cudaStream_t stream);
+cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int pc, int pw,
+                        int* ipiv, double* cand, double* cur, int* bar, int* status, int grid,
+                        int leaf_kind, cudaStream_t stream, bool* swapped);
 template <typename T>
 cudaError_t launch_panel_swap(T* A, int64_t ld, const int* ipiv, int r0, int c0, int w, int pc,
                               int pw, cudaStream_t stream);

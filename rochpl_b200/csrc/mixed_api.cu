@@ -47,10 +47,14 @@ struct Mixed {
   hplb_status leaf(int r0, int c0, int wdt, int pc, int pw) {
     hplb_ctx* ctx  = this->ctx;
     const int grid = leaf_grid_size(ctx->num_sms, n - r0);
-    CK(launch_leaf<float>(W, ldw, r0, n, c0, wdt, ctx->d_ipiv, ctx->d_cand, ctx->d_cur,
-                          ctx->d_bar, ctx->d_status, grid, ctx->leaf_kind, st));
-    CK(launch_panel_swap<float>(W, ldw, ctx->d_ipiv, r0, c0, wdt, pc, pw, st));
-    ctx->launches += 2;
+    bool swapped = false;
+    CK(launch_leaf<float>(W, ldw, r0, n, c0, wdt, pc, pw, ctx->d_ipiv, ctx->d_cand, ctx->d_cur,
+                          ctx->d_bar, ctx->d_status, grid, ctx->leaf_kind, st, &swapped));
+    ctx->launches += 1;
+    if(!swapped) {
+      CK(launch_panel_swap<float>(W, ldw, ctx->d_ipiv, r0, c0, wdt, pc, pw, st));
+      ctx->launches += 1;
+    }
     return HPLB_OK;
   }
 

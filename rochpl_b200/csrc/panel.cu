@@ -72,6 +72,8 @@ struct LeafParams {
   double* cur;      // [2][w]            (the diagonal row's leaf values)
   int*    bar;      // grid barrier words
   int*    status;
+  int     pc, pw;   // the panel [pc, pc + pw) the leaf belongs to (cluster leaf:
+                    // it also swaps the panel's other columns)
 };
 
 // Publish this block's pivot candidate for leaf column k (its rows >= d) and,
@@ -622,6 +624,8 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafPa
   __shared__ double s_cur[kRegLeafW];
   __shared__ double s_piv;
   __shared__ int    s_p;
+  __shared__ int    s_pv[kRegLeafW];  // the leaf's pivots, relative to r0
+  __shared__ int    s_src[kRegLeafW], s_dst[kRegLeafW];
 
   const unsigned G    = cluster_nctarank();
   const unsigned me   = cluster_ctarank();
@@ -696,6 +700,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafPa
       P.ipiv[P.c0 + k] = p;
       if(piv == (T)0) record_info(P.status, P.c0 + k + 1);
     }
+    if(threadIdx.x == 0) s_pv[k] = p - P.r0;
     leaf_rows_step(x, row, k, d, p, piv, s_u, s_uz, s_cur);
   }
   cluster_barrier();
@@ -706,21 +711,64 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafPa
 #pragma unroll
       for(int c = 0; c < kRegLeafW; ++c)
         if(c < w) P.A[(size_t)row[q] + (size_t)(P.c0 + c) * ld] = x[q][c];
+
+  // The leaf's interchanges on the panel's other columns (the work of
+  // panel_swap_kernel, which this leaf replaces): the interchange sequence
+  // traced into a row map, then per column all reads before any write.  The
+  // leaf's own columns are not touched here, so no ordering with the
+  // write-back above is needed.
+  const int ncols = P.pw - w;
+  if(ncols <= 0) return;
+  if(threadIdx.x < w) {
+    const int xr = threadIdx.x;
+    int       pos = xr;
+    for(int i = w - 1; i >= 0; --i) {
+      const int pp = s_pv[i];
+      pos          = (pos == i) ? pp : (pos == pp ? i : pos);
+    }
+    s_src[xr] = pos;
+    pos       = xr;
+    for(int i = 0; i < w; ++i) {
+      const int pp = s_pv[i];
+      pos          = (pos == i) ? pp : (pos == pp ? i : pos);
+    }
+    s_dst[xr] = pos >= w ? pos : -1;
+  }
+  __syncthreads();
+  // A warp per column, lane = row of the leaf's top block: the top rows'
+  // writes are one contiguous segment, and every warp of the cluster takes
+  // columns in turn.
+  const int nwarp = (int)G * (int)(blockDim.x >> 5);
+  for(int j = (int)me * (int)(blockDim.x >> 5) + (int)(threadIdx.x >> 5); j < ncols; j += nwarp) {
+    const int col = (P.pc + j < P.c0) ? P.pc + j : P.pc + j + w;
+    T*        a   = P.A + (size_t)col * ld + P.r0;
+    T         v = (T)0, o = (T)0;
+    const int dst = lane < w ? s_dst[lane] : -1;
+    if(lane < w) {
+      v = a[s_src[lane]];
+      if(dst >= 0) o = a[lane];
+    }
+    __syncwarp();  // every read of the column before any write to it
+    if(dst >= 0) a[dst] = o;
+    if(lane < w) a[lane] = v;
+    __syncwarp();
+  }
 }
 
 // Apply the w interchanges of leaf columns [c0, c0+w) to the panel columns
-// outside the leaf, one thread per column.  For w <= 32 the interchange
-// sequence is traced once per block into a row map (src[x]: the row whose
-// value ends in row r0 + x; dst[x]: where the old row r0 + x ends when it
-// leaves the top w rows, else -1), and every column then reads all the rows it
-// needs before writing any, so its w reads are in flight together instead of
-// forming a chain of w dependent swaps.  Wider leaves swap in order.
+// outside the leaf.  For w <= 32 the interchange sequence is traced once per
+// block into a row map (src[x]: the row whose value ends in row r0 + x;
+// dst[x]: where the old row r0 + x ends when it leaves the top w rows, else
+// -1), and a warp takes each column, lane = row of the top block: every read
+// of the column before any write, the top rows written as one contiguous
+// segment.  Wider leaves swap in order, a thread per column.
+constexpr int kSwapWarps = 8;
 template <typename T>
-__global__ void panel_swap_kernel(T* A, int64_t ld, const int* ipiv, int r0, int c0,
-                                  int w, int pc, int pw) {
+__global__ void __launch_bounds__(kSwapWarps * 32)
+panel_swap_kernel(T* A, int64_t ld, const int* ipiv, int r0, int c0, int w, int pc, int pw) {
   constexpr int kMap = 32;
   __shared__ int s_src[kMap], s_dst[kMap];
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int ncols = pw - w;
   if(w <= kMap) {
     if(threadIdx.x < w) {
       const int x = threadIdx.x;
@@ -738,33 +786,32 @@ __global__ void panel_swap_kernel(T* A, int64_t ld, const int* ipiv, int r0, int
       s_dst[x] = pos >= w ? pos : -1;
     }
     __syncthreads();
-    if(j >= pw - w) return;
+    const int lane = threadIdx.x & 31;
+    const int j    = blockIdx.x * kSwapWarps + (threadIdx.x >> 5);
+    if(j >= ncols) return;
     const int col = (pc + j < c0) ? pc + j : pc + j + w;
     T*        a   = A + (size_t)col * ld + r0;
-    T         v[kMap], o[kMap];
-#pragma unroll
-    for(int x = 0; x < kMap; ++x)
-      if(x < w) {
-        v[x] = a[s_src[x]];
-        o[x] = s_dst[x] >= 0 ? a[x] : (T)0;
-      }
-#pragma unroll
-    for(int x = 0; x < kMap; ++x)
-      if(x < w && s_dst[x] >= 0) a[s_dst[x]] = o[x];
-#pragma unroll
-    for(int x = 0; x < kMap; ++x)
-      if(x < w) a[x] = v[x];
+    T         v = (T)0, o = (T)0;
+    const int dst = lane < w ? s_dst[lane] : -1;
+    if(lane < w) {
+      v = a[s_src[lane]];
+      if(dst >= 0) o = a[lane];
+    }
+    __syncwarp();
+    if(dst >= 0) a[dst] = o;
+    if(lane < w) a[lane] = v;
     return;
   }
-  if(j >= pw - w) return;
-  const int col = (pc + j < c0) ? pc + j : pc + j + w;
-  T*        a   = A + (size_t)col * ld;
-  for(int k = 0; k < w; ++k) {
-    const int d = r0 + k, p = ipiv[c0 + k];
-    if(p != d) {
-      const T t = a[d];
-      a[d]           = a[p];
-      a[p]           = t;
+  for(int j = blockIdx.x * blockDim.x + threadIdx.x; j < ncols; j += gridDim.x * blockDim.x) {
+    const int col = (pc + j < c0) ? pc + j : pc + j + w;
+    T*        a   = A + (size_t)col * ld;
+    for(int k = 0; k < w; ++k) {
+      const int d = r0 + k, p = ipiv[c0 + k];
+      if(p != d) {
+        const T t = a[d];
+        a[d]      = a[p];
+        a[p]      = t;
+      }
     }
   }
 }
@@ -1125,9 +1172,10 @@ static cudaError_t try_leaf_cluster(const LeafParams<T>& P, int rows, cudaStream
 }
 
 template <typename T>
-cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* ipiv,
-                        double* cand, double* cur, int* bar, int* status, int grid,
-                        int leaf_kind, cudaStream_t stream) {
+cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int pc, int pw,
+                        int* ipiv, double* cand, double* cur, int* bar, int* status, int grid,
+                        int leaf_kind, cudaStream_t stream, bool* swapped) {
+  *swapped = false;
   // 0: cluster, then registers; 3: registers (grid-wide); 1: shared memory
   // first; 2: global memory.
   const int mode = leaf_kind == HPLB_LEAF_SHARED      ? 1
@@ -1152,8 +1200,11 @@ cudaError_t launch_leaf(T* A, int64_t ld, int r0, int end, int c0, int w, int* i
     P.cur    = cur;
     P.bar    = bar;
     P.status = status;
+    P.pc     = pc;
+    P.pw     = pw;
     bool              done = false;
     const cudaError_t e    = try_leaf_cluster<T>(P, rows, stream, &done);
+    *swapped               = done;
     if(done || e != cudaSuccess) return e;
   }
   if(w <= kRegLeafW && rows > 0 && (mode == 0 || mode == 3)) {
@@ -1229,7 +1280,9 @@ cudaError_t launch_panel_swap(T* A, int64_t ld, const int* ipiv, int r0, int c0,
                               int pw, cudaStream_t stream) {
   const int ncols = pw - w;
   if(ncols <= 0) return cudaSuccess;
-  panel_swap_kernel<T><<<(ncols + 127) / 128, 128, 0, stream>>>(A, ld, ipiv, r0, c0, w, pc, pw);
+  const int grid = w <= 32 ? (ncols + kSwapWarps - 1) / kSwapWarps
+                            : (ncols + kSwapWarps * 32 - 1) / (kSwapWarps * 32);
+  panel_swap_kernel<T><<<grid, kSwapWarps * 32, 0, stream>>>(A, ld, ipiv, r0, c0, w, pc, pw);
   return cudaGetLastError();
 }
 
@@ -1325,8 +1378,8 @@ cudaError_t launch_laswp_gather(T* A, int64_t ld, int ia, int jb, const int* per
 }
 
 #define HPLB_PANEL_INSTANTIATE(T)                                                              \
-  template cudaError_t launch_leaf<T>(T*, int64_t, int, int, int, int, int*, double*, double*, \
-                                      int*, int*, int, int, cudaStream_t);                     \
+  template cudaError_t launch_leaf<T>(T*, int64_t, int, int, int, int, int, int, int*, double*,  \
+                                      double*, int*, int*, int, int, cudaStream_t, bool*);     \
   template cudaError_t launch_panel_swap<T>(T*, int64_t, const int*, int, int, int, int, int,  \
                                             cudaStream_t);                                     \
   template cudaError_t launch_diag_inv<T>(const T*, int64_t, int, int, int, T*, cudaStream_t); \
