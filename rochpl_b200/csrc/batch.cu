@@ -718,25 +718,34 @@ HPLB_DEV void rec_leaf(double* A, double* B, int n, int nrhs, int* ip, int c0, i
     S.dst[x] = pos >= w ? pos : -1;
   }
   __syncthreads();
+  // Half a warp per column, lane = row of the leaf's top block (w <= 16): the
+  // top rows are written as one contiguous segment, and each column's reads
+  // all happen before any of its writes (the half-warp's own column only).
   const int ncol = n - w + nrhs;
-  for(int q = threadIdx.x; q < ncol; q += kBT) {
-    double* col = q < c0 ? A + (size_t)q * n
-                         : (q < n - w ? A + (size_t)(q + w) * n : B + (size_t)(q - (n - w)) * n);
-    col += c0;
-    double x[kRecLeaf], o[kRecLeaf];
-#pragma unroll
-    for(int r = 0; r < kRecLeaf; ++r)
-      if(r < w) {
-        x[r] = col[S.src[r]];
-        o[r] = S.dst[r] >= 0 ? col[r] : 0.0;
-      }
-    // The displaced old top rows go below the block (dst >= w).
-#pragma unroll
-    for(int r = 0; r < kRecLeaf; ++r)
-      if(r < w && S.dst[r] >= 0) col[S.dst[r]] = o[r];
-#pragma unroll
-    for(int r = 0; r < kRecLeaf; ++r)
-      if(r < w) col[r] = x[r];
+  const int hl   = threadIdx.x & 15;
+  const int src  = hl < w ? S.src[hl] : 0;
+  const int dst  = hl < w ? S.dst[hl] : -1;
+  // The whole warp iterates together (two columns per trip), so every lane
+  // reaches each __syncwarp; a half-warp past the last column idles.
+  for(int q0 = (threadIdx.x >> 5) * 2; q0 < ncol; q0 += kBT / 16) {
+    const int q  = q0 + ((threadIdx.x >> 4) & 1);
+    const bool on = q < ncol && hl < w;
+    double* col = nullptr;
+    double  v = 0.0, o = 0.0;
+    if(on) {
+      col = q < c0 ? A + (size_t)q * n
+                   : (q < n - w ? A + (size_t)(q + w) * n : B + (size_t)(q - (n - w)) * n);
+      col += c0;
+      v = col[src];
+      if(dst >= 0) o = col[hl];
+    }
+    __syncwarp();
+    if(on) {
+      // The displaced old top rows go below the block (dst >= w).
+      if(dst >= 0) col[dst] = o;
+      col[hl] = v;
+    }
+    __syncwarp();
   }
   __syncthreads();
 }
