@@ -1075,8 +1075,45 @@ def case_batch(args) -> None:
     plan.close()
 
 
+def case_autograd(args) -> None:
+    """hpl_solve (--n, --nb, 32 RHS from the LCG) forward and backward, four
+    times; CUDA events on the current stream, the mean of the last three."""
+    import torch
+
+    from rochpl_b200 import library
+    from rochpl_b200.autograd import hpl_solve
+
+    lib = library(0)
+    n, nrhs = args.n, 32
+    M = torch.empty((n + nrhs) * n, dtype=torch.float64, device="cuda")
+    lib.matgen(n, n + nrhs, 100, M.data_ptr(), n)
+    A = M.view(n + nrhs, n)[:n].t().contiguous().requires_grad_(True)
+    B = M.view(n + nrhs, n)[n:].t().contiguous().requires_grad_(True)
+    del M
+    Xbar = torch.ones(n, nrhs, dtype=torch.float64, device="cuda")
+    fwd, bwd = [], []
+    for it in range(4):
+        A.grad = B.grad = None
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record()
+        X = hpl_solve(A, B, nb=args.nb)
+        e1.record()
+        X.backward(Xbar)
+        e2.record()
+        torch.cuda.synchronize()
+        if it:
+            fwd.append(e0.elapsed_time(e1))
+            bwd.append(e1.elapsed_time(e2))
+    tf = statistics.mean(fwd)
+    f = 2.0 / 3.0 * n ** 3 + 2.0 * n ** 2 * nrhs
+    print(f"autograd N={n} NB={args.nb} nrhs={nrhs}: forward {tf:.2f} ms ({f / tf / 1e9:.2f} "
+          f"TFLOP/s), backward {statistics.mean(bwd):.2f} ms")
+
+
 CASES = {"dgemm": case_dgemm, "solve": case_solve, "gemm_lp": case_gemm_lp,
-         "getrf": case_getrf, "mixed": case_mixed, "batch": case_batch}
+         "getrf": case_getrf, "mixed": case_mixed, "batch": case_batch,
+         "autograd": case_autograd}
 
 
 def main():

@@ -105,6 +105,16 @@ hplb_status hplb_set_stream(hplb_ctx* ctx, void* stream);
 #define HPLB_LEAF_SHARED 1
 #define HPLB_LEAF_GLOBAL 2
 #define HPLB_LEAF_REGISTERS 3
+/*   HPLB_OPT_PANEL_SMS: SMs that the trailing-update DGEMM leaves to the panel
+ *   factorisation while the next panel is being factored beside it: 0 (the
+ *   DGEMM may take every SM; the high-priority panel kernels take SMs as its
+ *   CTAs retire), or k > 0 (the DGEMM's grid is capped at SMs - k CTAs, each
+ *   walking a longer run of tiles).  HPLB_PANEL_SMS_AUTO (-1, the default) is
+ *   0 on B200: a cap of 8 to 48 SMs slowed the solve at N = 4096 to 32768,
+ *   because the panel's own GEMMs and triangular solves then run on the few
+ *   SMs left to them.  Results do not depend on it. */
+#define HPLB_OPT_PANEL_SMS 2
+#define HPLB_PANEL_SMS_AUTO (-1)
 hplb_status hplb_set_option(hplb_ctx* ctx, int option, int value);
 
 const char* hplb_status_string(hplb_status s);

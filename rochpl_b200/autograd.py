@@ -20,19 +20,21 @@ from __future__ import annotations
 
 import torch
 
-from .hpl import Algo
+from .hpl import Algo, default_ld
 from .lib import HplError, library
 
 __all__ = ["HplSolve", "hpl_solve", "HplSolveBatch", "hpl_solve_batch"]
 
 
-def _colmajor(M: torch.Tensor) -> torch.Tensor:
-    """Column-major copy of a 2-D tensor: returns T with T[j, i] = M[i, j],
-    i.e. M stored column by column with leading dimension M.shape[0].  Always
-    a new buffer (the solve overwrites it): for an M that is already
+def _colmajor(M: torch.Tensor, ld: int | None = None) -> torch.Tensor:
+    """Column-major copy of a 2-D tensor: returns T (M.shape[1] x ld) with
+    T[j, i] = M[i, j] for i < M.shape[0], i.e. M stored column by column with
+    leading dimension ld (default M.shape[0]; rows beyond are padding).
+    Always a new buffer (the solve overwrites it): for an M that is already
     column-major, M.t().contiguous() would return M's own storage."""
-    out = torch.empty((M.shape[1], M.shape[0]), dtype=M.dtype, device=M.device)
-    out.copy_(M.t())
+    ld = M.shape[0] if ld is None else ld
+    out = torch.empty((M.shape[1], ld), dtype=M.dtype, device=M.device)
+    out[:, : M.shape[0]].copy_(M.t())
     return out
 
 
@@ -52,17 +54,21 @@ class HplSolve(torch.autograd.Function):
         lib = library(A.device.index or 0)
         lib.set_stream(torch.cuda.current_stream(A.device).cuda_stream)
         nbe = max(1, min(nb, max(n, 1)))
-        LU = _colmajor(A.detach())
+        # The factors get HPL's padded leading dimension: a power-of-two
+        # column stride (n = 16384) maps every column to the same L2 sets and
+        # DRAM channels and slows the factorisation.
+        ld = int(default_ld(n)) if n > 0 else 1
+        LU = _colmajor(A.detach(), ld)
         ipiv = torch.zeros(max(n, 1), dtype=torch.int32, device=A.device)
-        info = lib.getrf(Algo(nbe, min(nbmin, nbe), 2, 2, 2, 1, 0).c(), n, LU.data_ptr(),
-                         max(n, 1), ipiv.data_ptr())
+        info = lib.getrf(Algo(nbe, min(nbmin, nbe), 2, 2, 2, 1, 0).c(), n, LU.data_ptr(), ld,
+                         ipiv.data_ptr())
         if info:
             raise HplError(3, f"hpl_solve: A is singular (zero pivot in column {info})")
         Xc = _colmajor(B.detach())
-        lib.getrs(0, n, nbe, nrhs, LU.data_ptr(), max(n, 1), ipiv.data_ptr(), Xc.data_ptr(),
-                  max(n, 1))
+        lib.getrs(0, n, nbe, nrhs, LU.data_ptr(), ld, ipiv.data_ptr(), Xc.data_ptr(), max(n, 1))
         ctx.save_for_backward(LU, ipiv, Xc)
         ctx.nb = nbe
+        ctx.ld = ld
         return Xc.t()
 
     @staticmethod
@@ -72,7 +78,7 @@ class HplSolve(torch.autograd.Function):
         lib = library(LU.device.index or 0)
         lib.set_stream(torch.cuda.current_stream(LU.device).cuda_stream)
         Bc = _colmajor(Xbar.to(torch.float64))
-        lib.getrs(1, n, ctx.nb, nrhs, LU.data_ptr(), max(n, 1), ipiv.data_ptr(), Bc.data_ptr(),
+        lib.getrs(1, n, ctx.nb, nrhs, LU.data_ptr(), ctx.ld, ipiv.data_ptr(), Bc.data_ptr(),
                   max(n, 1))
         gA = None
         if ctx.needs_input_grad[0]:

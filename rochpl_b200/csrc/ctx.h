@@ -58,6 +58,7 @@ struct hplb_ctx {
   int*    r_perm = nullptr;  size_t r_perm_cap = 0;  // one panel's row map
 
   int          leaf_kind = HPLB_LEAF_AUTO;  // hplb_set_option(HPLB_OPT_LEAF)
+  int          panel_sms = HPLB_PANEL_SMS_AUTO;  // hplb_set_option(HPLB_OPT_PANEL_SMS)
   cudaStream_t caller   = nullptr;  // hplb_set_stream (null: the legacy default stream)
   cudaEvent_t  ev_enter = nullptr;  // recorded on `caller` at every entry
 

@@ -200,10 +200,12 @@ dgemm_sub_kernel(int m, int n, int k, const double* __restrict__ A, int64_t lda,
 
 static cudaError_t launch_dgemm_any(int m, int n, int k, const double* A, int64_t lda,
                                     const double* B, int64_t ldb, double* C, int64_t ldc,
-                                    int* status, bool accumulate, cudaStream_t stream) {
+                                    int* status, bool accumulate, cudaStream_t stream,
+                                    int max_ctas = 0) {
   if(m <= 0 || n <= 0) return cudaSuccess;
   if(k > 0 && status && dgemm_tma_eligible(m, n, k, A, lda, B, ldb)) {
-    cudaError_t e = launch_dgemm_tma(m, n, k, A, lda, B, ldb, C, ldc, status, accumulate, stream);
+    cudaError_t e = launch_dgemm_tma(m, n, k, A, lda, B, ldb, C, ldc, status, accumulate, stream,
+                                     max_ctas);
     if(e == cudaSuccess) return e;
     cudaGetLastError();  // fall back to the cp.async kernel
   }
@@ -212,9 +214,9 @@ static cudaError_t launch_dgemm_any(int m, int n, int k, const double* A, int64_
 
 cudaError_t launch_dgemm_sub(int m, int n, int k, const double* A, int64_t lda,
                              const double* B, int64_t ldb, double* C, int64_t ldc,
-                             int* status, cudaStream_t stream) {
+                             int* status, cudaStream_t stream, int max_ctas) {
   if(k <= 0) return cudaSuccess;
-  return launch_dgemm_any(m, n, k, A, lda, B, ldb, C, ldc, status, true, stream);
+  return launch_dgemm_any(m, n, k, A, lda, B, ldb, C, ldc, status, true, stream, max_ctas);
 }
 
 cudaError_t launch_dgemm_set(int m, int n, int k, const double* A, int64_t lda,

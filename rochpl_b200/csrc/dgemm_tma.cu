@@ -24,10 +24,12 @@
 // sets have distinct (bit0, bit3) -- what the B swizzle needs -- and distinct
 // (bit1, bit2) -- what the A swizzle needs -- so both fragments load without
 // bank conflicts.
-// A CTA computes TPC consecutive 128 x 128 tiles of a grouped order (4 column
+// A CTA computes tpc consecutive 128 x 128 tiles of a grouped order (4 column
 // tiles per A row-tile), so an A tile is fetched from HBM once and re-read
-// from L2 three times, and CTAs retire every few tiles so the high-priority
-// panel stream can get onto SMs.
+// from L2 three times.  Either CTAs retire every few tiles, so that the
+// high-priority panel stream can get onto SMs as they free up, or (a cap on
+// the grid) a fixed number of CTAs each walks a long run of tiles and the
+// SMs beyond the cap stay free for the panel stream for the whole launch.
 //
 // Every mbarrier wait is bounded: a wait only expires when a copy never lands;
 // the CTA then records the site in the status word and exits.
@@ -144,11 +146,11 @@ HPLB_DEV void issue_slice(int q, int t_begin, int KT, int tiles_m, int tiles_n,
   tma_load_2d(sB + s * B_BYTES, tmB, &full[s], kt * BK, tn * BN);
 }
 
-template <int TPC, bool ACCUM>
+template <bool ACCUM>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  int m, int n, int k, double* __restrict__ C, int64_t ldc, int tiles_m,
-                 int tiles_n, int* status) {
+                 int tiles_n, int tpc, int* status) {
   extern __shared__ unsigned char smem_raw[];
   unsigned char* base = (unsigned char*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   unsigned char* sA   = base;                      // [STAGES][A_BYTES]
@@ -159,8 +161,8 @@ dgemm_tma_kernel(const __grid_constant__ CUtensorMap tmA, const __grid_constant_
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int ntiles  = tiles_m * tiles_n;
-  const int t_begin = blockIdx.x * TPC;
-  const int t_end   = min(ntiles, t_begin + TPC);
+  const int t_begin = blockIdx.x * tpc;
+  const int t_end   = min(ntiles, t_begin + tpc);
   const int KT      = (k + BK - 1) / BK;
   const int nslices = (t_end - t_begin) * KT;
 
@@ -335,29 +337,28 @@ int tiles_per_cta(long long ntiles) {
   return ntiles >= 256LL * sms ? 4 : 1;
 }
 
-template <int TPC>
 cudaError_t launch_tpc(const CUtensorMap& mA, const CUtensorMap& mB, int m, int n, int k,
-                       double* C, int64_t ldc, int tiles_m, int tiles_n, bool accumulate,
+                       double* C, int64_t ldc, int tiles_m, int tiles_n, int tpc, bool accumulate,
                        int* status, cudaStream_t stream) {
   static bool attr = false;
   if(!attr) {
-    cudaError_t e = cudaFuncSetAttribute(dgemm_tma_kernel<TPC, true>,
+    cudaError_t e = cudaFuncSetAttribute(dgemm_tma_kernel<true>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if(e == cudaSuccess)
-      e = cudaFuncSetAttribute(dgemm_tma_kernel<TPC, false>,
+      e = cudaFuncSetAttribute(dgemm_tma_kernel<false>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM_BYTES);
     if(e != cudaSuccess) return e;
     attr = true;
   }
   const long long ntiles = (long long)tiles_m * tiles_n;
-  const long long grid   = (ntiles + TPC - 1) / TPC;
+  const long long grid   = (ntiles + tpc - 1) / tpc;
   if(grid > 0x7fffffff) return cudaErrorInvalidValue;
   if(accumulate)
-    dgemm_tma_kernel<TPC, true><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
-        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
+    dgemm_tma_kernel<true><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
+        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, tpc, status);
   else
-    dgemm_tma_kernel<TPC, false><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
-        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, status);
+    dgemm_tma_kernel<false><<<(unsigned)grid, THREADS, SMEM_BYTES, stream>>>(
+        mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, tpc, status);
   return cudaGetLastError();
 }
 
@@ -375,7 +376,7 @@ bool dgemm_tma_eligible(int m, int n, int k, const double* A, int64_t lda, const
 
 cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda, const double* B,
                              int64_t ldb, double* C, int64_t ldc, int* status, bool accumulate,
-                             cudaStream_t stream) {
+                             cudaStream_t stream, int max_ctas) {
   CUtensorMap mA, mB;
   {
     cuuint64_t dims[3]    = {16, (cuuint64_t)k, (cuuint64_t)((m + 15) / 16)};
@@ -397,15 +398,13 @@ cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda, 
                           CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if(r != CUDA_SUCCESS) return cudaErrorInvalidValue;
   }
-  const int tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
-  switch(tiles_per_cta((long long)tiles_m * tiles_n)) {
-    case 1:
-      return launch_tpc<1>(mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, accumulate, status, stream);
-    case 2:
-      return launch_tpc<2>(mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, accumulate, status, stream);
-    default:
-      return launch_tpc<4>(mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, accumulate, status, stream);
-  }
+  const int       tiles_m = (m + BM - 1) / BM, tiles_n = (n + BN - 1) / BN;
+  const long long ntiles  = (long long)tiles_m * tiles_n;
+  long long       tpc     = tiles_per_cta(ntiles);
+  if(max_ctas > 0 && (ntiles + tpc - 1) / tpc > max_ctas) tpc = (ntiles + max_ctas - 1) / max_ctas;
+  if(tpc > 0x7fffffff) return cudaErrorInvalidValue;
+  return launch_tpc(mA, mB, m, n, k, C, ldc, tiles_m, tiles_n, (int)tpc, accumulate, status,
+                    stream);
 }
 
 }  // namespace hplb

@@ -109,13 +109,12 @@ struct Solve {
         rem -= jb;
         if((s = rpanel(r0 + jj, c0 + jj, jb, pc, pw)) != HPLB_OK) return s;
         if(rem > 0) {
-          CK(launch_diag_inv(A, ld, r0 + jj, c0 + jj, jb, ctx->d_dinv_piece, st));
-          CK(launch_laswp_trsm(A, ld, r0 + jj, jb, c0 + jj, nullptr, ctx->d_dinv_piece,
-                               c0 + jj + jb, rem, st));
+          CK(launch_trsm_node(A, ld, r0 + jj, jb, c0 + jj, ctx->d_dinv_piece, c0 + jj + jb, rem,
+                              st, &ctx->launches));
           CK(launch_dgemm_sub(n - (r0 + jj + jb), rem, jb, a(r0 + jj + jb, c0 + jj), ld,
                               a(r0 + jj, c0 + jj + jb), ld, a(r0 + jj + jb, c0 + jj + jb), ld,
                               ctx->d_status, st));
-          ctx->launches += 3;
+          ctx->launches += 1;
         }
         jj += jb;
         jb = std::min(rem, nbs);
@@ -125,11 +124,10 @@ struct Solve {
         rem -= jb;
         const int cj = c0 + jj;
         if(jj > 0) {
-          CK(launch_diag_inv(A, ld, r0, c0, jj, ctx->d_dinv_piece, st));
-          CK(launch_laswp_trsm(A, ld, r0, jj, c0, nullptr, ctx->d_dinv_piece, cj, jb, st));
+          CK(launch_trsm_node(A, ld, r0, jj, c0, ctx->d_dinv_piece, cj, jb, st, &ctx->launches));
           CK(launch_dgemm_sub(n - (r0 + jj), jb, jj, a(r0 + jj, c0), ld, a(r0, cj), ld,
                               a(r0 + jj, cj), ld, ctx->d_status, st));
-          ctx->launches += 3;
+          ctx->launches += 1;
         }
         if((s = rpanel(r0 + jj, cj, jb, pc, pw)) != HPLB_OK) return s;
         jj += jb;
@@ -161,7 +159,8 @@ struct Solve {
   }
 
   // Row interchanges + U12 + trailing DGEMM of panel j on columns [c, c+w).
-  hplb_status update(int j, int set, int c, int w) {
+  // max_ctas > 0 caps the grids of the update's DGEMMs (SMs left to the panel).
+  hplb_status update(int j, int set, int c, int w, int max_ctas = 0) {
     hplb_ctx* ctx = this->ctx;
     if(w <= 0) return HPLB_OK;
     const int jb = std::min(algo->nb, n - j);
@@ -176,7 +175,7 @@ struct Solve {
       cudaEvent_t e0 = next_event(ctx), e1 = next_event(ctx);
       CK(cudaEventRecord(e0, ctx->s_upd));
       CK(launch_dgemm_sub(m, w, jb, a(j + jb, j), ld, a(j, c), ld, a(j + jb, c), ld,
-                          ctx->d_status, ctx->s_upd));
+                          ctx->d_status, ctx->s_upd, max_ctas));
       CK(cudaEventRecord(e1, ctx->s_upd));
       ctx->launches += 1;
       gemm_ev.emplace_back(e0, e1);
@@ -212,6 +211,12 @@ hplb_status hplb_set_option(hplb_ctx* ctx, int option, int value) {
       if(value < HPLB_LEAF_AUTO || value > HPLB_LEAF_REGISTERS)
         return set_err(ctx, HPLB_ERR_ARG, "hplb_set_option: leaf kind %d out of range", value);
       ctx->leaf_kind = value;
+      return HPLB_OK;
+    case HPLB_OPT_PANEL_SMS:
+      if(value < HPLB_PANEL_SMS_AUTO || value >= ctx->num_sms)
+        return set_err(ctx, HPLB_ERR_ARG, "hplb_set_option: panel SMs %d out of range [-1, %d)",
+                       value, ctx->num_sms);
+      ctx->panel_sms = value;
       return HPLB_OK;
   }
   return set_err(ctx, HPLB_ERR_ARG, "hplb_set_option: unknown option %d", option);
@@ -308,6 +313,13 @@ hplb_status hplb_matgen_block(hplb_ctx* ctx, int64_t mg, int64_t ng, int64_t i0,
 
 }  // extern "C"
 
+// Grid cap of the trailing-update DGEMM of a step whose next panel is
+// factored beside it (0: none), from HPLB_OPT_PANEL_SMS.
+static int update_cap(const hplb_ctx* ctx) {
+  const int keep = ctx->panel_sms == HPLB_PANEL_SMS_AUTO ? 0 : ctx->panel_sms;
+  return keep > 0 ? std::max(1, ctx->num_sms - keep) : 0;
+}
+
 // The factorisation loop shared by hplb_pdgesv (rhs: column n of A is b,
 // carried through the updates, then the back-solve into dX) and hplb_getrf
 // (A alone, no back-solve).
@@ -352,7 +364,8 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
       CK(cudaStreamWaitEvent(ctx->s_pan, ev_la, 0));
       if((s = S.panel(c1, set ^ 1, ev_panel[set ^ 1])) != HPLB_OK) return s;
     }
-    if((s = S.update(j, set, c1 + la, n + (rhs ? 1 : 0) - (c1 + la))) != HPLB_OK) return s;
+    const int cap = la > 0 ? update_cap(ctx) : 0;
+    if((s = S.update(j, set, c1 + la, n + (rhs ? 1 : 0) - (c1 + la), cap)) != HPLB_OK) return s;
     // Step j ends when its trailing update is done (the update stream has
     // already waited for panel j); the progress report reads these.
     step_end.push_back(next_event(ctx));

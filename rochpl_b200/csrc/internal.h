@@ -17,9 +17,11 @@ cudaError_t launch_matgen_block(int64_t mg, int64_t i0, int64_t j0, int m, int n
 // C -= A B.  Uses the TMA-fed warp-specialised kernel when the operands
 // qualify (dgemm_tma_eligible), the cp.async kernel otherwise.  status may be
 // null (then only the cp.async kernel, which has no waits, is used).
+// max_ctas > 0 caps the TMA kernel's grid (each CTA then walks a longer run of
+// tiles), leaving the other SMs free for concurrent work.
 cudaError_t launch_dgemm_sub(int m, int n, int k, const double* A, int64_t lda,
                              const double* B, int64_t ldb, double* C, int64_t ldc,
-                             int* status, cudaStream_t stream);
+                             int* status, cudaStream_t stream, int max_ctas = 0);
 // C = A B (store form of the same kernels; C is not read).
 cudaError_t launch_dgemm_set(int m, int n, int k, const double* A, int64_t lda,
                              const double* B, int64_t ldb, double* C, int64_t ldc,
@@ -28,7 +30,8 @@ bool        dgemm_tma_eligible(int m, int n, int k, const double* A, int64_t lda
                                const double* B, int64_t ldb);
 cudaError_t launch_dgemm_tma(int m, int n, int k, const double* A, int64_t lda,
                              const double* B, int64_t ldb, double* C, int64_t ldc,
-                             int* status, bool accumulate, cudaStream_t stream);
+                             int* status, bool accumulate, cudaStream_t stream,
+                             int max_ctas = 0);
 cudaError_t launch_dgemm_cpasync(int m, int n, int k, const double* A, int64_t lda,
                                  const double* B, int64_t ldb, double* C, int64_t ldc,
                                  bool accumulate, cudaStream_t stream);
@@ -54,10 +57,20 @@ template <typename T>
 cudaError_t launch_diag_inv(const T* A, int64_t ld, int r0, int c0, int n, T* inv,
                             cudaStream_t stream);
 int         trsm_wcol(int jb);
-size_t      trsm_smem_bytes(int jb);
+size_t      trsm_smem_bytes(int jb, bool own_dinv);
+// Largest jb for which launch_laswp_trsm may be given dinv = null (the kernel
+// then inverts the diagonal blocks itself).
+constexpr int kFusedTri = 256;
 template <typename T>
 cudaError_t launch_laswp_trsm(T* A, int64_t ld, int ia, int jb, int lc, const int* permU,
                               const T* dinv, int c0, int n, cudaStream_t stream);
+// U12 = L11^-1 A12 of one node of the recursive panel (L11 the unit-lower
+// jb x jb block at (ia, lc), A12 rows [ia, ia+jb) of columns [c0, c0+n)): one
+// launch for jb <= kFusedTri, else diag_inv into dinv_scratch and the TRSM.
+// Adds the kernels it launched to *launches.
+template <typename T>
+cudaError_t launch_trsm_node(T* A, int64_t ld, int ia, int jb, int lc, T* dinv_scratch, int c0,
+                             int n, cudaStream_t stream, int* launches);
 // Linv (jb x jb, leading dimension ldinv) = L^-1 for the unit-lower L at L
 // (leading dimension ldl), by the blocked substitution applied to the identity.
 template <typename T>

@@ -72,13 +72,12 @@ struct Mixed {
         rem -= jb;
         if((s = rpanel(r0 + jj, c0 + jj, jb, pc, pw)) != HPLB_OK) return s;
         if(rem > 0) {
-          CK(launch_diag_inv<float>(W, ldw, r0 + jj, c0 + jj, jb, dinv_piece(), st));
-          CK(launch_laswp_trsm<float>(W, ldw, r0 + jj, jb, c0 + jj, nullptr, dinv_piece(),
-                                      c0 + jj + jb, rem, st));
+          CK(launch_trsm_node<float>(W, ldw, r0 + jj, jb, c0 + jj, dinv_piece(), c0 + jj + jb,
+                                     rem, st, &ctx->launches));
           CK(launch_sgemm(n - (r0 + jj + jb), rem, jb, w(r0 + jj + jb, c0 + jj), ldw,
                           w(r0 + jj, c0 + jj + jb), ldw, w(r0 + jj + jb, c0 + jj + jb), ldw,
                           true, st));
-          ctx->launches += 3;
+          ctx->launches += 1;
         }
         jj += jb;
         jb = std::min(rem, nbs);
@@ -88,11 +87,11 @@ struct Mixed {
         rem -= jb;
         const int cj = c0 + jj;
         if(jj > 0) {
-          CK(launch_diag_inv<float>(W, ldw, r0, c0, jj, dinv_piece(), st));
-          CK(launch_laswp_trsm<float>(W, ldw, r0, jj, c0, nullptr, dinv_piece(), cj, jb, st));
+          CK(launch_trsm_node<float>(W, ldw, r0, jj, c0, dinv_piece(), cj, jb, st,
+                                     &ctx->launches));
           CK(launch_sgemm(n - (r0 + jj), jb, jj, w(r0 + jj, c0), ldw, w(r0, cj), ldw,
                           w(r0 + jj, cj), ldw, true, st));
-          ctx->launches += 3;
+          ctx->launches += 1;
         }
         if((s = rpanel(r0 + jj, cj, jb, pc, pw)) != HPLB_OK) return s;
         jj += jb;

@@ -874,6 +874,10 @@ __global__ void diag_inv_kernel(const T* A, int64_t ld, int r0, int c0, int n, T
 //   semantics: gather the new top rows, send displaced top rows down).
 //   Then X := L^-1 X with L the unit-lower jb x jb block at (ia, lc), blocked
 //   by kTri rows: X_b = Dinv_b (X_b - L(b, 0:b) X(0:b)).
+//   dinv: the diagonal blocks' inverses (diag_inv_kernel), or null for
+//   jb <= kFusedTri: then every CTA inverts them itself into shared memory
+//   first (a warp per block, the operations of diag_inv_kernel), which saves
+//   the recursion a launch per node.
 template <int WCOL, typename T>
 __global__ void __launch_bounds__(256)
 laswp_trsm_kernel(T* A, int64_t ld, int ia, int jb, const T* L, int64_t ldl,
@@ -884,6 +888,32 @@ laswp_trsm_kernel(T* A, int64_t ld, int ia, int jb, const T* L, int64_t ldl,
   const int cb  = c0 + blockIdx.x * WCOL;
   const int nc  = min(WCOL, c0 + n - cb);
   const size_t lds = (size_t)ld;
+  constexpr int kSlot = kTri * (kTri + 1);
+  T* sD = sx + (size_t)WCOL * ldx;  // [nblk][kTri][kTri + 1] when dinv is null
+
+  if(!dinv) {
+    const int lane = threadIdx.x & 31;
+    for(int b = threadIdx.x >> 5; b * kTri < jb; b += blockDim.x >> 5) {
+      T*        slot = sD + (size_t)b * kSlot;
+      const int base = b * kTri;
+      for(int c = 0; c < kTri; ++c) {  // row `lane` of the block, row-major
+        const bool in = (base + lane < jb) && (base + c < jb);
+        slot[lane * (kTri + 1) + c] = in ? L[(size_t)(base + lane) + (size_t)(base + c) * ldl] : (T)0;
+      }
+      __syncwarp();
+      T x[kTri];  // column `lane` of the inverse, by forward substitution
+#pragma unroll
+      for(int i = 0; i < kTri; ++i) {
+        T s = (i == lane) ? (T)1 : (T)0;
+#pragma unroll
+        for(int k = 0; k < i; ++k) s -= slot[i * (kTri + 1) + k] * x[k];
+        x[i] = (i < lane) ? (T)0 : s;
+      }
+      __syncwarp();
+#pragma unroll
+      for(int i = 0; i < kTri; ++i) slot[lane * (kTri + 1) + i] = x[i];  // Dinv(i, lane)
+    }
+  }
 
   // Load the top block; with permU, gather the new top rows first (the old
   // top rows are still intact in global memory), then send displaced top
@@ -952,13 +982,14 @@ laswp_trsm_kernel(T* A, int64_t ld, int ia, int jb, const T* L, int64_t ldl,
       if(gr < jb) sx[(size_t)c * ldx + gr] = rv[q];
     }
     __syncthreads();
-    const T* D = dinv + (size_t)b * kTri * kTri;
+    const T*  D    = dinv ? dinv + (size_t)b * kTri * kTri : sD + (size_t)b * kSlot;
+    const int dstr = dinv ? kTri : kTri + 1;
 #pragma unroll
     for(int q = 0; q < CPT; ++q) acc[q] = (T)0;
     {
       T dv[kTri];  // row r of Dinv_b, all loads in flight at once
 #pragma unroll
-      for(int kk = 0; kk < kTri; ++kk) dv[kk] = D[(size_t)kk * kTri + r];
+      for(int kk = 0; kk < kTri; ++kk) dv[kk] = D[kk * dstr + r];
 #pragma unroll
       for(int kk = 0; kk < kTri; ++kk)
         if(row0 + kk < jb)
@@ -1302,9 +1333,13 @@ cudaError_t launch_diag_inv(const T* A, int64_t ld, int r0, int c0, int n, T* in
 
 int trsm_wcol(int jb) { return jb <= 512 ? 32 : (jb <= 1024 ? 16 : 8); }
 
-size_t trsm_smem_bytes(int jb) {
+// Shared memory of laswp_trsm_kernel (sized for double; ample for float):
+// the X block, plus the diagonal inverses when the kernel makes them.
+size_t trsm_smem_bytes(int jb, bool own_dinv) {
   const int w = trsm_wcol(jb);
-  return (size_t)w * (jb + 1) * 8;
+  size_t    b = (size_t)w * (jb + 1) * 8;
+  if(own_dinv) b += (size_t)((jb + kTri - 1) / kTri) * kTri * (kTri + 1) * 8;
+  return b;
 }
 
 template <int W, typename T>
@@ -1324,8 +1359,9 @@ static cudaError_t launch_trsm_any(T* X, int64_t ldx, int ia, int jb, const T* L
                                    const int* permU, const T* dinv, int c0, int n,
                                    cudaStream_t stream) {
   if(n <= 0 || jb <= 0) return cudaSuccess;
+  if(!dinv && jb > kFusedTri) return cudaErrorInvalidValue;
   const int    w    = trsm_wcol(jb);
-  const size_t smem = trsm_smem_bytes(jb);  // sized for double; ample for float
+  const size_t smem = trsm_smem_bytes(jb, !dinv);
   const int    grid = (n + w - 1) / w;
   switch(w) {
     case 32:
@@ -1342,6 +1378,20 @@ cudaError_t launch_laswp_trsm(T* A, int64_t ld, int ia, int jb, int lc, const in
                               const T* dinv, int c0, int n, cudaStream_t stream) {
   return launch_trsm_any<T>(A, ld, ia, jb, A + (size_t)ia + (size_t)lc * ld, ld, permU, dinv, c0,
                             n, stream);
+}
+
+template <typename T>
+cudaError_t launch_trsm_node(T* A, int64_t ld, int ia, int jb, int lc, T* dinv_scratch, int c0,
+                             int n, cudaStream_t stream, int* launches) {
+  if(n <= 0 || jb <= 0) return cudaSuccess;
+  if(jb <= kFusedTri) {
+    *launches += 1;
+    return launch_laswp_trsm<T>(A, ld, ia, jb, lc, nullptr, nullptr, c0, n, stream);
+  }
+  cudaError_t e = launch_diag_inv<T>(A, ld, ia, lc, jb, dinv_scratch, stream);
+  if(e != cudaSuccess) return e;
+  *launches += 2;
+  return launch_laswp_trsm<T>(A, ld, ia, jb, lc, nullptr, dinv_scratch, c0, n, stream);
 }
 
 // X (jb x n, leading dimension ldx) <- L^-1 X for the unit-lower jb x jb L at
@@ -1385,6 +1435,8 @@ cudaError_t launch_laswp_gather(T* A, int64_t ld, int ia, int jb, const int* per
   template cudaError_t launch_diag_inv<T>(const T*, int64_t, int, int, int, T*, cudaStream_t); \
   template cudaError_t launch_laswp_trsm<T>(T*, int64_t, int, int, int, const int*, const T*,  \
                                             int, int, cudaStream_t);                           \
+  template cudaError_t launch_trsm_node<T>(T*, int64_t, int, int, int, T*, int, int,            \
+                                           cudaStream_t, int*);                                \
   template cudaError_t launch_unit_lower_inverse<T>(const T*, int64_t, int, const T*, T*,      \
                                                     int64_t, cudaStream_t);                    \
   template cudaError_t launch_laswp_gather<T>(T*, int64_t, int, int, const int*, T*, int64_t,  \

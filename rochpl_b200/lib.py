@@ -73,6 +73,7 @@ PREC_BF16, PREC_FP16, PREC_BF16X3, PREC_FP16X3 = 0, 1, 2, 3
 # hplb_set_option options and values
 HPLB_OPT_LEAF = 1
 LEAF_AUTO, LEAF_SHARED, LEAF_GLOBAL, LEAF_REGISTERS = 0, 1, 2, 3
+HPLB_OPT_PANEL_SMS, PANEL_SMS_AUTO = 2, -1
 
 
 class HplError(RuntimeError):
@@ -234,6 +235,11 @@ class Library:
         """hplb_set_option(HPLB_OPT_LEAF): LEAF_AUTO, LEAF_REGISTERS, LEAF_SHARED or
         LEAF_GLOBAL."""
         self._check(self.L.hplb_set_option(self.ctx, HPLB_OPT_LEAF, int(kind)))
+
+    def set_panel_sms(self, sms: int):
+        """hplb_set_option(HPLB_OPT_PANEL_SMS): PANEL_SMS_AUTO (-1), 0, or the
+        SMs the trailing-update DGEMM leaves to the panel stream."""
+        self._check(self.L.hplb_set_option(self.ctx, HPLB_OPT_PANEL_SMS, int(sms)))
 
     def getrf(self, algo: hplb_algo, n: int, A: int, ld: int, ipiv: int | None = None) -> int:
         """hplb_getrf: factor A alone; returns info (0, or the first zero pivot)."""

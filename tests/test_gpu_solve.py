@@ -75,6 +75,28 @@ def test_leaf_kinds_give_identical_results(hlib, oracle):
         hlib.set_leaf(4)
 
 
+def test_panel_sms_cap_gives_identical_results(hlib, oracle):
+    """hplb_set_option(HPLB_OPT_PANEL_SMS) only changes how the trailing
+    update's tiles are spread over CTAs, never a tile's arithmetic: capped and
+    uncapped solves give the oracle's pivots and bit-identical x; values
+    outside [-1, SMs) are rejected."""
+    from rochpl_b200.lib import PANEL_SMS_AUTO, HplError
+
+    xs = []
+    try:
+        for keep in (PANEL_SMS_AUTO, 0, 16, 100):
+            hlib.set_panel_sms(keep)
+            r = solve_both(hlib, oracle, 4096, 256, 32)
+            assert np.array_equal(r["ipiv"], r["po"]), keep
+            xs.append(r["x"])
+    finally:
+        hlib.set_panel_sms(PANEL_SMS_AUTO)
+    assert all(np.array_equal(x.view(np.uint64), xs[0].view(np.uint64)) for x in xs)
+    for bad in (-2, 100000):
+        with pytest.raises(HplError):
+            hlib.set_panel_sms(bad)
+
+
 def test_solve_parity_n16384_against_the_oracle(hlib, oracle):
     """The parity solve at N = 16384, NB = 512 (the size the bench's CPU leg
     factors): identical pivot vectors, x within 64 N eps kappa_oo of the
