@@ -108,11 +108,12 @@ hplb_status hplb_set_stream(hplb_ctx* ctx, void* stream);
 /*   HPLB_OPT_PANEL_SMS: SMs that the trailing-update DGEMM leaves to the panel
  *   factorisation while the next panel is being factored beside it: 0 (the
  *   DGEMM may take every SM; the high-priority panel kernels take SMs as its
- *   CTAs retire), or k > 0 (the DGEMM's grid is capped at SMs - k CTAs, each
- *   walking a longer run of tiles).  HPLB_PANEL_SMS_AUTO (-1, the default) is
- *   0 on B200: a cap of 8 to 48 SMs slowed the solve at N = 4096 to 32768,
- *   because the panel's own GEMMs and triangular solves then run on the few
- *   SMs left to them.  Results do not depend on it. */
+ *   CTAs retire), or k > 0 in every step (the DGEMM's grid is capped at
+ *   SMs - k CTAs, each walking a longer run of tiles).  HPLB_PANEL_SMS_AUTO
+ *   (-1, the default) keeps 32 SMs only in the steps whose update is at most 4
+ *   waves of tiles, where the panel is the longer chain; a cap in every step
+ *   slows the solve, because the panel's own GEMMs and triangular solves then
+ *   run on the few SMs left to them.  Results do not depend on it. */
 #define HPLB_OPT_PANEL_SMS 2
 #define HPLB_PANEL_SMS_AUTO (-1)
 hplb_status hplb_set_option(hplb_ctx* ctx, int option, int value);
@@ -152,6 +153,17 @@ hplb_status hplb_matgen_block(hplb_ctx* ctx, int64_t mg, int64_t ng, int64_t i0,
  * HPLB_ERR_SINGULAR after the solve completes. */
 hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA,
                         int64_t ld, double* dX, int* ipiv_out, int* info);
+
+/* hplb_pdgesv for nrhs >= 1 right-hand sides at once: B occupies columns
+ * n .. n + nrhs - 1 of the same column-major array (A | B, leading dimension
+ * ld >= n, n + nrhs columns) and takes every interchange and trailing update
+ * as HPL_pdgesv's column n does, so no separate forward solve is needed; then
+ * X = U^-1 B (device, n x nrhs, leading dimension ldx >= n) by a persistent
+ * back-solve of 32 right-hand sides per launch.  dA, ipiv_out and info as in
+ * hplb_pdgesv; nrhs = 1 gives the same result as hplb_pdgesv.  The reference
+ * carries exactly one right-hand side (include/hpl_pgesv.hpp:162). */
+hplb_status hplb_gesv(hplb_ctx* ctx, const hplb_algo* algo, int n, int nrhs, double* dA,
+                      int64_t ld, double* dX, int64_t ldx, int* ipiv_out, int* info);
 
 /* The factorisation of hplb_pdgesv on the n x n A alone (no right-hand side
  * column, no back-solve): the same panels, pivots and layout, for use with

@@ -1,9 +1,10 @@
 """Differentiable HPL solve: X = A^-1 B as a torch.autograd.Function.
 
-Forward: hplb_getrf factors a column-major copy of A with the HPL panel
+Forward: hplb_gesv factors a column-major copy of [A | B] with the HPL panel
 algorithm (partial pivoting, recursive panel, look-ahead; the same kernels as
-hplb_pdgesv), then hplb_getrs solves for the columns of B.  The factors and
-pivots are saved for the backward pass, which never refactors:
+hplb_pdgesv), B riding through the interchanges and updates as HPL's b does,
+then back-solves with U for the columns of X.  The factors and pivots are
+saved for the backward pass, which never refactors:
 
     Bbar = A^-T Xbar      hplb_getrs(trans = 1) on the stored LU and pivots
     Abar = -Bbar X^T      hplb_rank_k, one fused rank-nrhs kernel
@@ -58,14 +59,22 @@ class HplSolve(torch.autograd.Function):
         # column stride (n = 16384) maps every column to the same L2 sets and
         # DRAM channels and slows the factorisation.
         ld = int(default_ld(n)) if n > 0 else 1
-        LU = _colmajor(A.detach(), ld)
+        # [A | B] column-major in one buffer: B takes every interchange and
+        # trailing update with the factorisation (hplb_gesv), so the forward
+        # needs only the back-solve with U afterwards.
+        LU = torch.empty((n + nrhs, ld), dtype=torch.float64, device=A.device)
+        LU[:n, :n].copy_(A.detach().t())
+        LU[n:, :n].copy_(B.detach().t())
         ipiv = torch.zeros(max(n, 1), dtype=torch.int32, device=A.device)
-        info = lib.getrf(Algo(nbe, min(nbmin, nbe), 2, 2, 2, 1, 0).c(), n, LU.data_ptr(), ld,
-                         ipiv.data_ptr())
+        Xc = torch.empty((nrhs, n), dtype=torch.float64, device=A.device)
+        algo = Algo(nbe, min(nbmin, nbe), 2, 2, 2, 1, 0).c()
+        if nrhs > 0:
+            info = lib.gesv(algo, n, nrhs, LU.data_ptr(), ld, Xc.data_ptr(), max(n, 1),
+                            ipiv.data_ptr())
+        else:
+            info = lib.getrf(algo, n, LU.data_ptr(), ld, ipiv.data_ptr())
         if info:
             raise HplError(3, f"hpl_solve: A is singular (zero pivot in column {info})")
-        Xc = _colmajor(B.detach())
-        lib.getrs(0, n, nbe, nrhs, LU.data_ptr(), ld, ipiv.data_ptr(), Xc.data_ptr(), max(n, 1))
         ctx.save_for_backward(LU, ipiv, Xc)
         ctx.nb = nbe
         ctx.ld = ld

@@ -313,18 +313,27 @@ hplb_status hplb_matgen_block(hplb_ctx* ctx, int64_t mg, int64_t ng, int64_t i0,
 
 }  // extern "C"
 
-// Grid cap of the trailing-update DGEMM of a step whose next panel is
-// factored beside it (0: none), from HPLB_OPT_PANEL_SMS.
-static int update_cap(const hplb_ctx* ctx) {
-  const int keep = ctx->panel_sms == HPLB_PANEL_SMS_AUTO ? 0 : ctx->panel_sms;
+// Grid cap of the trailing-update DGEMM (m x w) of a step whose next panel
+// is factored beside it (0: none), from HPLB_OPT_PANEL_SMS.  Automatic: 32 SMs
+// stay with the panel once the update is at most 4 waves of 128 x 128 tiles
+// (the steps where the panel, not the update, is the longer of the two).
+static int update_cap(const hplb_ctx* ctx, int m, int w) {
+  int keep = ctx->panel_sms;
+  if(keep == HPLB_PANEL_SMS_AUTO) {
+    const long long tiles = (long long)((m + 127) / 128) * ((w + 127) / 128);
+    keep = tiles <= 4LL * ctx->num_sms ? 32 : 0;
+  }
   return keep > 0 ? std::max(1, ctx->num_sms - keep) : 0;
 }
 
-// The factorisation loop shared by hplb_pdgesv (rhs: column n of A is b,
-// carried through the updates, then the back-solve into dX) and hplb_getrf
-// (A alone, no back-solve).
+// The factorisation loop shared by hplb_pdgesv (nrhs = 1: column n of A is b,
+// carried through the updates, then the back-solve into dX), hplb_gesv
+// (columns n .. n + nrhs - 1 are B, then the multi-RHS back-solve into dX,
+// leading dimension ldx) and hplb_getrf (nrhs = 0: A alone, no back-solve).
 static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA,
-                                 int64_t ld, double* dX, int* ipiv_out, int* info, bool rhs) {
+                                 int64_t ld, double* dX, int64_t ldx, int* ipiv_out, int* info,
+                                 int nrhs) {
+  const bool rhs = nrhs > 0;
   if(!ctx) return HPLB_ERR_ARG;
   hplb_status s = check_algo(ctx, algo, n, ld, true);
   if(s != HPLB_OK) return s;
@@ -364,8 +373,8 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
       CK(cudaStreamWaitEvent(ctx->s_pan, ev_la, 0));
       if((s = S.panel(c1, set ^ 1, ev_panel[set ^ 1])) != HPLB_OK) return s;
     }
-    const int cap = la > 0 ? update_cap(ctx) : 0;
-    if((s = S.update(j, set, c1 + la, n + (rhs ? 1 : 0) - (c1 + la), cap)) != HPLB_OK) return s;
+    const int cap = la > 0 ? update_cap(ctx, n - c1, n + nrhs - (c1 + la)) : 0;
+    if((s = S.update(j, set, c1 + la, n + nrhs - (c1 + la), cap)) != HPLB_OK) return s;
     // Step j ends when its trailing update is done (the update stream has
     // already waited for panel j); the progress report reads these.
     step_end.push_back(next_event(ctx));
@@ -373,7 +382,11 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
     ctx->step_col.push_back(j);
   }
   CK(cudaEventRecord(ev_lu, ctx->s_upd));
-  if(rhs) CK(launch_trsv(dA, ld, n, dX, ctx->d_trsv, ctx->d_status, ctx->s_upd, &ctx->launches));
+  if(nrhs == 1)
+    CK(launch_trsv(dA, ld, n, dX, ctx->d_trsv, ctx->d_status, ctx->s_upd, &ctx->launches));
+  else if(nrhs > 1)
+    CK(launch_trsm_upper(dA, ld, n, nrhs, dA + (size_t)n * (size_t)ld, ld, dX, ldx, ctx->d_trsv,
+                         ctx->d_status, ctx->s_upd, &ctx->launches));
   if(ipiv_out)
     CK(cudaMemcpyAsync(ipiv_out, ctx->d_ipiv, (size_t)n * sizeof(int), cudaMemcpyDeviceToDevice,
                        ctx->s_upd));
@@ -420,12 +433,20 @@ extern "C" {
 
 hplb_status hplb_pdgesv(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA, int64_t ld,
                         double* dX, int* ipiv_out, int* info) {
-  return factor_driver(ctx, algo, n, dA, ld, dX, ipiv_out, info, true);
+  return factor_driver(ctx, algo, n, dA, ld, dX, n, ipiv_out, info, 1);
+}
+
+hplb_status hplb_gesv(hplb_ctx* ctx, const hplb_algo* algo, int n, int nrhs, double* dA,
+                      int64_t ld, double* dX, int64_t ldx, int* ipiv_out, int* info) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(nrhs < 1) return set_err(ctx, HPLB_ERR_ARG, "hplb_gesv: nrhs must be >= 1");
+  if(n > 0 && ldx < n) return set_err(ctx, HPLB_ERR_ARG, "hplb_gesv: ldx < n");
+  return factor_driver(ctx, algo, n, dA, ld, dX, ldx, ipiv_out, info, nrhs);
 }
 
 hplb_status hplb_getrf(hplb_ctx* ctx, const hplb_algo* algo, int n, double* dA, int64_t ld,
                        int* ipiv_out, int* info) {
-  return factor_driver(ctx, algo, n, dA, ld, nullptr, ipiv_out, info, false);
+  return factor_driver(ctx, algo, n, dA, ld, nullptr, 0, ipiv_out, info, 0);
 }
 
 static hplb_status residual_common(hplb_ctx* ctx, int n, const double* dA, int64_t ld, bool lcg,

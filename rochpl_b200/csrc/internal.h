@@ -95,6 +95,12 @@ cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* flag
 cudaError_t launch_trsv_y(const double* A, int64_t ld, int n, const double* Y, double* X,
                           int* flags, int* status, cudaStream_t stream, int* launches);
 // z[0:m] += U[0:m, 0:k] x (U column-major, leading dimension ld); r = y - s.
+// X (n x nrhs, leading dimension ldx) = U^-1 Y for the upper triangle of A
+// (n x n, leading dimension ld); Y (leading dimension ldy) may be X itself.
+// Persistent, one launch per 32 right-hand sides; flags: trsv_flag_ints(n).
+cudaError_t launch_trsm_upper(const double* A, int64_t ld, int n, int nrhs, const double* Y,
+                              int64_t ldy, double* X, int64_t ldx, int* flags, int* status,
+                              cudaStream_t stream, int* launches);
 cudaError_t launch_gemv_acc(int m, int k, const double* U, int64_t ld, const double* x,
                             double* z, cudaStream_t stream);
 cudaError_t launch_vsub(int n, const double* y, const double* s, double* r, cudaStream_t stream);

@@ -104,6 +104,11 @@ struct Rhs {
       CK(update(n - j - jb, jb, lu(j + jb, j), ld, b(j), ldb, b(j + jb), ldb));
       ctx->launches += 3;
     }
+    if(nrhs <= 128) {  // U X = Y in one persistent launch per 32 right-hand sides
+      CK(launch_trsm_upper(LU, ld, n, nrhs, B, ldb, B, ldb, ctx->d_trsv, ctx->d_status, st,
+                           &ctx->launches));
+      return HPLB_OK;
+    }
     for(int j = (n - 1) / nb * nb; j >= 0; j -= nb) {
       const int jb = std::min(nb, n - j);
       if((s = solve_view(0, j, jb)) != HPLB_OK) return s;
@@ -181,6 +186,7 @@ hplb_status hplb_getrs(hplb_ctx* ctx, int trans, int n, int nb, int nrhs, const 
      (s = grow(ctx, &ctx->r_perm, &ctx->r_perm_cap, 2 * (size_t)R.nb)) != HPLB_OK)
     return s;
   if(trans && (s = grow(ctx, &ctx->r_t, &ctx->r_t_cap, (size_t)R.ldt * n)) != HPLB_OK) return s;
+  if((s = grow(ctx, &ctx->d_trsv, &ctx->trsv_cap, trsv_flag_ints(n))) != HPLB_OK) return s;
   R.carve(ctx->r_ws);
   R.perm = ctx->r_perm;
   R.T    = ctx->r_t;

@@ -30,7 +30,7 @@ EXPORTS = [
     "hplb_set_stream", "hplb_set_option", "hplb_batch_create", "hplb_batch_destroy", "hplb_batch_layout",
     "hplb_batch_matgen", "hplb_batch_gesv", "hplb_batch_getrs", "hplb_batch_rank_k",
     "hplb_batch_residual", "hplb_batch_last_ms", "hplb_batch_tune",
-    "hplb_panel_factor", "hplb_panel_update", "hplb_trsv_block",
+    "hplb_panel_factor", "hplb_panel_update", "hplb_trsv_block", "hplb_gesv",
 ]
 
 HPLB_BATCH_CLASSES = 6
@@ -150,6 +150,9 @@ def load() -> C.CDLL:
     L.hplb_getrf.restype = i32
     L.hplb_getrs.argtypes = [vp, i32, i32, i32, i32, vp, i64, vp, vp, i64]
     L.hplb_getrs.restype = i32
+    L.hplb_gesv.argtypes = [vp, C.POINTER(hplb_algo), i32, i32, vp, i64, vp, i64, vp,
+                            C.POINTER(C.c_int)]
+    L.hplb_gesv.restype = i32
     L.hplb_panel_factor.argtypes = [vp, C.POINTER(hplb_algo), i32, i32, i32, vp, i64, i32, vp,
                                     C.POINTER(C.c_int)]
     L.hplb_panel_factor.restype = i32
@@ -206,6 +209,16 @@ class Library:
         info = C.c_int(0)
         st = self.L.hplb_pdgesv(self.ctx, C.byref(algo), n, A, ld, X, ipiv or None,
                                 C.byref(info))
+        self._check(st, allow=(HPLB_OK, HPLB_ERR_SINGULAR))
+        return info.value
+
+    def gesv(self, algo: hplb_algo, n: int, nrhs: int, A: int, ld: int, X: int, ldx: int,
+             ipiv: int | None = None) -> int:
+        """hplb_gesv: factor [A | B] (B in columns n .. n + nrhs - 1 of A) and
+        write X = A^-1 B (n x nrhs, leading dimension ldx); returns info."""
+        info = C.c_int(0)
+        st = self.L.hplb_gesv(self.ctx, C.byref(algo), n, nrhs, A, ld, X, ldx, ipiv or None,
+                              C.byref(info))
         self._check(st, allow=(HPLB_OK, HPLB_ERR_SINGULAR))
         return info.value
 

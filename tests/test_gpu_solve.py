@@ -75,6 +75,50 @@ def test_leaf_kinds_give_identical_results(hlib, oracle):
         hlib.set_leaf(4)
 
 
+@pytest.mark.parametrize("n,nb,nrhs,ld", [(1, 1, 3, None), (100, 32, 2, None), (500, 64, 5, 501),
+                                          (1031, 96, 33, None), (2048, 256, 1, None),
+                                          (2048, 256, 32, None), (4096, 512, 70, None)])
+def test_gesv_multi_rhs(hlib, oracle, n, nb, nrhs, ld):
+    """hplb_gesv: B in columns n .. n + nrhs - 1 of [A | B] rides through the
+    factorisation.  The factors and pivots are bit-identical to hplb_pdgesv's
+    on the same A (the extra columns never feed back into A), every column of
+    X is within 64 n eps kappa_oo of LAPACK's solve, and with one right-hand
+    side x is hplb_pdgesv's x bit for bit (the same back-solve kernel).  An
+    odd ld takes the back-solve's 8-byte staging path."""
+    import torch
+
+    from rochpl_b200.hpl import Algo
+
+    ld = ld or oracle.default_ld(n)
+    algo = Algo(nb, min(32, nb), 2, 2, 2, 1, 0).c()
+    dAB = torch.empty(ld * (n + nrhs), dtype=torch.float64, device="cuda")
+    hlib.matgen(n, n + nrhs, 7, dAB.data_ptr(), ld, nb)
+    AB = dAB.view(n + nrhs, ld).cpu().numpy()
+    A0, B0 = AB[:n, :n].T.copy(), AB[n:, :n].T.copy()
+    dX = torch.full((nrhs, n), float("nan"), dtype=torch.float64, device="cuda")
+    dP = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert hlib.gesv(algo, n, nrhs, dAB.data_ptr(), ld, dX.data_ptr(), n, dP.data_ptr()) == 0
+
+    dA1 = torch.empty(ld * (n + 1), dtype=torch.float64, device="cuda")
+    hlib.matgen(n, n + 1, 7, dA1.data_ptr(), ld, nb)
+    dx1 = torch.zeros(n, dtype=torch.float64, device="cuda")
+    dP1 = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert hlib.pdgesv(algo, n, dA1.data_ptr(), ld, dx1.data_ptr(), dP1.data_ptr()) == 0
+    assert np.array_equal(dP.cpu().numpy(), dP1.cpu().numpy())
+    f_multi = dAB[: ld * n].view(n, ld)[:, :n].cpu().numpy().view(np.uint64)
+    f_one = dA1[: ld * n].view(n, ld)[:, :n].cpu().numpy().view(np.uint64)
+    assert np.array_equal(f_multi, f_one)
+
+    X = dX.cpu().numpy().T
+    Xr = np.linalg.solve(A0, B0)
+    kappa = np.linalg.cond(A0, np.inf)
+    tol = 64 * n * EPS * kappa
+    err = np.max(np.abs(X - Xr), axis=0) / np.max(np.abs(Xr), axis=0)
+    assert np.all(err <= tol), (err.max(), tol)
+    if nrhs == 1:
+        assert np.array_equal(X[:, 0].view(np.uint64), dx1.cpu().numpy().view(np.uint64))
+
+
 def test_panel_sms_cap_gives_identical_results(hlib, oracle):
     """hplb_set_option(HPLB_OPT_PANEL_SMS) only changes how the trailing
     update's tiles are spread over CTAs, never a tile's arithmetic: capped and
