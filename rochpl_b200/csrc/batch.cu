@@ -284,26 +284,35 @@ HPLB_DEV int next_system(const Args& a, Smem& S) {
   return S.next;
 }
 
-// x[c] for a column index c known only at run time, by selects over the
-// row's registers (so the row stays in registers).
+// x[c] for a column index c < KB known only at run time, by a tree of
+// selects on the bits of c (log2 KB deep; the row stays in registers).
 template <int KB>
 HPLB_DEV double pick(const double (&x)[KB], int c) {
-  double s = x[0];
+  static_assert((KB & (KB - 1)) == 0, "pick: KB must be a power of two");
+  double t[KB];
 #pragma unroll
-  for(int q = 1; q < KB; ++q) s = (q == c) ? x[q] : s;
-  return s;
+  for(int q = 0; q < KB; ++q) t[q] = x[q];
+#pragma unroll
+  for(int h = KB / 2; h >= 1; h /= 2)
+#pragma unroll
+    for(int q = 0; q < h; ++q) t[q] = (c & h) ? t[q + h] : t[q];
+  return t[0];
 }
 
 // The m x kb panel at A (leading dimension lda; rows k0.. of the system),
 // kb <= KB, with each thread's rows t + q * kBT (q < RPT) in registers.  The
 // column loop is a run-time loop whose body touches every register of the row
-// (selects and predicated updates), so the code stays a few KB and is fetched
-// once, not once per column.  Per column: each warp finds its candidate by
-// shuffles and publishes it with the row's values, the owner of the diagonal
-// row publishes that row, one barrier, then every thread picks the winner and
-// applies the interchange, the division by the pivot and the update to its own
-// rows.  The factored panel goes back to A and, if P is given, to the shared
-// copy P (leading dimension ldp) that the trailing update reads L21 from.
+// (selects and FMAs), so the code stays a few KB and is fetched once, not once
+// per column.  Per column: each warp finds its candidate by shuffles and
+// publishes it with the row's values, the owner of the diagonal row publishes
+// that row, one barrier, then every thread picks the winner and applies the
+// interchange, the scaling by the pivot's reciprocal (as LAPACK's dgetf2) and
+// the update to its own rows.  The update runs against the pivot row with its
+// entries of columns <= j selected to zero, so each entry costs one FMA and two
+// selects, no branch; a non-finite multiplier keeps the predicated form, which
+// leaves the columns before j untouched.  The factored
+// panel goes back to A and, if P is given, to the shared copy P (leading
+// dimension ldp) that the trailing update reads L21 from.
 template <int RPT, int KB>
 __device__ __noinline__ void panel_reg(double* Ag, int lda, int m, int kb, int k0, int* ip, double* P, int ldp,
                         Smem& S) {
@@ -362,6 +371,7 @@ __device__ __noinline__ void panel_reg(double* Ag, int lda, int m, int kb, int k
       ip[k0 + j] = k0 + br;
       if(bv == 0.0 && S.info == 0) S.info = k0 + j + 1;
     }
+    const double rcp = bv != 0.0 ? 1.0 / bv : 0.0;
 #pragma unroll
     for(int q = 0; q < RPT; ++q) {
       if(row[q] == j) {
@@ -372,11 +382,20 @@ __device__ __noinline__ void panel_reg(double* Ag, int lda, int m, int kb, int k
         for(int c = 0; c < KB; ++c) x[q][c] = S.pr.cur[par][c];
       }
       if(bv != 0.0 && row[q] > j) {
-        const double l = pick(x[q], j) / bv;
+        const double l = pick(x[q], j) * rcp;
+        if(isfinite(l)) {
 #pragma unroll
-        for(int c = 0; c < KB; ++c) {
-          if(c == j) x[q][c] = l;
-          else if(c > j) x[q][c] = x[q][c] - l * u[c];
+          for(int c = 0; c < KB; ++c) {
+            const double uc = u[c];
+            const double nx = fma(-l, c > j ? uc : 0.0, x[q][c]);
+            x[q][c]         = (c == j) ? l : nx;
+          }
+        } else {
+#pragma unroll
+          for(int c = 0; c < KB; ++c) {
+            if(c == j) x[q][c] = l;
+            else if(c > j) x[q][c] = fma(-l, u[c], x[q][c]);
+          }
         }
       }
     }
@@ -720,31 +739,43 @@ HPLB_DEV void rec_leaf(double* A, double* B, int n, int nrhs, int* ip, int c0, i
   __syncthreads();
   // Half a warp per column, lane = row of the leaf's top block (w <= 16): the
   // top rows are written as one contiguous segment, and each column's reads
-  // all happen before any of its writes (the half-warp's own column only).
+  // all happen before any of its writes (the half-warp's own columns only).
+  // A half-warp takes kSwapCols columns per trip, so that many columns' loads
+  // are in flight at once.
+  constexpr int kSwapCols = 4;
   const int ncol = n - w + nrhs;
   const int hl   = threadIdx.x & 15;
   const int src  = hl < w ? S.src[hl] : 0;
   const int dst  = hl < w ? S.dst[hl] : -1;
-  // The whole warp iterates together (two columns per trip), so every lane
-  // reaches each __syncwarp; a half-warp past the last column idles.
-  for(int q0 = (threadIdx.x >> 5) * 2; q0 < ncol; q0 += kBT / 16) {
-    const int q  = q0 + ((threadIdx.x >> 4) & 1);
-    const bool on = q < ncol && hl < w;
-    double* col = nullptr;
-    double  v = 0.0, o = 0.0;
-    if(on) {
-      col = q < c0 ? A + (size_t)q * n
-                   : (q < n - w ? A + (size_t)(q + w) * n : B + (size_t)(q - (n - w)) * n);
-      col += c0;
-      v = col[src];
-      if(dst >= 0) o = col[hl];
+  const int half = (threadIdx.x >> 4) & 1;
+  // The whole warp iterates together (2 kSwapCols columns per trip), so every
+  // lane reaches each __syncwarp; a half-warp past the last column idles.
+  for(int q0 = (threadIdx.x >> 5) * 2 * kSwapCols; q0 < ncol; q0 += (kBT / 16) * kSwapCols) {
+    double* col[kSwapCols];
+    double  v[kSwapCols], o[kSwapCols];
+    bool    on[kSwapCols];
+#pragma unroll
+    for(int i = 0; i < kSwapCols; ++i) {
+      const int q = q0 + half + 2 * i;
+      on[i]       = q < ncol && hl < w;
+      col[i]      = nullptr;
+      v[i] = o[i] = 0.0;
+      if(on[i]) {
+        col[i] = (q < c0 ? A + (size_t)q * n
+                         : (q < n - w ? A + (size_t)(q + w) * n : B + (size_t)(q - (n - w)) * n)) +
+                 c0;
+        v[i] = col[i][src];
+        if(dst >= 0) o[i] = col[i][hl];
+      }
     }
     __syncwarp();
-    if(on) {
-      // The displaced old top rows go below the block (dst >= w).
-      if(dst >= 0) col[dst] = o;
-      col[hl] = v;
-    }
+#pragma unroll
+    for(int i = 0; i < kSwapCols; ++i)
+      if(on[i]) {
+        // The displaced old top rows go below the block (dst >= w).
+        if(dst >= 0) col[i][dst] = o[i];
+        col[i][hl] = v[i];
+      }
     __syncwarp();
   }
   __syncthreads();
