@@ -28,7 +28,7 @@ using namespace hplb;
 
 namespace {
 
-hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
+hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin, int nrhs = 1) {
   hplb_status s;
   if((s = grow(ctx, &ctx->d_ipiv, &ctx->ipiv_cap, (size_t)std::max(n, 1))) != HPLB_OK) return s;
   if(nb > ctx->nb_cap) {
@@ -58,7 +58,8 @@ hplb_status ensure_solve_ws(hplb_ctx* ctx, int n, int nb, int nbmin) {
     ctx->nb_cap = nb;
   }
   if(n > 0 &&
-     (s = grow(ctx, &ctx->d_w, &ctx->w_cap, (size_t)nb * (size_t)(n + 1))) != HPLB_OK)
+     (s = grow(ctx, &ctx->d_w, &ctx->w_cap, (size_t)nb * (size_t)(n + std::max(nrhs, 1)))) !=
+         HPLB_OK)
     return s;
   if((s = grow(ctx, &ctx->d_trsv, &ctx->trsv_cap, trsv_flag_ints(std::max(n, 1)))) != HPLB_OK)
     return s;
@@ -344,7 +345,7 @@ static hplb_status factor_driver(hplb_ctx* ctx, const hplb_algo* algo, int n, do
   if(n == 0) return HPLB_OK;
   if(!dA || (rhs && !dX)) return set_err(ctx, HPLB_ERR_ARG, "null matrix or solution");
   ENTER(ctx);
-  s = ensure_solve_ws(ctx, n, algo->nb, algo->nbmin);
+  s = ensure_solve_ws(ctx, n, algo->nb, algo->nbmin, nrhs);
   if(s != HPLB_OK) return s;
 
   ctx->ev_next  = 0;

@@ -75,7 +75,8 @@ def test_leaf_kinds_give_identical_results(hlib, oracle):
         hlib.set_leaf(4)
 
 
-@pytest.mark.parametrize("n,nb,nrhs,ld", [(1, 1, 3, None), (100, 32, 2, None), (500, 64, 5, 501),
+@pytest.mark.parametrize("n,nb,nrhs,ld", [(1, 1, 3, None), (100, 32, 2, None), (100, 8, 70, None),
+                                          (500, 64, 5, 501),
                                           (1031, 96, 33, None), (2048, 256, 1, None),
                                           (2048, 256, 32, None), (4096, 512, 70, None)])
 def test_gesv_multi_rhs(hlib, oracle, n, nb, nrhs, ld):
