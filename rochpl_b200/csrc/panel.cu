@@ -43,12 +43,14 @@ HPLB_DEV bool better(double av, int ar, double bv, int br) {
 }
 
 // Block-wide arg-max in the order of `better`; result valid in every thread.
-// Two barriers: the first also orders this call's writes of s_v / s_r after
-// the previous call's reads.
-HPLB_DEV void block_argmax(double& v, int& r, double* s_v, int* s_r) {
+// Two barriers: the first orders this call's writes of s_v / s_r after the
+// previous call's reads.  With `separated` (every warp has passed a
+// block-wide barrier -- a grid or cluster barrier counts -- since it last read
+// the slots) the first is left out.
+HPLB_DEV void block_argmax(double& v, int& r, double* s_v, int* s_r, bool separated = false) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   warp_argmax(v, r);
-  __syncthreads();
+  if(!separated) __syncthreads();
   if(lane == 0) {
     s_v[warp] = v;
     s_r[warp] = r;
@@ -502,7 +504,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_reg_kernel(LeafParams
         r = row[q];
       }
     }
-    block_argmax(v, r, s_v, s_r);
+    block_argmax(v, r, s_v, s_r, true);  // the grid barrier separates the columns
     double* slot = P.cand + ((size_t)par * G + blockIdx.x) * sw;
     if(threadIdx.x == 0) *reinterpret_cast<double2*>(slot) = make_double2(v, (double)r);
     leaf_rows_publish(x, row, r, d, w, slot + 2, P.cur + par * w);
@@ -660,7 +662,7 @@ __global__ void __launch_bounds__(kRegLeafThreads, 1) leaf_cluster_kernel(LeafPa
         r = row[q];
       }
     }
-    block_argmax(v, r, s_v, s_r);
+    block_argmax(v, r, s_v, s_r, true);  // the cluster barrier separates the columns
     if(threadIdx.x == 0) {
       s_slot[par][0] = v;
       s_slot[par][1] = (double)r;
