@@ -319,11 +319,14 @@ bool get_encoder() {
 // Tiles per CTA.  Four (a whole group: the A tile fetched once and re-read
 // from L2 by the group's other column tiles, one pipeline across them) for a
 // large product, at least 256 tiles per SM -- the trailing update while it is
-// the critical path.  Below that, one: the panel's own updates spread over
-// the SMs, and the trailing update's CTAs retire every tile, so the
-// high-priority panel kernels (the critical path once the trailing matrix is
-// small) wait less for SMs.  Measured at N = 16384 (getrf, NB = 512, B200):
-// 251 ms with four, 208 ms with one, identical bits.
+// the critical path -- and eight (two groups) from 1024 tiles per SM, where the
+// panel beside it has ample slack: fewer pipeline fills and CTA starts
+// (N = 131072 solve: DGEMM 31.89 -> 32.13 TFLOP/s, 48.02 -> 47.66 s).  Below
+// 256, one: the panel's own updates spread over the SMs, and the trailing
+// update's CTAs retire every tile, so the high-priority panel kernels (the
+// critical path once the trailing matrix is small) wait less for SMs.
+// Measured at N = 16384 (getrf, NB = 512, B200): 251 ms with four, 208 ms
+// with one, identical bits.
 int tiles_per_cta(long long ntiles) {
   static const int sms = [] {
     int dev = 0, n = 148;
@@ -334,7 +337,7 @@ int tiles_per_cta(long long ntiles) {
     }
     return n;
   }();
-  return ntiles >= 256LL * sms ? 4 : 1;
+  return ntiles >= 1024LL * sms ? 8 : (ntiles >= 256LL * sms ? 4 : 1);
 }
 
 cudaError_t launch_tpc(const CUtensorMap& mA, const CUtensorMap& mB, int m, int n, int k,
