@@ -151,6 +151,12 @@ class DistGroup:
     def all_reduce_sum(self, t):
         self.dist.all_reduce(t, group=self.group)
 
+    def all_gather(self, t):
+        """(size, *t.shape): every member's t, in rank order."""
+        out = [torch.empty_like(t) for _ in range(self.size)]
+        self.dist.all_gather(out, t, group=self.group)
+        return torch.stack(out)
+
 
 class LocalGroup:
     """Q ranks as threads of one process: rank r calls LocalGroup.member(r)
@@ -194,6 +200,15 @@ class _LocalMember:
         self.g.barrier.wait()
         t.copy_(acc)
         self._sync(t)
+
+    def all_gather(self, t):
+        self._sync(t)
+        self.g.slots[self.rank] = t.clone()
+        self.g.barrier.wait()
+        out = torch.stack([s.to(t.device) for s in self.g.slots])
+        self.g.barrier.wait()
+        self._sync(out)
+        return out
 
 
 def matgen_local(backend, grid: Grid1xQ, seed: int, A, ld: int):
