@@ -288,6 +288,39 @@ hplb_status hplb_panel_update(hplb_ctx* ctx, int n, int j, int jb, const double*
 hplb_status hplb_trsv_block(hplb_ctx* ctx, int n, int j, int jb, const double* dA, int64_t ld,
                             int lc, const double* dy, const double* ds, double* dx, double* dz);
 
+/* Building blocks of the solve on a P x Q process grid (rows block-cyclic as
+ * well; the driver is rochpl_b200/grid2d.py), where a panel column's rows are
+ * spread over the processes of a process column.
+ *
+ * hplb_col_argmax: the local part of one column's pivot search
+ * (HPL_pdmxswp, src/pfact/HPL_pdmxswp.cpp:19-126, combines these across the
+ * process column): the value of largest magnitude in rows [r0, r1) of column
+ * col of dA, and its row (the lowest among equal magnitudes), to host
+ * *v_out / *row_out; -1 for an empty range. */
+hplb_status hplb_col_argmax(hplb_ctx* ctx, const double* dA, int64_t ld, int r0, int r1, int col,
+                            double* v_out, int* row_out);
+
+/* The leaf's column step on local rows [r0, r1) (the scale and rank-1 update
+ * of src/pfact/HPL_pdpanrlT_device.cpp:225-240): l = A[r, c0+k] / piv into
+ * column c0 + k, then A[r, c0+c] -= l du[c] for k < c < kend (du: the pivot
+ * row's panel values, device). */
+hplb_status hplb_col_rank1(hplb_ctx* ctx, double* dA, int64_t ld, int r0, int r1, int c0, int k,
+                           int kend, double piv, const double* du);
+
+/* X <- L^-1 X for the unit-lower n x n L (leading dimension ldl) and X
+ * (n x nrhs, leading dimension ldx), device (the rocblas_dtrsm of
+ * src/pgesv/HPL_pdupdateTT.cpp:95-106 and of the recursive panel,
+ * src/pfact/HPL_pdrpanrlT.cpp:124-140). */
+hplb_status hplb_trsm_lower_unit(hplb_ctx* ctx, int n, int nrhs, const double* dL, int64_t ldl,
+                                 double* dX, int64_t ldx);
+
+/* X = U^-1 Y for the upper triangle of the n x n U (leading dimension ldu)
+ * and Y, X (n x nrhs), device; X may be Y.  The persistent multi-RHS
+ * back-solve of hplb_gesv (the diagonal-block solve of HPL_pdtrsv,
+ * src/pgesv/HPL_pdtrsv_device.cpp:170-307, for any number of columns). */
+hplb_status hplb_trsm_upper(hplb_ctx* ctx, int n, int nrhs, const double* dU, int64_t ldu,
+                            const double* dY, int64_t ldy, double* dX, int64_t ldx);
+
 /* The HPL residual check: dA must hold the regenerated [A|b] (hplb_matgen with
  * the seed of the solve), dX the solution.  Results go to *out (host). */
 hplb_status hplb_residual(hplb_ctx* ctx, int n, const double* dA, int64_t ld,

@@ -576,6 +576,70 @@ hplb_status hplb_trsv_block(hplb_ctx* ctx, int n, int j, int jb, const double* d
   return read_status(ctx, nullptr);
 }
 
+hplb_status hplb_col_argmax(hplb_ctx* ctx, const double* dA, int64_t ld, int r0, int r1, int col,
+                            double* v_out, int* row_out) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(!v_out || !row_out || r0 < 0 || r1 < r0 || col < 0 || (r1 > r0 && (!dA || ld < r1)))
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_col_argmax: bad argument");
+  *v_out   = 0.0;
+  *row_out = -1;
+  if(r1 == r0) return HPLB_OK;
+  ENTER(ctx);
+  CK(launch_col_argmax(dA, ld, r0, r1, col, ctx->d_out8, ctx->s_upd));
+  double o[2];
+  CK(cudaMemcpyAsync(o, ctx->d_out8, sizeof o, cudaMemcpyDeviceToHost, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  *v_out   = o[0];
+  *row_out = (int)o[1];
+  return HPLB_OK;
+}
+
+hplb_status hplb_col_rank1(hplb_ctx* ctx, double* dA, int64_t ld, int r0, int r1, int c0, int k,
+                           int kend, double piv, const double* du) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(r0 < 0 || r1 < r0 || c0 < 0 || k < 0 || kend <= k ||
+     (r1 > r0 && (!dA || !du || ld < r1)))
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_col_rank1: bad argument");
+  if(r1 == r0) return HPLB_OK;
+  ENTER(ctx);
+  CK(launch_col_rank1(dA, ld, r0, r1, c0, k, kend, piv, du, ctx->num_sms, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return HPLB_OK;
+}
+
+hplb_status hplb_trsm_lower_unit(hplb_ctx* ctx, int n, int nrhs, const double* dL, int64_t ldl,
+                                 double* dX, int64_t ldx) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(n < 0 || nrhs < 0 || (n > 0 && nrhs > 0 && (!dL || !dX || ldl < n || ldx < n)))
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_trsm_lower_unit: bad argument");
+  if(n == 0 || nrhs == 0) return HPLB_OK;
+  ENTER(ctx);
+  hplb_status s = ensure_solve_ws(ctx, 1, n, 1);
+  if(s != HPLB_OK) return s;
+  CK(launch_diag_inv<double>(dL, ldl, 0, 0, n, ctx->d_dinv_piece, ctx->s_upd));
+  CK(launch_trsm_unit_lower(dX, ldx, n, dL, ldl, ctx->d_dinv_piece, nrhs, ctx->s_upd));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return HPLB_OK;
+}
+
+hplb_status hplb_trsm_upper(hplb_ctx* ctx, int n, int nrhs, const double* dU, int64_t ldu,
+                            const double* dY, int64_t ldy, double* dX, int64_t ldx) {
+  if(!ctx) return HPLB_ERR_ARG;
+  if(n < 0 || nrhs < 0 ||
+     (n > 0 && nrhs > 0 && (!dU || !dY || !dX || ldu < n || ldy < n || ldx < n)))
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_trsm_upper: bad argument");
+  if(n == 0 || nrhs == 0) return HPLB_OK;
+  ENTER(ctx);
+  hplb_status s = grow(ctx, &ctx->d_trsv, &ctx->trsv_cap, trsv_flag_ints(n));
+  if(s != HPLB_OK) return s;
+  CK(cudaMemsetAsync(ctx->d_status, 0, ST_COUNT * sizeof(int), ctx->s_upd));
+  int launches = 0;
+  CK(launch_trsm_upper(dU, ldu, n, nrhs, dY, ldy, dX, ldx, ctx->d_trsv, ctx->d_status,
+                       ctx->s_upd, &launches));
+  CK(cudaStreamSynchronize(ctx->s_upd));
+  return read_status(ctx, nullptr);
+}
+
 hplb_status hplb_last_timing(const hplb_ctx* ctx, hplb_timing* out) {
   if(!ctx || !out) return HPLB_ERR_ARG;
   *out = ctx->timing;

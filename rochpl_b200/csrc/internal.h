@@ -95,6 +95,13 @@ cudaError_t launch_trsv(const double* A, int64_t ld, int n, double* X, int* flag
 cudaError_t launch_trsv_y(const double* A, int64_t ld, int n, const double* Y, double* X,
                           int* flags, int* status, cudaStream_t stream, int* launches);
 // z[0:m] += U[0:m, 0:k] x (U column-major, leading dimension ld); r = y - s.
+// The P x Q grid's local column steps (grid2d.cu): the arg-max of |A[r, c]|
+// over rows [r0, r1) into out[0] (value) and out[1] (row, -1 if none), and the
+// leaf step on rows [r0, r1) of columns c0 + k .. c0 + kend - 1.
+cudaError_t launch_col_argmax(const double* A, int64_t ld, int r0, int r1, int c, double* out,
+                              cudaStream_t stream);
+cudaError_t launch_col_rank1(double* A, int64_t ld, int r0, int r1, int c0, int k, int kend,
+                             double piv, const double* u, int num_sms, cudaStream_t stream);
 // X (n x nrhs, leading dimension ldx) = U^-1 Y for the upper triangle of A
 // (n x n, leading dimension ld); Y (leading dimension ldy) may be X itself.
 // Persistent, one launch per 32 right-hand sides; flags: trsv_flag_ints(n).

@@ -31,6 +31,7 @@ EXPORTS = [
     "hplb_batch_matgen", "hplb_batch_gesv", "hplb_batch_getrs", "hplb_batch_rank_k",
     "hplb_batch_residual", "hplb_batch_last_ms", "hplb_batch_tune",
     "hplb_panel_factor", "hplb_panel_update", "hplb_trsv_block", "hplb_gesv",
+    "hplb_col_argmax", "hplb_col_rank1", "hplb_trsm_lower_unit", "hplb_trsm_upper",
 ]
 
 HPLB_BATCH_CLASSES = 6
@@ -153,6 +154,13 @@ def load() -> C.CDLL:
     L.hplb_gesv.argtypes = [vp, C.POINTER(hplb_algo), i32, i32, vp, i64, vp, i64, vp,
                             C.POINTER(C.c_int)]
     L.hplb_gesv.restype = i32
+    L.hplb_col_argmax.argtypes = [vp, vp, i64, i32, i32, i32, C.POINTER(C.c_double),
+                                  C.POINTER(C.c_int)]
+    L.hplb_col_rank1.argtypes = [vp, vp, i64, i32, i32, i32, i32, i32, C.c_double, vp]
+    L.hplb_trsm_lower_unit.argtypes = [vp, i32, i32, vp, i64, vp, i64]
+    L.hplb_trsm_upper.argtypes = [vp, i32, i32, vp, i64, vp, i64, vp, i64]
+    for name in ("hplb_col_argmax", "hplb_col_rank1", "hplb_trsm_lower_unit", "hplb_trsm_upper"):
+        getattr(L, name).restype = i32
     L.hplb_panel_factor.argtypes = [vp, C.POINTER(hplb_algo), i32, i32, i32, vp, i64, i32, vp,
                                     C.POINTER(C.c_int)]
     L.hplb_panel_factor.restype = i32
@@ -221,6 +229,23 @@ class Library:
                               C.byref(info))
         self._check(st, allow=(HPLB_OK, HPLB_ERR_SINGULAR))
         return info.value
+
+    def col_argmax(self, A: int, ld: int, r0: int, r1: int, col: int) -> tuple[float, int]:
+        """hplb_col_argmax: (value, row) of the largest |A[r, col]|, r in [r0, r1)."""
+        v, r = C.c_double(0.0), C.c_int(-1)
+        self._check(self.L.hplb_col_argmax(self.ctx, A, ld, r0, r1, col, C.byref(v), C.byref(r)))
+        return v.value, r.value
+
+    def col_rank1(self, A: int, ld: int, r0: int, r1: int, c0: int, k: int, kend: int,
+                  piv: float, u: int):
+        self._check(self.L.hplb_col_rank1(self.ctx, A, ld, r0, r1, c0, k, kend, piv, u))
+
+    def trsm_lower_unit(self, n: int, nrhs: int, L: int, ldl: int, X: int, ldx: int):
+        self._check(self.L.hplb_trsm_lower_unit(self.ctx, n, nrhs, L, ldl, X, ldx))
+
+    def trsm_upper(self, n: int, nrhs: int, U: int, ldu: int, Y: int, ldy: int, X: int,
+                   ldx: int):
+        self._check(self.L.hplb_trsm_upper(self.ctx, n, nrhs, U, ldu, Y, ldy, X, ldx))
 
     def pdgesv_mixed(self, algo: hplb_algo, n: int, X: int, seed: int = 100, A: int | None = None,
                      ld: int = 0, precision: int = PREC_BF16X3, restart: int = 20,

@@ -116,6 +116,47 @@ def test_grid2d_solve_threads_match_the_oracle(oracle, n, nb, P, Q, nbmin, ndiv)
     _check(oracle, n, nb, 100, algo, out)
 
 
+@pytest.mark.parametrize("n,nb,P,Q", [(100, 16, 2, 2), (97, 8, 3, 2)])
+def test_grid2d_device_backend_mapping_on_host_memory(oracle, n, nb, P, Q):
+    """DeviceBackend2D's calls (element offsets, leading dimensions, sizes)
+    through a stand-in for the library that does each C ABI call's work on
+    host memory: the same solve as with the host backend."""
+    import threading
+
+    import torch
+
+    from grid2d_host import FakeDeviceLib, local_to_global_2d
+    from rochpl_b200.grid2d import (DeviceBackend2D, LocalGrid2D, matgen_local_2d,
+                                    pdgesv_2d)
+    from rochpl_b200.hpl import Algo
+
+    algo = Algo(nb, 4, 2, 2, 2, 1, 0)
+    grp = LocalGrid2D(P, Q)
+    out, errs = [None] * (P * Q), []
+
+    def work(p, q):
+        try:
+            be = DeviceBackend2D(FakeDeviceLib(oracle))
+            g = Grid2D(n, nb, p, q, P, Q)
+            ld = max(g.mp, 1) + 1
+            A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64)
+            matgen_local_2d(be, g, 100, A, ld)
+            x, ipiv, info = pdgesv_2d(be, grp.comms(p, q), g, algo, A, ld)
+            out[p * Q + q] = (x.numpy().copy(), ipiv.numpy().copy(), info,
+                              local_to_global_2d(g, A, ld))
+        except BaseException as e:  # surfaced below
+            errs.append(e)
+            grp.abort()
+
+    ts = [threading.Thread(target=work, args=(p, q)) for p in range(P) for q in range(Q)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=180)
+    assert not errs, errs
+    _check(oracle, n, nb, 100, algo, out)
+
+
 def test_grid2d_rejects_left_and_crout_factorisations():
     import torch
 
