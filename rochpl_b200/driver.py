@@ -136,11 +136,16 @@ def sweep(cfg: HplConfig):
                                                                 cfg.l1notran)
 
 
-def skipped(p: int, q: int, algo: Algo, world: int = 1) -> bool:
-    """Tests this driver counts as skipped: grids other than 1 x (the number
-    of processes), and values the library does not take (NBMIN > 128,
-    NB > 2048, DEPTH != 1)."""
-    return p != 1 or q != world or algo.nbmin > 128 or algo.nb > 2048 or algo.depth != 1
+def skipped(p: int, q: int, algo: Algo, world: int = 1, two_d: bool = False) -> bool:
+    """Tests this driver counts as skipped: values the library does not take
+    (NBMIN > 128, NB > 2048, DEPTH != 1), and grids it cannot run: P x Q must
+    use all the processes, and P must be 1 unless the solver runs 2-D grids
+    (`two_d`), which factor with PFACT = RFACT = right only."""
+    if algo.nbmin > 128 or algo.nb > 2048 or algo.depth != 1 or p * q != world:
+        return True
+    if p == 1:
+        return False
+    return not two_d or algo.pfact != 2 or algo.rfact != 2
 
 
 class GpuSolver:
@@ -202,51 +207,71 @@ class GpuSolver:
 
 
 class GridSolver:
-    """This process's part of one system on the 1 x W grid of all processes
-    (torch.distributed already initialised, one GPU each).  The solve is timed
-    by the wall clock between two barriers, the slowest process's time (as
-    HPL_ptimer_combine takes the maximum); the residual is computed on rank 0
-    against the regenerated matrix."""
+    """This process's part of one system on a P x Q grid of all processes
+    (torch.distributed already initialised, one GPU each): the 1 x Q solve of
+    rochpl_b200.grid, or the 2-D one of rochpl_b200.grid2d when P > 1.  The
+    solve is timed by the wall clock between two barriers, the slowest
+    process's time (as HPL_ptimer_combine takes the maximum); the residual is
+    computed on rank 0 against the regenerated matrix."""
+
+    takes_grid = True  # run() passes each test's (P, Q)
 
     def __init__(self, device: int = 0):
         import torch
         import torch.distributed as dist
 
         from .grid import DeviceBackend, DistGroup
+        from .grid2d import DeviceBackend2D
         from .lib import library
 
         self.torch, self.dist = torch, dist
         self.device = device
         self.lib = library(device)
         self.backend = DeviceBackend(self.lib)
+        self.backend2d = DeviceBackend2D(self.lib)
         self.comm = DistGroup()
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        self._comms2d = {}  # (P, Q) -> (row, col, world); every rank builds the same groups
 
-    def _solve(self, algo: Algo, n: int, seed: int):
+    def _run(self, algo: Algo, n: int, seed: int, grid):
         from .grid import Grid1xQ, matgen_local, pdgesv_grid
+        from .grid2d import Grid2D, dist_comms, matgen_local_2d, pdgesv_2d
 
         torch = self.torch
-        g = Grid1xQ(n, algo.nb, self.rank, self.world)
-        ld = default_ld(n)
-        A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64,
-                        device=torch.device("cuda", self.device))
-        matgen_local(self.backend, g, seed, A, ld)
+        P, Q = grid if grid is not None else (1, self.world)
+        dev = torch.device("cuda", self.device)
+        if P == 1:
+            g = Grid1xQ(n, algo.nb, self.rank, self.world)
+            ld = default_ld(n)
+            A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64, device=dev)
+            matgen_local(self.backend, g, seed, A, ld)
+            solve = lambda: pdgesv_grid(self.backend, self.comm, g, algo, A, ld)  # noqa: E731
+        else:
+            if (P, Q) not in self._comms2d:
+                self._comms2d[(P, Q)] = dist_comms(P, Q)
+            p, q = divmod(self.rank, Q)
+            g = Grid2D(n, algo.nb, p, q, P, Q)
+            ld = (max(g.mp, 1) + 1) // 2 * 2  # even: the DGEMM's TMA path
+            A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64, device=dev)
+            matgen_local_2d(self.backend2d, g, seed, A, ld)
+            comms = self._comms2d[(P, Q)]
+            solve = lambda: pdgesv_2d(self.backend2d, comms, g, algo, A, ld)  # noqa: E731
         torch.cuda.synchronize(self.device)
         self.dist.barrier()
         t_start = time.time()
         t0 = time.perf_counter()
-        x, ipiv, info = pdgesv_grid(self.backend, self.comm, g, algo, A, ld)
+        x, ipiv, info = solve()
         torch.cuda.synchronize(self.device)
-        w = torch.tensor([time.perf_counter() - t0], dtype=torch.float64,
-                         device=torch.device("cuda", self.device))
+        w = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
         self.dist.all_reduce(w, op=self.dist.ReduceOp.MAX)
         return x, info, float(w.item()), t_start, time.time()
 
-    def warmup(self, algo: Algo, n: int) -> None:
-        self._solve(algo, min(n, 2 * algo.nb * self.world + 1), HPL_ISEED)
+    def warmup(self, algo: Algo, n: int, grid=None) -> None:
+        self._run(algo, min(n, 2 * algo.nb * self.world + 1), HPL_ISEED, grid)
 
-    def __call__(self, algo: Algo, n: int, seed: int = HPL_ISEED, progress: bool = False) -> dict:
-        x, info, wtime, t_start, t_end = self._solve(algo, n, seed)
+    def __call__(self, algo: Algo, n: int, seed: int = HPL_ISEED, progress: bool = False,
+                 grid=None) -> dict:
+        x, info, wtime, t_start, t_end = self._run(algo, n, seed, grid)
         res = (self.lib.residual_lcg(n, seed, x.data_ptr()) if self.rank == 0 else
                {"resid": 0.0})
         return {"wtime": wtime, "t_start": t_start, "t_end": t_end, "info": info, **res}
@@ -269,15 +294,17 @@ def run(cfg: HplConfig, out=None, solver=None, progress: bool = False, world: in
     solver = solver if solver is not None else GpuSolver()
     kpass = kfail = kskip = 0
     first = True
+    two_d = getattr(solver, "takes_grid", False)
     for n, p, q, bc, algo in sweep(cfg):
-        if skipped(p, q, algo, world):
+        if skipped(p, q, algo, world, two_d):
             kskip += 1
             continue
+        kw = {"grid": (p, q)} if two_d else {}
         warm = getattr(solver, "warmup", None)
         if warm is not None:
-            warm(algo, n)
+            warm(algo, n, **kw)
         for _ in range(max(cfg.iters, 1)):
-            r = solver(algo, n, progress=progress)
+            r = solver(algo, n, progress=progress, **kw)
             # The table header precedes every result while residuals are
             # checked, only the first without checking (src/HPL_pdtest.cpp:144-158).
             if first:
@@ -328,7 +355,7 @@ def main(argv=None) -> int:
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     solver, rank = None, 0
-    if world > 1:  # one process per GPU under torchrun: the 1 x world grids
+    if world > 1:  # one process per GPU under torchrun: the P x Q = world grids
         import torch
         import torch.distributed as dist
 

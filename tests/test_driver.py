@@ -159,3 +159,27 @@ def test_grids_run_when_they_match_the_process_count():
         tally = run(cfg, io.StringIO(), solver=s, world=world)
         assert tally == {"passed": runs, "failed": 0, "skipped": 4 - runs}, world
         assert len(s.calls) == runs
+
+
+def test_two_d_grids_run_with_a_grid_solver():
+    """A solver that takes the grid shape (GridSolver) gets P x Q grids with
+    P > 1 when P Q is the process count and the panel is factored right-looking;
+    left / Crout panels on such grids are skipped."""
+    class GridFake(FakeSolver):
+        takes_grid = True
+
+        def warmup(self, algo, n, grid=None):
+            self.warmups.append((algo.nb, n, grid))
+
+        def __call__(self, algo, n, progress=False, grid=None):
+            self.calls.append((n, grid, algo.pfact, algo.rfact))
+            return super().__call__(algo, n, progress)
+
+    cfg = HplConfig(ns=[100], nbs=[32], ps=[1, 2, 2], qs=[2, 1, 2], pfacts=[2, 0], rfacts=[2])
+    s = GridFake()
+    tally = run(cfg, io.StringIO(), solver=s, world=2)
+    grids = [c[1] for c in s.calls if c[0] == 100 and len(c) == 4]
+    assert (1, 2) in grids and (2, 1) in grids and (2, 2) not in grids
+    assert all(not (g == (2, 1) and pf == 0) for _, g, pf, _ in
+               [c for c in s.calls if len(c) == 4])
+    assert tally["passed"] == 3 and tally["skipped"] == 3
