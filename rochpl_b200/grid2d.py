@@ -312,10 +312,7 @@ def _update(be, col, grid, j, jb, pj, T, Lb, lr2, m2, ipiv, A, ld):
     """Row interchanges, U = L1^-1 (new top rows) and A22 -= L2 U on this
     process's trailing columns (global columns >= j + jb, b included)."""
     c0 = grid.lcol_from(j + jb)
-    ncols = grid.nq - c0
-    if ncols <= 0:
-        # Still take part in the column's gather, which every member joins.
-        ncols = 0
+    ncols = max(grid.nq - c0, 0)  # the same on every process of this column
     # The panel's interchanges as a map: perm[r] = the original row now at r.
     perm = {}
     for x in range(jb):
@@ -332,8 +329,8 @@ def _update(be, col, grid, j, jb, pj, T, Lb, lr2, m2, ipiv, A, ld):
         for i, r in enumerate(rows):
             if grid.row_owner(r) == grid.p:
                 Bv[i].copy_(_block(A, ld, grid.lrow(r), c0, 1, ncols)[:, 0])
-    allb = col.all_gather(buf)  # (P, len(rows) * ncols): each row from its owner
-    if ncols <= 0:
+    allb = col.all_gather(buf)  # every member joins, with or without trailing columns
+    if ncols == 0:
         return
     old = torch.stack([allb[grid.row_owner(r)].view(len(rows), ncols)[i]
                        for i, r in enumerate(rows)])
