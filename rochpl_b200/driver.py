@@ -140,12 +140,10 @@ def skipped(p: int, q: int, algo: Algo, world: int = 1, two_d: bool = False) -> 
     """Tests this driver counts as skipped: values the library does not take
     (NBMIN > 128, NB > 2048, DEPTH != 1), and grids it cannot run: P x Q must
     use all the processes, and P must be 1 unless the solver runs 2-D grids
-    (`two_d`), which factor with PFACT = RFACT = right only."""
+    (`two_d`)."""
     if algo.nbmin > 128 or algo.nb > 2048 or algo.depth != 1 or p * q != world:
         return True
-    if p == 1:
-        return False
-    return not two_d or algo.pfact != 2 or algo.rfact != 2
+    return p != 1 and not two_d
 
 
 class GpuSolver:

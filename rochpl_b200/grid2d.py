@@ -28,9 +28,10 @@ local work (DeviceBackend2D runs it through the C ABI on each process's GPU;
 the tests supply a host one) and three communicators -- the process row, the
 process column and the whole grid -- with broadcast / all_gather /
 all_reduce on tensors (torch.distributed groups, or LocalGroup threads).  The
-panel is factored with HPL's right-looking recursion and leaves (PFACT = RFACT
-= right); look-ahead is not used (the order of the work changes, its results do
-not).  Every process returns x, the global pivot vector and info, replicated.
+panel recursion takes RFACT's right-looking or left-looking / Crout order (the
+orderings of hplb_pdgesv's panel); its leaves are right-looking for every
+PFACT, as hplb_pdgesv's are.  Look-ahead is not used (the order of the work
+changes, its results do not).  Every process returns x, the global pivot vector and info, replicated.
 """
 from __future__ import annotations
 
@@ -194,8 +195,6 @@ def pdgesv_2d(backend, comms, grid: Grid2D, algo, A, ld: int):
     (ipiv[j] = row swapped into row j) and the first zero-pivot column
     (1-based, 0 if none).  On exit A holds this process's blocks of the
     factors (U; the multipliers unpivoted across panels, as in rocHPL)."""
-    if algo.pfact != 2 or algo.rfact != 2:
-        raise NotImplementedError("the P x Q grid factors with PFACT = RFACT = right only")
     row, col, world = comms
     n, nb, p, q = grid.n, grid.nb, grid.p, grid.q
     dev, f64 = A.device, torch.float64
@@ -216,7 +215,8 @@ def pdgesv_2d(backend, comms, grid: Grid2D, algo, A, ld: int):
             if p == pj:
                 _block(T, jb, 0, 0, jb, jb).copy_(_block(A, ld, grid.lrow(j), lc, jb, jb))
             col.broadcast(T, pj)
-            pinfo = _factor_panel(backend, col, grid, j, jb, lc, lr2, T, A, ld, nbmin, ndiv, piv)
+            pinfo = _factor_panel(backend, col, grid, j, jb, lc, lr2, T, A, ld, nbmin, ndiv,
+                                  algo.rfact, piv)
             piv[jb] = float(pinfo)
             if p == pj:
                 _block(A, ld, grid.lrow(j), lc, jb, jb).copy_(_block(T, jb, 0, 0, jb, jb))
@@ -235,7 +235,7 @@ def pdgesv_2d(backend, comms, grid: Grid2D, algo, A, ld: int):
     return x, ipiv[:n].to(torch.int32), info
 
 
-def _factor_panel(be, col, grid, j, jb, lc, lr2, T, A, ld, nbmin, ndiv, piv) -> int:
+def _factor_panel(be, col, grid, j, jb, lc, lr2, T, A, ld, nbmin, ndiv, rfact, piv) -> int:
     """The panel's recursion and leaves on one process column; T (jb x jb,
     leading dimension jb) is the replicated top block, the local rows
     [lr2, mp) of columns [lc, lc + jb) the rest.  Fills piv[:jb] with the
@@ -282,6 +282,18 @@ def _factor_panel(be, col, grid, j, jb, lc, lr2, T, A, ld, nbmin, ndiv, piv) -> 
             be.col_rank1(T, jb, k + 1, jb, 0, k, jj + w, bv, u)
             be.col_rank1(A, ld, lr2, mp, lc, k, jj + w, bv, u)
 
+    def node_update(a, k, b, w):
+        """Columns [b, b + w) of the rows at and below panel row a: the top
+        rows a .. a+k get U = L11^-1 (L11 the unit-lower k x k block at
+        (a, a) of the replicated top block), every row below them
+        -= (its columns [a, a + k)) U -- the rest of the top block and the
+        local rows."""
+        be.trsm_lower_unit(k, w, T, jb, a + a * jb, T, jb, a + b * jb)
+        be.gemm_sub(jb - (a + k), w, k, T, jb, (a + k) + a * jb, T, jb, a + b * jb, T, jb,
+                    (a + k) + b * jb)
+        be.gemm_sub(mp - lr2, w, k, A, ld, lr2 + (lc + a) * ld, T, jb, a + b * jb, A, ld,
+                    lr2 + (lc + b) * ld)
+
     def rpanel(jj, w):
         if w <= nbmin:
             leaf(jj, w)
@@ -291,16 +303,14 @@ def _factor_panel(be, col, grid, j, jb, lc, lr2, T, A, ld, nbmin, ndiv, piv) -> 
         while rem > 0:
             rem -= jbs
             a = jj + off
-            rpanel(a, jbs)
-            if rem > 0:
-                b = a + jbs
-                # U12 = L11^-1 A12 on the replicated top block, then the rows
-                # below: the rest of the top block and the local rows.
-                be.trsm_lower_unit(jbs, rem, T, jb, a + a * jb, T, jb, a + b * jb)
-                be.gemm_sub(jb - b, rem, jbs, T, jb, b + a * jb, T, jb, a + b * jb, T, jb,
-                            b + b * jb)
-                be.gemm_sub(mp - lr2, rem, jbs, A, ld, lr2 + (lc + a) * ld, T, jb, a + b * jb,
-                            A, ld, lr2 + (lc + b) * ld)
+            if rfact == 2:  # right-looking: factor the piece, then update everything to its right
+                rpanel(a, jbs)
+                if rem > 0:
+                    node_update(a, jbs, a + jbs, rem)
+            else:  # left-looking / Crout: bring the piece up to date, then factor it
+                if off > 0:
+                    node_update(jj, off, a, jbs)
+                rpanel(a, jbs)
             off += jbs
             jbs = min(rem, nbs)
 

@@ -157,18 +157,34 @@ def test_grid2d_device_backend_mapping_on_host_memory(oracle, n, nb, P, Q):
     _check(oracle, n, nb, 100, algo, out)
 
 
-def test_grid2d_rejects_left_and_crout_factorisations():
-    import torch
+@pytest.mark.parametrize("n,nb,P,Q", [(100, 16, 2, 2), (150, 32, 3, 2)])
+@pytest.mark.parametrize("pfact,rfact", [(0, 1), (1, 0), (2, 1)])
+def test_grid2d_left_and_crout_orderings_match_the_oracle(oracle, n, nb, P, Q, pfact, rfact):
+    """RFACT's left-looking and Crout recursion orderings on the 2-D grid
+    (the leaves right-looking for every PFACT, as hplb_pdgesv's)."""
+    import threading
 
-    from grid2d_host import HostBackend2D
-    from oracle import oracle as O
-    from rochpl_b200.grid2d import LocalGrid2D, pdgesv_2d
+    from rochpl_b200.grid2d import LocalGrid2D
     from rochpl_b200.hpl import Algo
 
-    g = Grid2D(8, 4, 0, 0, 1, 1)
-    with pytest.raises(NotImplementedError):
-        pdgesv_2d(HostBackend2D(O), LocalGrid2D(1, 1).comms(0, 0), g, Algo(4, 4, 2, 0, 2, 1, 0),
-                  torch.zeros(64, dtype=torch.float64), 8)
+    algo = Algo(nb, 4, 2, pfact, rfact, 1, 0)
+    grp = LocalGrid2D(P, Q)
+    out, errs = [None] * (P * Q), []
+
+    def work(p, q):
+        try:
+            out[p * Q + q] = _run_rank(oracle, grp.comms(p, q), n, nb, P, Q, p, q, 100, algo)
+        except BaseException as e:  # surfaced below
+            errs.append(e)
+            grp.abort()
+
+    ts = [threading.Thread(target=work, args=(p, q)) for p in range(P) for q in range(Q)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=180)
+    assert not errs, errs
+    _check(oracle, n, nb, 100, algo, out)
 
 
 _CHILD = r"""
