@@ -76,9 +76,10 @@ def _single(hlib, n, nb, algo):
     return dX.cpu().numpy(), dP.cpu().numpy(), from_dev(dA, ld, n + 1)[:n]
 
 
-@pytest.mark.parametrize("n,nb,P,Q", [(1000, 128, 2, 1), (1000, 128, 2, 2), (1531, 96, 3, 2),
-                                      (800, 256, 1, 2)])
-def test_grid2d_on_virtual_ranks_matches_single_gpu(hlib, oracle, n, nb, P, Q):
+@pytest.mark.parametrize("n,nb,P,Q,rfact", [(1000, 128, 2, 1, 2), (1000, 128, 2, 2, 2),
+                                            (1531, 96, 3, 2, 2), (800, 256, 1, 2, 2),
+                                            (1000, 128, 2, 2, 0), (700, 64, 2, 1, 1)])
+def test_grid2d_on_virtual_ranks_matches_single_gpu(hlib, oracle, n, nb, P, Q, rfact):
     import torch
 
     from rochpl_b200.grid2d import (DeviceBackend2D, Grid2D, LocalGrid2D, matgen_local_2d,
@@ -86,7 +87,7 @@ def test_grid2d_on_virtual_ranks_matches_single_gpu(hlib, oracle, n, nb, P, Q):
     from rochpl_b200.hpl import Algo
     from rochpl_b200.lib import Library
 
-    algo = Algo(nb, 32, 2, 2, 2, 1, 0)
+    algo = Algo(nb, 32, 2, 2, rfact, 1, 0)
     x1, p1, F1 = _single(hlib, n, nb, algo)
     grp = LocalGrid2D(P, Q)
     out, errs = [None] * (P * Q), []

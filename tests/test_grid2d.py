@@ -116,8 +116,9 @@ def test_grid2d_solve_threads_match_the_oracle(oracle, n, nb, P, Q, nbmin, ndiv)
     _check(oracle, n, nb, 100, algo, out)
 
 
-@pytest.mark.parametrize("n,nb,P,Q", [(100, 16, 2, 2), (97, 8, 3, 2)])
-def test_grid2d_device_backend_mapping_on_host_memory(oracle, n, nb, P, Q):
+@pytest.mark.parametrize("n,nb,P,Q,rfact", [(100, 16, 2, 2, 2), (97, 8, 3, 2, 2),
+                                            (100, 16, 2, 2, 0), (97, 8, 3, 2, 1)])
+def test_grid2d_device_backend_mapping_on_host_memory(oracle, n, nb, P, Q, rfact):
     """DeviceBackend2D's calls (element offsets, leading dimensions, sizes)
     through a stand-in for the library that does each C ABI call's work on
     host memory: the same solve as with the host backend."""
@@ -130,7 +131,7 @@ def test_grid2d_device_backend_mapping_on_host_memory(oracle, n, nb, P, Q):
                                     pdgesv_2d)
     from rochpl_b200.hpl import Algo
 
-    algo = Algo(nb, 4, 2, 2, 2, 1, 0)
+    algo = Algo(nb, 4, 2, 2, rfact, 1, 0)
     grp = LocalGrid2D(P, Q)
     out, errs = [None] * (P * Q), []
 
