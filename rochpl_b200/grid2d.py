@@ -199,6 +199,11 @@ def pdgesv_2d(backend, comms, grid: Grid2D, algo, A, ld: int):
     n, nb, p, q = grid.n, grid.nb, grid.p, grid.q
     dev, f64 = A.device, torch.float64
     mp, nq = grid.mp, grid.nq
+    if A.dtype != f64 or A.dim() != 1:
+        raise ValueError("A must be a flat float64 tensor")
+    if ld < max(mp, 1) or A.numel() < ld * max(nq, 1):
+        raise ValueError(f"process ({p}, {q}) holds {mp} x {nq}: needs ld >= {max(mp, 1)} and "
+                         f"ld * {max(nq, 1)} entries (ld {ld}, {A.numel()} entries)")
     nbmin = max(1, min(algo.nbmin, nb))
     ndiv = max(2, algo.ndiv)
     ipiv = torch.zeros(max(n, 1), dtype=torch.int64)

@@ -239,3 +239,22 @@ def test_grid2d_solve_four_gloo_processes(oracle, tmp_path):
     results = [(np.array(r["x"]), np.array(r["ipiv"], dtype=np.int32), r["info"],
                 np.load(tmp_path / f"rank{r['rank']}.npy")) for r in res]
     _check(oracle, n, nb, 100, Algo(nb, 8, 2, 2, 2, 1, 0), results)
+
+
+def test_grid2d_rejects_a_local_array_that_is_too_small(oracle):
+    import torch
+
+    from grid2d_host import HostBackend2D
+    from rochpl_b200.grid2d import LocalGrid2D, pdgesv_2d
+    from rochpl_b200.hpl import Algo
+
+    g = Grid2D(64, 16, 0, 0, 1, 1)
+    comms = LocalGrid2D(1, 1).comms(0, 0)
+    algo = Algo(16, 4, 2, 2, 2, 1, 0)
+    be = HostBackend2D(oracle)
+    with pytest.raises(ValueError, match="ld >= 64"):
+        pdgesv_2d(be, comms, g, algo, torch.zeros(63 * 65, dtype=torch.float64), 63)
+    with pytest.raises(ValueError, match="entries"):
+        pdgesv_2d(be, comms, g, algo, torch.zeros(64 * 65 - 1, dtype=torch.float64), 64)
+    with pytest.raises(ValueError, match="float64"):
+        pdgesv_2d(be, comms, g, algo, torch.zeros(64 * 65, dtype=torch.float32), 64)
