@@ -307,10 +307,14 @@ hplb_status hplb_col_argmax(hplb_ctx* ctx, const double* dA, int64_t ld, int r0,
 hplb_status hplb_col_rank1(hplb_ctx* ctx, double* dA, int64_t ld, int r0, int r1, int c0, int k,
                            int kend, double piv, const double* du);
 
+/* Largest n hplb_trsm_lower_unit accepts: a panel's width (NB) at most; each
+ * CTA keeps a slice of X's columns, n rows deep, in shared memory. */
+#define HPLB_TRSM_LOWER_MAX_N 2048
+
 /* X <- L^-1 X for the unit-lower n x n L (leading dimension ldl) and X
  * (n x nrhs, leading dimension ldx), device (the rocblas_dtrsm of
  * src/pgesv/HPL_pdupdateTT.cpp:95-106 and of the recursive panel,
- * src/pfact/HPL_pdrpanrlT.cpp:124-140). */
+ * src/pfact/HPL_pdrpanrlT.cpp:124-140); n <= HPLB_TRSM_LOWER_MAX_N. */
 hplb_status hplb_trsm_lower_unit(hplb_ctx* ctx, int n, int nrhs, const double* dL, int64_t ldl,
                                  double* dX, int64_t ldx);
 

@@ -612,6 +612,8 @@ hplb_status hplb_trsm_lower_unit(hplb_ctx* ctx, int n, int nrhs, const double* d
   if(!ctx) return HPLB_ERR_ARG;
   if(n < 0 || nrhs < 0 || (n > 0 && nrhs > 0 && (!dL || !dX || ldl < n || ldx < n)))
     return set_err(ctx, HPLB_ERR_ARG, "hplb_trsm_lower_unit: bad argument");
+  if(n > HPLB_TRSM_LOWER_MAX_N)
+    return set_err(ctx, HPLB_ERR_ARG, "hplb_trsm_lower_unit: n above HPLB_TRSM_LOWER_MAX_N");
   if(n == 0 || nrhs == 0) return HPLB_OK;
   ENTER(ctx);
   hplb_status s = ensure_solve_ws(ctx, 1, n, 1);
