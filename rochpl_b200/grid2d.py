@@ -128,6 +128,8 @@ class DeviceBackend2D:
     Local arrays are flat float64 CUDA tensors, column-major, addressed by
     element offsets."""
 
+    max_nb = 2048  # HPLB_TRSM_LOWER_MAX_N: the panel's triangular solve
+
     def __init__(self, lib):
         self.lib = lib
 
@@ -201,6 +203,9 @@ def pdgesv_2d(backend, comms, grid: Grid2D, algo, A, ld: int):
     mp, nq = grid.mp, grid.nq
     if A.dtype != f64 or A.dim() != 1:
         raise ValueError("A must be a flat float64 tensor")
+    max_nb = getattr(backend, "max_nb", None)
+    if max_nb is not None and nb > max_nb:  # every process fails here, before any exchange
+        raise ValueError(f"NB {nb} above this backend's limit {max_nb}")
     if ld < max(mp, 1) or A.numel() < ld * max(nq, 1):
         raise ValueError(f"process ({p}, {q}) holds {mp} x {nq}: needs ld >= {max(mp, 1)} and "
                          f"ld * {max(nq, 1)} entries (ld {ld}, {A.numel()} entries)")
