@@ -79,7 +79,10 @@ typedef struct hplb_timing {
 } hplb_timing;
 
 /* Create a context on CUDA device `device`.  Returns NULL on failure, with the
- * reason in *status when status is not NULL. */
+ * reason in *status when status is not NULL.  A process may hold several
+ * contexts (one per host thread, say), all on one device: some kernels' shared
+ * memory limits are raised once per process, so drive each GPU from its own
+ * process, as rocHPL's one MPI rank per GPU does. */
 hplb_ctx* hplb_create(int device, hplb_status* status);
 void      hplb_destroy(hplb_ctx* ctx);
 
