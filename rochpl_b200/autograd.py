@@ -7,7 +7,7 @@ then back-solves with U for the columns of X.  The factors and pivots are
 saved for the backward pass, which never refactors:
 
     Bbar = A^-T Xbar      hplb_getrs(trans = 1) on the stored LU and pivots
-    Abar = -Bbar X^T      hplb_rank_k, one fused rank-nrhs kernel
+    Abar = -Bbar X^T      hplb_rank_k, one fused kernel per 64 right-hand sides
 
 HplSolveBatch / hpl_solve_batch do the same for a whole batch of systems of
 uneven size (hplb_batch_gesv forward; hplb_batch_getrs with trans = 1 and
@@ -39,9 +39,24 @@ def _colmajor(M: torch.Tensor, ld: int | None = None) -> torch.Tensor:
     return out
 
 
+RANK_K_MAX = 64  # right-hand sides per hplb_rank_k call
+
+
+def _rank_k_chunks(lib, n: int, nrhs: int, Bc: torch.Tensor, Xc: torch.Tensor,
+                   Ac: torch.Tensor) -> None:
+    """Ac (n x n, column-major) = -Bbar X^T from the column-major n x nrhs
+    Bbar and X held as (nrhs, n) tensors Bc and Xc: one hplb_rank_k call per
+    RANK_K_MAX right-hand sides, the first storing and the rest accumulating
+    (nrhs = 0: one call with k = 0, which stores zeros)."""
+    for c0 in range(0, max(nrhs, 1), RANK_K_MAX):
+        kc = min(RANK_K_MAX, nrhs - c0)
+        lib.rank_k(n, n, kc, -1.0, Bc.data_ptr() + 8 * c0 * n, max(n, 1),
+                   Xc.data_ptr() + 8 * c0 * n, max(n, 1), Ac.data_ptr(), max(n, 1),
+                   accumulate=c0 > 0)
+
+
 class HplSolve(torch.autograd.Function):
-    """X = A^-1 B for a square FP64 CUDA A (n x n) and B (n x nrhs, nrhs <= 64
-    for the adjoint's fused rank-k kernel)."""
+    """X = A^-1 B for a square FP64 CUDA A (n x n) and B (n x nrhs)."""
 
     @staticmethod
     def forward(ctx, A: torch.Tensor, B: torch.Tensor, nb: int = 256, nbmin: int = 32):
@@ -91,11 +106,8 @@ class HplSolve(torch.autograd.Function):
                   max(n, 1))
         gA = None
         if ctx.needs_input_grad[0]:
-            if nrhs > 64:
-                raise HplError(6, "hpl_solve backward: the fused rank-k kernel takes <= 64 RHS")
             Ac = torch.empty(n, n, dtype=torch.float64, device=LU.device)
-            lib.rank_k(n, n, nrhs, -1.0, Bc.data_ptr(), max(n, 1), Xc.data_ptr(), max(n, 1),
-                       Ac.data_ptr(), max(n, 1))
+            _rank_k_chunks(lib, n, nrhs, Bc, Xc, Ac)
             gA = Ac.t()
         gB = Bc.t() if ctx.needs_input_grad[1] else None
         return gA, gB, None, None
