@@ -225,6 +225,11 @@ def pdgesv_grid(backend, comm, grid: Grid1xQ, algo, A, ld: int):
     all replicated.  On exit A holds this process's columns of the factors."""
     n, nb, q = grid.n, grid.nb, grid.q
     dev, f64, i32 = A.device, torch.float64, torch.int32
+    if A.dtype != f64:
+        raise ValueError("A must be a float64 tensor")
+    if ld < max(n, 1) or A.numel() < ld * grid.nq:
+        raise ValueError(f"process {q} holds {n} x {grid.nq}: needs ld >= {max(n, 1)} and "
+                         f"ld * {grid.nq} entries (ld {ld}, {A.numel()} entries)")
     ldl = (n + 1) & ~1  # even leading dimension of the broadcast panels
     Lb = [torch.zeros(ldl * nb, dtype=f64, device=dev) for _ in range(2)]
     # nb pivots + the panel's zero-pivot column, per buffer.

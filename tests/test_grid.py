@@ -162,3 +162,21 @@ def test_grid_solve_two_gloo_processes(oracle, tmp_path):
     results = [(np.array(r["x"]), np.array(r["ipiv"], dtype=np.int32), r["info"],
                 np.load(tmp_path / f"rank{r['rank']}.npy")) for r in res]
     _check(oracle, n, nb, 100, Algo(nb, 16, 2, 2, 2, 1, 0), results)
+
+
+def test_grid_rejects_a_local_array_that_is_too_small(oracle):
+    import torch
+
+    from grid_host import HostBackend
+    from rochpl_b200.grid import LocalGroup, pdgesv_grid
+    from rochpl_b200.hpl import Algo
+
+    g = Grid1xQ(64, 16, 0, 1)
+    comm = LocalGroup(1).member(0)
+    be, algo = HostBackend(oracle), Algo(16, 4, 2, 2, 2, 1, 0)
+    with pytest.raises(ValueError, match="ld >= 64"):
+        pdgesv_grid(be, comm, g, algo, torch.zeros(63 * 65, dtype=torch.float64), 63)
+    with pytest.raises(ValueError, match="entries"):
+        pdgesv_grid(be, comm, g, algo, torch.zeros(64 * 65 - 1, dtype=torch.float64), 64)
+    with pytest.raises(ValueError, match="float64"):
+        pdgesv_grid(be, comm, g, algo, torch.zeros(64 * 65, dtype=torch.float32), 64)
