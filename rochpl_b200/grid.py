@@ -35,8 +35,25 @@ from dataclasses import dataclass
 
 import torch
 
-__all__ = ["numroc", "Grid1xQ", "DeviceBackend", "LocalGroup", "DistGroup", "pdgesv_grid",
-           "matgen_local"]
+__all__ = ["check_algo", "numroc", "Grid1xQ", "DeviceBackend", "LocalGroup", "DistGroup",
+           "pdgesv_grid", "matgen_local"]
+
+
+def check_algo(algo) -> None:
+    """The checks hplb_pdgesv makes on the solve's HPL.dat parameters (the
+    HPL_pdinfo rules, src/pauxil/HPL_pdinfo.cpp, plus this library's limits),
+    made by every process before its first exchange, so that a bad value stops
+    the whole grid at once instead of the one process that factors a panel."""
+    if algo.nb < 1 or algo.nbmin < 1 or algo.ndiv < 2:
+        raise ValueError(f"NB {algo.nb}, NBMIN {algo.nbmin}, NDIV {algo.ndiv}: "
+                         "NB and NBMIN must be at least 1, NDIV at least 2")
+    if not (0 <= algo.pfact <= 2 and 0 <= algo.rfact <= 2):
+        raise ValueError(f"PFACT {algo.pfact} / RFACT {algo.rfact} outside 0 (left), "
+                         "1 (Crout), 2 (right)")
+    if algo.depth != 1:
+        raise ValueError("only look-ahead depth 1 is supported")
+    if algo.nbmin > 128 or algo.nb > 2048:
+        raise ValueError(f"NBMIN {algo.nbmin} / NB {algo.nb} above the limits 128 / 2048")
 
 
 def numroc(n: int, nb: int, iproc: int, nprocs: int) -> int:
@@ -225,6 +242,7 @@ def pdgesv_grid(backend, comm, grid: Grid1xQ, algo, A, ld: int):
     all replicated.  On exit A holds this process's columns of the factors."""
     n, nb, q = grid.n, grid.nb, grid.q
     dev, f64, i32 = A.device, torch.float64, torch.int32
+    check_algo(algo)
     if A.dtype != f64:
         raise ValueError("A must be a float64 tensor")
     if ld < max(n, 1) or A.numel() < ld * grid.nq:

@@ -39,7 +39,7 @@ from dataclasses import dataclass
 
 import torch
 
-from .grid import numroc
+from .grid import check_algo, numroc
 
 __all__ = ["Grid2D", "DeviceBackend2D", "pdgesv_2d", "matgen_local_2d", "LocalGrid2D", "dist_comms"]
 
@@ -128,8 +128,6 @@ class DeviceBackend2D:
     Local arrays are flat float64 CUDA tensors, column-major, addressed by
     element offsets."""
 
-    max_nb = 2048  # HPLB_TRSM_LOWER_MAX_N: the panel's triangular solve
-
     def __init__(self, lib):
         self.lib = lib
 
@@ -203,9 +201,7 @@ def pdgesv_2d(backend, comms, grid: Grid2D, algo, A, ld: int):
     mp, nq = grid.mp, grid.nq
     if A.dtype != f64 or A.dim() != 1:
         raise ValueError("A must be a flat float64 tensor")
-    max_nb = getattr(backend, "max_nb", None)
-    if max_nb is not None and nb > max_nb:  # every process fails here, before any exchange
-        raise ValueError(f"NB {nb} above this backend's limit {max_nb}")
+    check_algo(algo)  # on every process, before any exchange (NB <= 2048 among the rest)
     if ld < max(mp, 1) or A.numel() < ld * max(nq, 1):
         raise ValueError(f"process ({p}, {q}) holds {mp} x {nq}: needs ld >= {max(mp, 1)} and "
                          f"ld * {max(nq, 1)} entries (ld {ld}, {A.numel()} entries)")

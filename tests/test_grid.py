@@ -180,3 +180,19 @@ def test_grid_rejects_a_local_array_that_is_too_small(oracle):
         pdgesv_grid(be, comm, g, algo, torch.zeros(64 * 65 - 1, dtype=torch.float64), 64)
     with pytest.raises(ValueError, match="float64"):
         pdgesv_grid(be, comm, g, algo, torch.zeros(64 * 65, dtype=torch.float32), 64)
+
+
+@pytest.mark.parametrize("kw,msg", [({"nb": 0}, "at least 1"), ({"nbmin": 0}, "at least 1"),
+                                    ({"ndiv": 1}, "NDIV at least 2"), ({"pfact": 3}, "PFACT 3"),
+                                    ({"rfact": -1}, "RFACT -1"), ({"depth": 0}, "depth 1"),
+                                    ({"nbmin": 129}, "above the limits"),
+                                    ({"nb": 2049}, "above the limits")])
+def test_grid_algo_checks(kw, msg):
+    from dataclasses import replace
+
+    from rochpl_b200.grid import check_algo
+    from rochpl_b200.hpl import Algo
+
+    check_algo(Algo(512))
+    with pytest.raises(ValueError, match=msg):
+        check_algo(replace(Algo(512), **kw))

@@ -260,7 +260,7 @@ def test_grid2d_rejects_a_local_array_that_is_too_small(oracle):
         pdgesv_2d(be, comms, g, algo, torch.zeros(64 * 65, dtype=torch.float32), 64)
 
 
-def test_grid2d_device_backend_rejects_nb_above_its_limit(oracle):
+def test_grid2d_rejects_nb_above_the_limit_before_any_exchange(oracle):
     import torch
 
     from grid2d_host import FakeDeviceLib
@@ -268,6 +268,6 @@ def test_grid2d_device_backend_rejects_nb_above_its_limit(oracle):
     from rochpl_b200.hpl import Algo
 
     g = Grid2D(3000, 4096, 0, 0, 1, 1)
-    with pytest.raises(ValueError, match="NB 4096 above"):
+    with pytest.raises(ValueError, match="NB 4096 above the limits"):
         pdgesv_2d(DeviceBackend2D(FakeDeviceLib(oracle)), LocalGrid2D(1, 1).comms(0, 0), g,
                   Algo(4096), torch.zeros(3000 * 3001, dtype=torch.float64), 3000)
