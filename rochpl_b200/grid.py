@@ -56,6 +56,33 @@ def check_algo(algo) -> None:
         raise ValueError(f"NBMIN {algo.nbmin} / NB {algo.nb} above the limits 128 / 2048")
 
 
+def start_checks(comm, values, local_error, algo, device) -> None:
+    """The first step of a grid solve, the same on every process: one small
+    all-gather of this process's problem and solve parameters (`values`) and
+    of whether its local array is usable (`local_error`: a message, or None).
+    Then every process raises if its own array is unusable, if another
+    process's is, if the parameters differ between processes, or if
+    check_algo rejects them -- so a bad call stops the whole grid at once
+    instead of leaving processes waiting in an exchange that one of them
+    never reaches."""
+    flags = [float(v) for v in values] + [0.0 if local_error is None else 1.0]
+    allv = comm.all_gather(torch.tensor(flags, dtype=torch.float64, device=device)).cpu()
+    if local_error is not None:
+        raise ValueError(local_error)
+    bad = [r for r in range(allv.shape[0]) if allv[r, -1] != 0]
+    if bad:
+        raise ValueError(f"process {bad[0]} of the grid cannot run the solve (its local array)")
+    diff = [r for r in range(allv.shape[0]) if not torch.equal(allv[r, :-1], allv[0, :-1])]
+    if diff:
+        raise ValueError(f"the problem or solve parameters of process {diff[0]} differ from "
+                         "those of process 0")
+    check_algo(algo)
+
+
+def _algo_values(algo):
+    return [algo.nb, algo.nbmin, algo.ndiv, algo.pfact, algo.rfact, algo.depth]
+
+
 def numroc(n: int, nb: int, iproc: int, nprocs: int) -> int:
     """Columns of an n-column matrix in NB blocks that process iproc of nprocs
     holds, the distribution starting on process 0 (HPL_numroc)."""
@@ -242,12 +269,13 @@ def pdgesv_grid(backend, comm, grid: Grid1xQ, algo, A, ld: int):
     all replicated.  On exit A holds this process's columns of the factors."""
     n, nb, q = grid.n, grid.nb, grid.q
     dev, f64, i32 = A.device, torch.float64, torch.int32
-    check_algo(algo)
+    err = None
     if A.dtype != f64:
-        raise ValueError("A must be a float64 tensor")
-    if ld < max(n, 1) or A.numel() < ld * grid.nq:
-        raise ValueError(f"process {q} holds {n} x {grid.nq}: needs ld >= {max(n, 1)} and "
-                         f"ld * {grid.nq} entries (ld {ld}, {A.numel()} entries)")
+        err = "A must be a float64 tensor"
+    elif ld < max(n, 1) or A.numel() < ld * grid.nq:
+        err = (f"process {q} holds {n} x {grid.nq}: needs ld >= {max(n, 1)} and "
+               f"ld * {grid.nq} entries (ld {ld}, {A.numel()} entries)")
+    start_checks(comm, [n, nb, grid.Q] + _algo_values(algo), err, algo, dev)
     ldl = (n + 1) & ~1  # even leading dimension of the broadcast panels
     Lb = [torch.zeros(ldl * nb, dtype=f64, device=dev) for _ in range(2)]
     # nb pivots + the panel's zero-pivot column, per buffer.

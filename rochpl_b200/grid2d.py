@@ -39,7 +39,7 @@ from dataclasses import dataclass
 
 import torch
 
-from .grid import check_algo, numroc
+from .grid import _algo_values, numroc, start_checks
 
 __all__ = ["Grid2D", "DeviceBackend2D", "pdgesv_2d", "matgen_local_2d", "LocalGrid2D", "dist_comms"]
 
@@ -199,12 +199,14 @@ def pdgesv_2d(backend, comms, grid: Grid2D, algo, A, ld: int):
     n, nb, p, q = grid.n, grid.nb, grid.p, grid.q
     dev, f64 = A.device, torch.float64
     mp, nq = grid.mp, grid.nq
+    err = None
     if A.dtype != f64 or A.dim() != 1:
-        raise ValueError("A must be a flat float64 tensor")
-    check_algo(algo)  # on every process, before any exchange (NB <= 2048 among the rest)
-    if ld < max(mp, 1) or A.numel() < ld * max(nq, 1):
-        raise ValueError(f"process ({p}, {q}) holds {mp} x {nq}: needs ld >= {max(mp, 1)} and "
-                         f"ld * {max(nq, 1)} entries (ld {ld}, {A.numel()} entries)")
+        err = "A must be a flat float64 tensor"
+    elif ld < max(mp, 1) or A.numel() < ld * max(nq, 1):
+        err = (f"process ({p}, {q}) holds {mp} x {nq}: needs ld >= {max(mp, 1)} and "
+               f"ld * {max(nq, 1)} entries (ld {ld}, {A.numel()} entries)")
+    # Over the whole grid, before any other exchange (NB <= 2048 among the checks).
+    start_checks(world, [n, nb, grid.P, grid.Q] + _algo_values(algo), err, algo, dev)
     nbmin = max(1, min(algo.nbmin, nb))
     ndiv = max(2, algo.ndiv)
     ipiv = torch.zeros(max(n, 1), dtype=torch.int64)

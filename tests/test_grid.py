@@ -196,3 +196,47 @@ def test_grid_algo_checks(kw, msg):
     check_algo(Algo(512))
     with pytest.raises(ValueError, match=msg):
         check_algo(replace(Algo(512), **kw))
+
+
+@pytest.mark.parametrize("fault", ["small_array", "other_nb", "bad_algo_on_one"])
+def test_grid_bad_call_on_one_process_stops_every_process(oracle, fault):
+    """A bad call on one process (its local array too small, a different NB,
+    an invalid solve parameter) makes every process raise at the start of
+    the solve; none is left waiting in an exchange."""
+    import threading
+    from dataclasses import replace
+
+    import torch
+
+    from grid_host import HostBackend
+    from rochpl_b200.grid import LocalGroup, pdgesv_grid
+    from rochpl_b200.hpl import Algo
+
+    n, Q = 64, 2
+    grp = LocalGroup(Q)
+    errs = [None] * Q
+
+    def work(q):
+        nb = 8 if (fault == "other_nb" and q == 1) else 16
+        algo = Algo(16, 4, 2, 2, 2, 1, 0)
+        if fault == "bad_algo_on_one" and q == 1:
+            algo = replace(algo, ndiv=1)
+        g = Grid1xQ(n, nb, q, Q)
+        ld = oracle.default_ld(n)
+        size = ld * max(g.nq, 1) - (1 if (fault == "small_array" and q == 1) else 0)
+        try:
+            pdgesv_grid(HostBackend(oracle), grp.member(q), g, algo,
+                        torch.zeros(size, dtype=torch.float64), ld)
+        except ValueError as e:
+            errs[q] = str(e)
+        except BaseException as e:  # anything else is a failure of the test
+            errs[q] = e
+            grp.barrier.abort()
+
+    ts = [threading.Thread(target=work, args=(q,)) for q in range(Q)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=60)
+    assert not any(t.is_alive() for t in ts), "a process was left waiting"
+    assert all(isinstance(e, str) for e in errs), errs

@@ -271,3 +271,47 @@ def test_grid2d_rejects_nb_above_the_limit_before_any_exchange(oracle):
     with pytest.raises(ValueError, match="NB 4096 above the limits"):
         pdgesv_2d(DeviceBackend2D(FakeDeviceLib(oracle)), LocalGrid2D(1, 1).comms(0, 0), g,
                   Algo(4096), torch.zeros(3000 * 3001, dtype=torch.float64), 3000)
+
+
+@pytest.mark.parametrize("fault", ["small_array", "other_n", "bad_algo_on_one"])
+def test_grid2d_bad_call_on_one_process_stops_every_process(oracle, fault):
+    """As for the 1 x Q grid: a bad call on one process of a 2 x 2 grid makes
+    all four raise at the start of the solve."""
+    import threading
+    from dataclasses import replace
+
+    import torch
+
+    from grid2d_host import HostBackend2D
+    from rochpl_b200.grid2d import LocalGrid2D, pdgesv_2d
+    from rochpl_b200.hpl import Algo
+
+    P, Q = 2, 2
+    grp = LocalGrid2D(P, Q)
+    errs = [None] * (P * Q)
+
+    def work(p, q):
+        r = p * Q + q
+        n = 63 if (fault == "other_n" and r == 3) else 64
+        algo = Algo(16, 4, 2, 2, 2, 1, 0)
+        if fault == "bad_algo_on_one" and r == 2:
+            algo = replace(algo, pfact=5)
+        g = Grid2D(n, 16, p, q, P, Q)
+        ld = max(g.mp, 1)
+        size = ld * max(g.nq, 1) - (1 if (fault == "small_array" and r == 1) else 0)
+        try:
+            pdgesv_2d(HostBackend2D(oracle), grp.comms(p, q), g, algo,
+                      torch.zeros(size, dtype=torch.float64), ld)
+        except ValueError as e:
+            errs[r] = str(e)
+        except BaseException as e:  # anything else is a failure of the test
+            errs[r] = e
+            grp.abort()
+
+    ts = [threading.Thread(target=work, args=(p, q)) for p in range(P) for q in range(Q)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=60)
+    assert not any(t.is_alive() for t in ts), "a process was left waiting"
+    assert all(isinstance(e, str) for e in errs), errs
