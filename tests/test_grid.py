@@ -240,3 +240,53 @@ def test_grid_bad_call_on_one_process_stops_every_process(oracle, fault):
         t.join(timeout=60)
     assert not any(t.is_alive() for t in ts), "a process was left waiting"
     assert all(isinstance(e, str) for e in errs), errs
+
+
+_BAD_CHILD = r"""
+import os, sys
+import torch
+import torch.distributed as dist
+sys.path.insert(0, os.path.join(os.getcwd(), "tests"))
+from oracle import oracle as O
+from grid_host import HostBackend
+from rochpl_b200.grid import DistGroup, Grid1xQ, pdgesv_grid
+from rochpl_b200.hpl import Algo
+dist.init_process_group("gloo", init_method="env://")
+rank, Q = dist.get_rank(), dist.get_world_size()
+nb = 8 if rank == 1 else 16  # rank 1 was given another NB
+g = Grid1xQ(64, nb, rank, Q)
+ld = O.default_ld(64)
+A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64)
+try:
+    pdgesv_grid(HostBackend(O), DistGroup(), g, Algo(16, 4, 2, 2, 2, 1, 0), A, ld)
+    print("SOLVED")
+except ValueError as e:
+    print("REJECTED " + str(e))
+dist.destroy_process_group()
+"""
+
+
+def test_grid_bad_call_stops_two_gloo_processes(tmp_path):
+    """Two gloo processes, one given another NB: both reject the call at the
+    start of the solve and exit, long before any process-group timeout."""
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", LOCAL_RANK=str(rank),
+                   MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
+                   PYTHONPATH=ROOT + os.pathsep + os.environ.get("PYTHONPATH", ""))
+        procs.append(subprocess.Popen([sys.executable, "-c", _BAD_CHILD], env=env, cwd=ROOT,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    outs = []
+    for p in procs:
+        try:
+            so, se = p.communicate(timeout=120)
+        except subprocess.TimeoutExpired:
+            for q in procs:
+                q.kill()
+            raise
+        assert p.returncode == 0, se[-3000:]
+        outs.append(so)
+    assert all("REJECTED" in so and "SOLVED" not in so for so in outs), outs
