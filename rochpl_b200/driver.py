@@ -339,19 +339,39 @@ def config_from_argv(argv) -> HplConfig:
     return cfg
 
 
+def shared_config(argv, rank: int):
+    """The run's configuration on every process of a torch.distributed job,
+    as HPL_pdinfo does it (src/HPL_pdinfo.cpp): process 0 alone reads the
+    command line and HPL.dat, and every process takes its values from it.
+    Returns the HplConfig, or the message of the input error, the same on
+    every process, so a bad input ends every process and none waits for the
+    others."""
+    import torch.distributed as dist
+
+    box = [None]
+    if rank == 0:
+        try:
+            box[0] = config_from_argv(argv)
+        except (HplInputError, OSError) as e:
+            box[0] = str(e)
+    dist.broadcast_object_list(box, src=0)
+    return box[0]
+
+
 def main(argv=None) -> int:
     argv = list(sys.argv[1:] if argv is None else argv)
     progress = "--progress" in argv
     if progress:
         argv.remove("--progress")
-    try:
-        cfg = config_from_argv(argv)
-    except HplInputError as e:
-        print(e, file=sys.stderr)
-        return 1
     import os
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world == 1:
+        try:
+            cfg = config_from_argv(argv)
+        except HplInputError as e:
+            print(e, file=sys.stderr)
+            return 1
     solver, rank = None, 0
     if world > 1:  # one process per GPU under torchrun: the P x Q = world grids
         import torch
@@ -360,6 +380,12 @@ def main(argv=None) -> int:
         rank, local = int(os.environ.get("RANK", "0")), int(os.environ.get("LOCAL_RANK", "0"))
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+        cfg = shared_config(argv, rank)
+        if isinstance(cfg, str):
+            if rank == 0:
+                print(cfg, file=sys.stderr)
+            dist.destroy_process_group()
+            return 1
         solver = GridSolver(local)
     try:
         if rank != 0:

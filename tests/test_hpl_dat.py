@@ -89,3 +89,58 @@ def test_cli():
     assert parse_cli(["-i", "HPL.dat"]) is None
     with pytest.raises(HplInputError):
         parse_cli(["-N", "0"])
+
+
+_SHARED_CHILD = r"""
+import json, os, sys
+import torch.distributed as dist
+from rochpl_b200.driver import shared_config
+dist.init_process_group("gloo", init_method="env://")
+rank = dist.get_rank()
+# Only process 0's input exists; the other process is given a path that does not.
+argv = ["-i", os.environ["DAT"] if rank == 0 else os.environ["DAT"] + ".missing"]
+cfg = shared_config(argv, rank)
+out = cfg if isinstance(cfg, str) else {"ns": cfg.ns, "nbs": cfg.nbs, "iters": cfg.iters}
+print("RESULT " + json.dumps(out))
+dist.destroy_process_group()
+"""
+
+
+@pytest.mark.parametrize("kw,want", [(dict(n="1000 2000", nn="2", nb="128"), None),
+                                     (dict(depth="0"), "Value of DEPTH must be 1")])
+def test_process_0_reads_the_input_for_every_process(tmp_path, kw, want):
+    """As HPL_pdinfo: under torch.distributed, process 0 reads HPL.dat and
+    every process takes its values -- or its input error -- from there."""
+    import json
+    import socket
+    import subprocess
+    import sys
+
+    path = tmp_path / "HPL.dat"
+    path.write_text(dat(**kw))
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    root = os.path.dirname(HERE)
+    procs = []
+    for rank in range(2):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE="2", MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), DAT=str(path),
+                   PYTHONPATH=root + os.pathsep + os.environ.get("PYTHONPATH", ""))
+        procs.append(subprocess.Popen([sys.executable, "-c", _SHARED_CHILD], env=env, cwd=root,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    res = []
+    for p in procs:
+        try:
+            so, se = p.communicate(timeout=120)
+        except subprocess.TimeoutExpired:
+            for q in procs:
+                q.kill()
+            raise
+        assert p.returncode == 0, se[-3000:]
+        res.append(json.loads([ln for ln in so.splitlines() if ln.startswith("RESULT ")][-1][7:]))
+    assert res[0] == res[1]
+    if want is None:
+        assert res[0] == {"ns": [1000, 2000], "nbs": [128], "iters": 1}
+    else:
+        assert want in res[0]
