@@ -15,7 +15,7 @@ import os
 
 import numpy as np
 
-from .lib import HPLB_BATCH_CLASSES, HPLB_OK, HplError, Library
+from .lib import HPLB_BATCH_CLASSES, Library
 
 __all__ = ["BatchPlan", "BatchShard", "autotune", "workload_sizes", "batch_flops",
            "system_cost", "partition_systems"]

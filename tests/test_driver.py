@@ -5,10 +5,8 @@ in place of the GPU.  Expected lines are rebuilt here with explicit padding
 (not with the driver's printf-style strings)."""
 import io
 
-import pytest
-
 from rochpl_b200.driver import (progress_lines, residual_lines, result_lines, run, summary_lines,
-                                sweep, table_header, tv_code)
+                                sweep, tv_code)
 from rochpl_b200.hpl import Algo, HplConfig, parse_hpl_dat
 
 EPS = 2.0 ** -53
