@@ -82,7 +82,8 @@ typedef struct hplb_timing {
  * reason in *status when status is not NULL.  A process may hold several
  * contexts (one per host thread, say), all on one device: some kernels' shared
  * memory limits are raised once per process, so drive each GPU from its own
- * process, as rocHPL's one MPI rank per GPU does. */
+ * process, as rocHPL's one MPI rank per GPU does.  A context on a second
+ * device is refused with HPLB_ERR_UNSUPPORTED (and a message on stderr). */
 hplb_ctx* hplb_create(int device, hplb_status* status);
 void      hplb_destroy(hplb_ctx* ctx);
 

@@ -15,6 +15,7 @@
 // kernel turns them into the row map the trailing swap uses (the reference
 // copies pivots to the host and back once per panel, HPL_pdpanel_swapids.cpp).
 #include <algorithm>
+#include <atomic>
 #include <cstdlib>
 #include <cstdarg>
 #include <cstdio>
@@ -240,6 +241,15 @@ hplb_ctx* hplb_create(int device, hplb_status* status) {
   if(cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
     cudaGetLastError();
     return fail(ndev == 0 ? HPLB_ERR_CUDA : HPLB_ERR_ARG);
+  }
+  // Some kernels' shared-memory limits are raised once per process, on the
+  // device current at the time: every context of a process is on one device.
+  static std::atomic<int> process_device{-1};
+  int first = -1;
+  if(!process_device.compare_exchange_strong(first, device) && first != device) {
+    std::fprintf(stderr, "hplb_create: device %d, but this process already uses device %d "
+                         "(one process drives one GPU)\n", device, first);
+    return fail(HPLB_ERR_UNSUPPORTED);
   }
   if(cudaSetDevice(device) != cudaSuccess) return fail(HPLB_ERR_CUDA);
   hplb_ctx* ctx = new hplb_ctx();
