@@ -374,7 +374,8 @@ _default = {}
 
 
 def library(device: int = 0) -> Library:
-    """Process-wide context per device."""
+    """The process's shared context on `device` (a process drives one device:
+    hplb_create refuses a second)."""
     if device not in _default:
         _default[device] = Library(device)
     return _default[device]
