@@ -210,11 +210,12 @@ class GridSolver:
     rochpl_b200.grid, or the 2-D one of rochpl_b200.grid2d when P > 1.  The
     solve is timed by the wall clock between two barriers, the slowest
     process's time (as HPL_ptimer_combine takes the maximum); the residual is
-    computed on rank 0 against the regenerated matrix."""
+    computed on rank 0 against the regenerated matrix.  pmap: HPL.dat's PMAP,
+    the order of the processes on a P x Q grid (0 row-, 1 column-major)."""
 
     takes_grid = True  # run() passes each test's (P, Q)
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, pmap: int = 0):
         import torch
         import torch.distributed as dist
 
@@ -229,6 +230,7 @@ class GridSolver:
         self.backend2d = DeviceBackend2D(self.lib)
         self.comm = DistGroup()
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
+        self.pmap = pmap
         self._comms2d = {}  # (P, Q) -> (row, col, world); every rank builds the same groups
 
     def _run(self, algo: Algo, n: int, seed: int, grid):
@@ -246,9 +248,9 @@ class GridSolver:
             solve = lambda: pdgesv_grid(self.backend, self.comm, g, algo, A, ld)  # noqa: E731
         else:
             if (P, Q) not in self._comms2d:
-                self._comms2d[(P, Q)] = dist_comms(P, Q)
-            p, q = divmod(self.rank, Q)
-            g = Grid2D(n, algo.nb, p, q, P, Q)
+                self._comms2d[(P, Q)] = dist_comms(P, Q, self.pmap)
+            p, q = Grid2D.coords(self.rank, P, Q, self.pmap)
+            g = Grid2D(n, algo.nb, p, q, P, Q, self.pmap)
             ld = (max(g.mp, 1) + 1) // 2 * 2  # even: the DGEMM's TMA path
             A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64, device=dev)
             matgen_local_2d(self.backend2d, g, seed, A, ld)
@@ -386,7 +388,7 @@ def main(argv=None) -> int:
                 print(cfg, file=sys.stderr)
             dist.destroy_process_group()
             return 1
-        solver = GridSolver(local)
+        solver = GridSolver(local, pmap=cfg.pmap)
     try:
         if rank != 0:
             tally = run(cfg, _Discard(), solver=solver, world=world)

@@ -47,13 +47,16 @@ __all__ = ["Grid2D", "DeviceBackend2D", "pdgesv_2d", "matgen_local_2d", "LocalGr
 @dataclass
 class Grid2D:
     """Block-cyclic bookkeeping of the N x (N+1) [A|b] on process (p, q) of a
-    P x Q grid (row-major process order: rank = p Q + q)."""
+    P x Q grid.  pmap is HPL.dat's PMAP, the order of the processes on the
+    grid (HPL_grid_init, src/grid/HPL_grid_init.cpp): 0 row-major
+    (rank = p Q + q), 1 column-major (rank = q P + p)."""
     n: int
     nb: int
     p: int
     q: int
     P: int
     Q: int
+    pmap: int = 0
 
     @property
     def mp(self) -> int:
@@ -68,7 +71,12 @@ class Grid2D:
         return (self.n + self.nb - 1) // self.nb
 
     def rank_of(self, p: int, q: int) -> int:
-        return p * self.Q + q
+        return p * self.Q + q if self.pmap == 0 else q * self.P + p
+
+    @staticmethod
+    def coords(rank: int, P: int, Q: int, pmap: int = 0):
+        """(p, q) of `rank` on a P x Q grid in PMAP order."""
+        return divmod(rank, Q) if pmap == 0 else (rank % P, rank // P)
 
     def row_owner(self, g: int) -> int:
         return (g // self.nb) % self.P
@@ -400,29 +408,30 @@ def _backsolve(be, row, world, grid, A, ld):
 class LocalGrid2D:
     """The three communicators of each process of a P x Q grid run as threads
     of one process (rochpl_b200.grid.LocalGroup for each process row, each
-    process column and the whole grid): comms(p, q) -> (row, col, world)."""
+    process column and the whole grid): comms(p, q) -> (row, col, world),
+    the world ranks in PMAP order."""
 
-    def __init__(self, P: int, Q: int):
+    def __init__(self, P: int, Q: int, pmap: int = 0):
         from .grid import LocalGroup
 
-        self.P, self.Q = P, Q
+        self.P, self.Q, self.pmap = P, Q, pmap
         self.rows = [LocalGroup(Q) for _ in range(P)]
         self.cols = [LocalGroup(P) for _ in range(Q)]
         self.world = LocalGroup(P * Q)
 
     def comms(self, p: int, q: int):
-        return (self.rows[p].member(q), self.cols[q].member(p),
-                self.world.member(p * self.Q + q))
+        rank = p * self.Q + q if self.pmap == 0 else q * self.P + p
+        return self.rows[p].member(q), self.cols[q].member(p), self.world.member(rank)
 
     def abort(self):
         for g in self.rows + self.cols + [self.world]:
             g.barrier.abort()
 
 
-def dist_comms(P: int, Q: int):
+def dist_comms(P: int, Q: int, pmap: int = 0):
     """(row, col, world) communicators of this process of a P x Q grid over
-    torch.distributed (rank = p Q + q; world size P Q).  Every process creates
-    every group, in the same order."""
+    torch.distributed (world size P Q; ranks on the grid in PMAP order, as
+    Grid2D.coords).  Every process creates every group, in the same order."""
     import torch.distributed as dist
 
     from .grid import DistGroup
@@ -430,7 +439,8 @@ def dist_comms(P: int, Q: int):
     rank = dist.get_rank()
     if dist.get_world_size() != P * Q:
         raise ValueError(f"a {P} x {Q} grid needs {P * Q} processes, not {dist.get_world_size()}")
-    p, q = divmod(rank, Q)
-    rows = [dist.new_group([pp * Q + qq for qq in range(Q)]) for pp in range(P)]
-    cols = [dist.new_group([pp * Q + qq for pp in range(P)]) for qq in range(Q)]
+    p, q = Grid2D.coords(rank, P, Q, pmap)
+    at = Grid2D(0, 1, 0, 0, P, Q, pmap).rank_of
+    rows = [dist.new_group([at(pp, qq) for qq in range(Q)]) for pp in range(P)]
+    cols = [dist.new_group([at(pp, qq) for pp in range(P)]) for qq in range(Q)]
     return DistGroup(rows[p]), DistGroup(cols[q]), DistGroup()

@@ -49,14 +49,28 @@ def test_grid2d_bookkeeping_matches_brute_force(n, nb, P, Q):
                                                len(cols))
 
 
-def _run_rank(oracle, comms, n, nb, P, Q, p, q, seed, algo):
+@pytest.mark.parametrize("P,Q", [(1, 1), (2, 3), (3, 2), (4, 1), (1, 4)])
+@pytest.mark.parametrize("pmap", [0, 1])
+def test_grid2d_process_order(P, Q, pmap):
+    """PMAP's two orders (HPL_grid_init): every rank has one (p, q) and back."""
+    seen = set()
+    for rank in range(P * Q):
+        p, q = Grid2D.coords(rank, P, Q, pmap)
+        assert 0 <= p < P and 0 <= q < Q
+        assert Grid2D(10, 2, p, q, P, Q, pmap).rank_of(p, q) == rank
+        assert rank == (p * Q + q if pmap == 0 else q * P + p)
+        seen.add((p, q))
+    assert len(seen) == P * Q
+
+
+def _run_rank(oracle, comms, n, nb, P, Q, p, q, seed, algo, pmap=0):
     import torch
 
     from grid2d_host import HostBackend2D, local_to_global_2d
     from rochpl_b200.grid2d import matgen_local_2d, pdgesv_2d
 
     be = HostBackend2D(oracle)
-    g = Grid2D(n, nb, p, q, P, Q)
+    g = Grid2D(n, nb, p, q, P, Q, pmap)
     ld = max(g.mp, 1) + 3  # any ld >= mp
     A = torch.zeros(ld * max(g.nq, 1), dtype=torch.float64)
     matgen_local_2d(be, g, seed, A, ld)
@@ -188,6 +202,36 @@ def test_grid2d_left_and_crout_orderings_match_the_oracle(oracle, n, nb, P, Q, p
     _check(oracle, n, nb, 100, algo, out)
 
 
+@pytest.mark.parametrize("n,nb,P,Q", [(100, 16, 2, 3), (97, 8, 3, 2)])  # P != Q: the orders differ
+def test_grid2d_column_major_process_order_matches_the_oracle(oracle, n, nb, P, Q):
+    """PMAP = 1: the world ranks in column-major order on the grid (the
+    back-solve's broadcasts of x use them); the same solve as row-major."""
+    import threading
+
+    from rochpl_b200.grid2d import LocalGrid2D
+    from rochpl_b200.hpl import Algo
+
+    algo = Algo(nb, 4, 2, 2, 2, 1, 0)
+    grp = LocalGrid2D(P, Q, pmap=1)
+    out, errs = [None] * (P * Q), []
+
+    def work(p, q):
+        try:
+            out[q * P + p] = _run_rank(oracle, grp.comms(p, q), n, nb, P, Q, p, q, 100, algo,
+                                       pmap=1)
+        except BaseException as e:  # surfaced below
+            errs.append(e)
+            grp.abort()
+
+    ts = [threading.Thread(target=work, args=(p, q)) for p in range(P) for q in range(Q)]
+    for t in ts:
+        t.start()
+    for t in ts:
+        t.join(timeout=180)
+    assert not errs, errs
+    _check(oracle, n, nb, 100, algo, out)
+
+
 _CHILD = r"""
 import json, os, sys
 import numpy as np
@@ -197,19 +241,22 @@ from oracle import oracle as O
 from rochpl_b200.grid2d import dist_comms
 from rochpl_b200.hpl import Algo
 from test_grid2d import _run_rank
-n, nb, P, Q = (int(os.environ[k]) for k in ("GN", "GNB", "GP", "GQ"))
+from rochpl_b200.grid2d import Grid2D
+n, nb, P, Q, pmap = (int(os.environ[k]) for k in ("GN", "GNB", "GP", "GQ", "GPMAP"))
 dist.init_process_group("gloo", init_method="env://")
 rank = dist.get_rank()
-p, q = divmod(rank, Q)
-comms = dist_comms(P, Q)
-x, ipiv, info, F = _run_rank(O, comms, n, nb, P, Q, p, q, 100, Algo(nb, 8, 2, 2, 2, 1, 0))
+p, q = Grid2D.coords(rank, P, Q, pmap)
+comms = dist_comms(P, Q, pmap)
+x, ipiv, info, F = _run_rank(O, comms, n, nb, P, Q, p, q, 100, Algo(nb, 8, 2, 2, 2, 1, 0),
+                             pmap=pmap)
 np.save(os.environ["GOUT"] + f"/rank{rank}.npy", F)
 print("RESULT " + json.dumps({"rank": rank, "x": x.tolist(), "ipiv": ipiv.tolist(), "info": info}))
 dist.destroy_process_group()
 """
 
 
-def test_grid2d_solve_four_gloo_processes(oracle, tmp_path):
+@pytest.mark.parametrize("pmap", [0, 1])
+def test_grid2d_solve_four_gloo_processes(oracle, tmp_path, pmap):
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
         port = s.getsockname()[1]
@@ -218,7 +265,7 @@ def test_grid2d_solve_four_gloo_processes(oracle, tmp_path):
     for rank in range(P * Q):
         env = dict(os.environ, RANK=str(rank), WORLD_SIZE=str(P * Q), LOCAL_RANK=str(rank),
                    MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), GN=str(n), GNB=str(nb),
-                   GP=str(P), GQ=str(Q), GOUT=str(tmp_path),
+                   GP=str(P), GQ=str(Q), GPMAP=str(pmap), GOUT=str(tmp_path),
                    PYTHONPATH=ROOT + os.pathsep + os.environ.get("PYTHONPATH", ""))
         procs.append(subprocess.Popen([sys.executable, "-c", _CHILD], env=env, cwd=ROOT,
                                       stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
