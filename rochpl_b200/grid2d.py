@@ -48,7 +48,8 @@ __all__ = ["Grid2D", "DeviceBackend2D", "pdgesv_2d", "matgen_local_2d", "LocalGr
 class Grid2D:
     """Block-cyclic bookkeeping of the N x (N+1) [A|b] on process (p, q) of a
     P x Q grid.  pmap is HPL.dat's PMAP, the order of the processes on the
-    grid (HPL_grid_init, src/grid/HPL_grid_init.cpp): 0 row-major
+    grid (HPL_grid_init, src/grid/HPL_grid_init.cpp:86-109, on one node,
+    where rocHPL's node-local tile is the whole grid): 0 row-major
     (rank = p Q + q), 1 column-major (rank = q P + p)."""
     n: int
     nb: int
