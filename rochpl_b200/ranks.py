@@ -1,10 +1,10 @@
 """Host-side plumbing for runs over several ranks, one process per GPU.
 
-The FP64 solve does not shard at P = Q = 1 (the reference's process grid,
-include/hpl_grid.hpp; its 2-D block-cyclic exchanges live in src/comm and
-src/pgesv/HPL_pdlaswp.cpp and are not part of this path): each rank solves its
-own system (replicas, seed 100 + rank) and the one exchange is the timing, the
-max over ranks.  The batched form shards: its systems are split across ranks
+The FP64 solve at P = Q = 1 does not shard: each rank solves its own system
+(replicas, seed 100 + rank) and the one exchange is the timing, the max over
+ranks.  (One system across ranks is the process-grid solve of
+rochpl_b200.grid, 1 x Q, and rochpl_b200.grid2d, P x Q, with communicators of
+their own.)  The batched form shards: its systems are split across ranks
 by a cost-balanced partition (batch.partition_systems), every rank generates
 and solves only its own systems, and the one data exchange is the per-system
 residual vector, assembled once at the end (Ranks.assemble).
