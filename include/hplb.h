@@ -1,5 +1,7 @@
 /*
- * hplb.h -- C ABI of the B200-native HPL solve path (single process, P = Q = 1).
+ * hplb.h -- C ABI of the B200-native HPL solve path: the single-process
+ * (P = Q = 1) solve, and the per-process building blocks of the process-grid
+ * drivers (rochpl_b200/grid.py for 1 x Q, rochpl_b200/grid2d.py for P x Q).
  *
  * Drop-in boundary for rocHPL's solve path.  Each entry point names the
  * reference interface it replaces (paths are within the rocHPL tree):

@@ -1,4 +1,4 @@
-"""The HPL run driver at P = Q = 1: what rocHPL's xhpl does around the solve.
+"""The HPL run driver: what rocHPL's xhpl does around the solve.
 
   sweep       the parameter loops of src/HPL_pddriver.cpp:120-212, in the same
               order: grids, then N, NB, DEPTH, BCAST, RFACT, PFACT, NBMIN, NDIV
@@ -13,9 +13,11 @@
               (HPL_PROGRESS_REPORT), from hplb_last_steps
 
 One process runs the 1 x 1 grids (GpuSolver).  Launched as W processes (one
-per GPU, torchrun), the driver runs the 1 x W grids as one distributed solve
-(GridSolver: rochpl_b200.grid, NB-wide column blocks cyclic over the GPUs,
-the panel broadcast over NCCL) and rank 0 writes the output.  Other grids are
+per GPU, torchrun), the driver runs the P x Q grids with P Q = W as one
+distributed solve (GridSolver: rochpl_b200.grid for 1 x W, NB-wide column
+blocks cyclic over the GPUs and the panel broadcast over NCCL;
+rochpl_b200.grid2d for P > 1, the processes placed in PMAP order); process 0
+reads the input for all and writes the output.  Grids of another size are
 counted as skipped tests.  The solve itself, the generator and the residual run
 on the GPU through libhplb200.so; the driver only formats and counts, so its
 loops and output are tested with a stand-in solver on the CPU.
