@@ -13,7 +13,8 @@
 // RFACT, PFACT, NBMIN, NDIV; src/HPL_pddriver.cpp:120-212); per test a warm-up
 // solve of at most 2 NB + 1 columns (the role of src/HPL_pdwarmup.cpp), then
 // `-it` repetitions of generate, timed hplb_pdgesv, residual check.  Grids
-// other than 1 x 1 are counted as skipped tests.  Output: the reference's lines
+// other than 1 x 1 are counted as skipped tests (the Python driver,
+// rochpl_b200/driver.py under torchrun, runs P x Q grids).  Output: the reference's lines
 // (src/HPL_pdtest.cpp:144-213 and :439-475, src/HPL_pddriver.cpp:226-283) and,
 // with --progress, the per-step rows of src/pgesv/HPL_pdgesv.cpp:155-341.
 // --list prints the sweep without touching a GPU.
@@ -442,7 +443,9 @@ const char* kUsage =
     "usage: hplb [-N n] [-NB nb] [-P p] [-Q q] [-p p] [-q q] [-f frac] [-it k] [-i HPL.dat]\n"
     "            [--progress] [--list] [--device d]\n"
     "  -N, -NB        problem size and block size (default 45312, 384)\n"
-    "  -P, -Q         process grid; only 1 x 1 runs, other grids count as skipped tests\n"
+    "  -P, -Q         process grid; this single process runs 1 x 1, other grids count as\n"
+    "                 skipped tests (P x Q grids: python -m rochpl_b200.driver, one process\n"
+    "                 per GPU under torchrun)\n"
     "  -p, -q, -f     accepted for compatibility (node-local grid, panel fraction)\n"
     "  -it k          timed repetitions of each test (after one warm-up)\n"
     "  -i HPL.dat     read the parameter sweep from an HPL.dat\n"
