@@ -217,19 +217,28 @@ class GridSolver:
 
     takes_grid = True  # run() passes each test's (P, Q)
 
-    def __init__(self, device: int = 0, pmap: int = 0):
+    def __init__(self, device: int = 0, pmap: int = 0, lib=None, backend=None, backend2d=None,
+                 dev=None):
+        """lib, backend, backend2d and dev, when given, stand in for the GPU's
+        library (its residual check), the two grid backends and the device:
+        the tests run this solver's orchestration on CPU with host
+        backends."""
         import torch
         import torch.distributed as dist
 
         from .grid import DeviceBackend, DistGroup
         from .grid2d import DeviceBackend2D
-        from .lib import library
 
         self.torch, self.dist = torch, dist
         self.device = device
-        self.lib = library(device)
-        self.backend = DeviceBackend(self.lib)
-        self.backend2d = DeviceBackend2D(self.lib)
+        if lib is None:
+            from .lib import library
+
+            lib = library(device)
+        self.lib = lib
+        self.backend = backend if backend is not None else DeviceBackend(lib)
+        self.backend2d = backend2d if backend2d is not None else DeviceBackend2D(lib)
+        self.dev = dev if dev is not None else torch.device("cuda", device)
         self.comm = DistGroup()
         self.rank, self.world = dist.get_rank(), dist.get_world_size()
         self.pmap = pmap
@@ -241,7 +250,7 @@ class GridSolver:
 
         torch = self.torch
         P, Q = grid if grid is not None else (1, self.world)
-        dev = torch.device("cuda", self.device)
+        dev = self.dev
         if P == 1:
             g = Grid1xQ(n, algo.nb, self.rank, self.world)
             ld = default_ld(n)
@@ -258,15 +267,19 @@ class GridSolver:
             matgen_local_2d(self.backend2d, g, seed, A, ld)
             comms = self._comms2d[(P, Q)]
             solve = lambda: pdgesv_2d(self.backend2d, comms, g, algo, A, ld)  # noqa: E731
-        torch.cuda.synchronize(self.device)
+        self._sync()
         self.dist.barrier()
         t_start = time.time()
         t0 = time.perf_counter()
         x, ipiv, info = solve()
-        torch.cuda.synchronize(self.device)
+        self._sync()
         w = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device=dev)
         self.dist.all_reduce(w, op=self.dist.ReduceOp.MAX)
         return x, info, float(w.item()), t_start, time.time()
+
+    def _sync(self):
+        if self.dev.type == "cuda":
+            self.torch.cuda.synchronize(self.dev)
 
     def warmup(self, algo: Algo, n: int, grid=None) -> None:
         self._run(algo, min(n, 2 * algo.nb * self.world + 1), HPL_ISEED, grid)

@@ -5,6 +5,8 @@ in place of the GPU.  Expected lines are rebuilt here with explicit padding
 (not with the driver's printf-style strings)."""
 import io
 
+import pytest
+
 from rochpl_b200.driver import (progress_lines, residual_lines, result_lines, run, summary_lines,
                                 sweep, tv_code)
 from rochpl_b200.hpl import Algo, HplConfig, parse_hpl_dat
@@ -179,3 +181,113 @@ def test_two_d_grids_run_with_a_grid_solver():
     assert (1, 2) in grids and (2, 1) in grids and (2, 2) not in grids
     assert sorted(pf for _, g, pf, _ in [c for c in s.calls if len(c) == 4] if g == (2, 1)) == [0, 2]
     assert tally["passed"] == 4 and tally["skipped"] == 2
+
+
+_GRID_DAT = """HPLinpack benchmark input file
+process-grid driver test
+HPL.out      output file name (if any)
+6            device out (6=stdout,7=stderr,file)
+2            # of problems sizes (N)
+64 100       Ns
+1            # of NBs
+16           NBs
+{pmap}            PMAP process mapping (0=Row-,1=Column-major)
+4            # of process grids (P x Q)
+2 4 1 1      Ps
+2 1 2 4      Qs
+16.0         threshold
+1            # of panel fact
+2            PFACTs (0=left, 1=Crout, 2=Right)
+1            # of recursive stopping criterium
+4            NBMINs (>= 1)
+1            # of panels in recursion
+2            NDIVs
+1            # of recursive panel fact.
+2            RFACTs (0=left, 1=Crout, 2=Right)
+1            # of broadcast
+0            BCASTs (0=1rg,1=1rM,2=2rg,3=2rM,4=Lng,5=LnM)
+1            # of lookahead depth
+1            DEPTHs (>=0)
+1            SWAP (0=bin-exch,1=long,2=mix)
+64           swapping threshold
+0            L1 in (0=transposed,1=no-transposed) form
+0            U  in (0=transposed,1=no-transposed) form
+0            Equilibration (0=no,1=yes)
+8            memory alignment in double (> 0)
+"""
+
+_GRID_CHILD = r"""
+import ctypes, io, json, os, sys
+import numpy as np
+import torch
+import torch.distributed as dist
+sys.path.insert(0, os.path.join(os.getcwd(), "tests"))
+from oracle import oracle as O
+from grid_host import HostBackend
+from grid2d_host import HostBackend2D
+from rochpl_b200.driver import GridSolver, run
+from rochpl_b200.hpl import parse_hpl_dat
+
+
+class HostResidual:  # the library's hplb_residual_lcg, on host memory
+    def residual_lcg(self, n, seed, xptr):
+        x = np.ctypeslib.as_array((ctypes.c_double * n).from_address(xptr)).copy()
+        return O.residual(O.matgen(n, n + 1, seed), n, x)
+
+
+dist.init_process_group("gloo", init_method="env://")
+rank = dist.get_rank()
+cfg = parse_hpl_dat(open(os.environ["DAT"]).read())
+solver = GridSolver(0, pmap=cfg.pmap, lib=HostResidual(), backend=HostBackend(O),
+                    backend2d=HostBackend2D(O), dev=torch.device("cpu"))
+out = io.StringIO()
+tally = run(cfg, out, solver=solver, world=dist.get_world_size())
+print("RESULT " + json.dumps({"rank": rank, "tally": tally, "out": out.getvalue()}))
+dist.destroy_process_group()
+"""
+
+
+@pytest.mark.parametrize("pmap", [0, 1])
+def test_grid_solver_runs_an_hpl_dat_on_four_gloo_processes(tmp_path, pmap):
+    """GridSolver's orchestration on CPU: four gloo processes run an HPL.dat
+    with grids 2 x 2, 4 x 1, 1 x 2 and 1 x 4 through the driver, host backends
+    standing in for the GPU.  The 1 x 4 grid takes the 1 x Q solve, 2 x 2 and
+    4 x 1 the P x Q solve in PMAP order, 1 x 2 is skipped (not four
+    processes); every solve passes the residual check on process 0."""
+    import json
+    import os
+    import socket
+    import subprocess
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    path = tmp_path / "HPL.dat"
+    path.write_text(_GRID_DAT.format(pmap=pmap))
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    procs = []
+    for rank in range(4):
+        env = dict(os.environ, RANK=str(rank), WORLD_SIZE="4", MASTER_ADDR="127.0.0.1",
+                   MASTER_PORT=str(port), DAT=str(path),
+                   PYTHONPATH=root + os.pathsep + os.environ.get("PYTHONPATH", ""))
+        procs.append(subprocess.Popen([sys.executable, "-c", _GRID_CHILD], env=env, cwd=root,
+                                      stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+    res = []
+    for p in procs:
+        try:
+            so, se = p.communicate(timeout=300)
+        except subprocess.TimeoutExpired:
+            for q in procs:
+                q.kill()
+            raise
+        assert p.returncode == 0, se[-3000:]
+        res.append(json.loads([ln for ln in so.splitlines() if ln.startswith("RESULT ")][-1][7:]))
+    res.sort(key=lambda r: r["rank"])
+    assert all(r["tally"] == {"passed": 6, "failed": 0, "skipped": 2} for r in res)
+    lines = res[0]["out"].splitlines()
+    tv = "WC" if pmap == 1 else "WR"
+    results = [ln.split() for ln in lines if ln.startswith(tv)]
+    assert sorted((int(f[1]), int(f[3]), int(f[4])) for f in results) == sorted(
+        (n, p, q) for n in (64, 100) for p, q in ((2, 2), (4, 1), (1, 4)))
+    assert sum("PASSED" in ln for ln in lines) == 6
